@@ -1,0 +1,219 @@
+/*
+ * tesserae_b200.h -- C ABI of libtesserae_b200.so, the B200 (sm_100a) explicit
+ * material-point-method step of Tesserae.jl.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns
+ * an int status (TB_OK = 0, negative on error; tb_last_error() gives the message).
+ * No C++ exception crosses this boundary.
+ *
+ * All particle, grid, partition and weight arrays are CALLER-OWNED device memory
+ * (Julia CuArrays via `pointer`, or cudaMalloc/torch in tests). The library owns
+ * only its scratch (sort buffers, scan partials, host-staging buffers), kept in
+ * the tb_ctx, and never frees caller memory.
+ *
+ * Precision forms (the `_f64` / `_f32` suffix):
+ *   _f64  "plain": every array is double. Drop-in for `gpu_preserve` data.
+ *   _f32  "mixed": every array is float EXCEPT the deformation gradient F,
+ *         which stays double; weights, P2G and G2P run in FP32, the P2G tile
+ *         uses compensated (two-term) sums, and F update, det F and log J run in
+ *         FP64. Drop-in for `gpu` (Float32-cast) data plus an FP64 F array.
+ *
+ * Index conventions follow the reference (Julia, column-major, 1-based):
+ *   block ids are 1-based linear ids over nblocks(mesh), 0 = outside the mesh
+ *     (Tesserae.jl src/Parallel/gpu_block_strategy.jl:46-53);
+ *   particleindices hold 1-based particle ids, block-contiguous, ascending
+ *     block id then ascending particle id (the reference CPU strategy's order,
+ *     src/Parallel/cpu_block_strategy.jl:174-190; its GPU strategy leaves the
+ *     order inside a block unspecified, gpu_block_strategy.jl:133-140);
+ *   offsets are 0-based exclusive prefix sums of counts, length nblocks+1.
+ *
+ * Tensor components are column-major: 3D grad_v/F/B = (11,21,31,12,22,32,13,23,33),
+ * 2D = (11,21,12,22). Symmetric sigma = (11,21,31,22,32,33) in 3D, (11,21,22) in 2D
+ * (Tensorial.jl SymmetricSecondOrderTensor independent-component order).
+ */
+#ifndef TESSERAE_B200_H
+#define TESSERAE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TB_OK 0
+#define TB_ERR_ARG (-1)         /* invalid argument (null pointer, bad size, bad enum) */
+#define TB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define TB_ERR_CAPACITY (-3)    /* a size exceeds the Int32 capacity of the partition */
+#define TB_ERR_UNSUPPORTED (-4) /* combination not supported (e.g. dim 1) */
+#define TB_ERR_DEVICE (-5)      /* a kernel reported an error status (e.g. bounded wait expired) */
+
+/* Uniform Cartesian mesh (reference: src/Mesh/cartesian.jl:38-102).
+ * xmin, h and h_inv are given in FP64 exactly as the caller's mesh stores them;
+ * the _f32 entry points cast each to float (src/adapt.jl:53-57: Float32(h_inv),
+ * not inv(Float32(h))), so block ids match the Float32 reference bit for bit. */
+typedef struct tb_mesh {
+    int32_t dim;          /* 2 or 3 */
+    int32_t block_log2;   /* cells per block edge = 1 << block_log2 (reference default 2) */
+    int64_t n_nodes[3];   /* nodes per axis (cells + 1); unused axes = 1 */
+    double xmin[3];       /* first node coordinate per axis */
+    double h;             /* spacing */
+    double h_inv;         /* stored inverse spacing */
+} tb_mesh;
+
+/* Basis kinds on the hot path (src/Basis/bspline.jl, gimp.jl, wls.jl). */
+enum tb_basis_kind {
+    TB_BSPLINE_QUADRATIC = 0,     /* BSpline(Quadratic()) */
+    TB_UGIMP = 1,                 /* uGIMP() */
+    TB_WLS_BSPLINE_QUADRATIC = 2, /* WLS(BSpline(Quadratic())), MLS-MPM */
+    TB_WLS_UGIMP = 3              /* WLS(uGIMP()) */
+};
+
+/* Transfer schemes of the recognised @P2G/@G2P equation sets. */
+enum tb_transfer_kind {
+    TB_TRANSFER_FLIP = 0, /* README.md:71-87: v += sum w (v_i - vn_i) (flip_alpha blends PIC) */
+    TB_TRANSFER_APIC = 1  /* docs/src/transfer.md:166-186: v = sum w v_i, B = sum w v_i (x) (x_i - x_p) */
+};
+
+/* Particle state as structure-of-arrays component pointers. Scalar type is T
+ * (double for _f64, float for _f32) except F, which is always double.
+ * Optional arrays may be NULL; the matching scalar in tb_step_params is used. */
+typedef struct tb_particles {
+    int64_t n;
+    void* x[3];       /* position (required) */
+    void* v[3];       /* velocity */
+    void* V;          /* current volume */
+    void* m;          /* optional per-particle mass */
+    void* l;          /* optional per-particle uGIMP length (absolute units) */
+    void* grad_v[9];  /* velocity gradient, column-major */
+    void* sigma[6];   /* symmetric Cauchy stress */
+    void* F[9];       /* deformation gradient, column-major, ALWAYS double */
+    void* B[9];       /* APIC affine matrix, column-major (TB_TRANSFER_APIC only) */
+    void* V0;         /* optional per-particle initial volume */
+    void* mu;         /* optional per-particle Lame mu */
+    void* lambda;     /* optional per-particle Lame lambda */
+} tb_particles;
+
+/* Grid fields as SoA component pointers (scalar type T), each of length
+ * prod(n_nodes), column-major node order (src/Grids/grid.jl:70-78). */
+typedef struct tb_grid {
+    void* m;
+    void* mv[3];
+    void* f[3];
+    void* v[3];
+    void* vn[3];
+} tb_grid;
+
+/* The GPUBlockStrategy arrays (src/Parallel/gpu_block_strategy.jl:10-22). */
+typedef struct tb_partition {
+    int32_t* blockids;        /* [n] */
+    int32_t* counts;          /* [nblocks] */
+    int32_t* offsets;         /* [nblocks + 1] */
+    int32_t* blocklist;       /* [nblocks] non-empty block ids ascending; first nactive valid */
+    int32_t* particleindices; /* [n] 1-based; first nassigned valid */
+    int64_t nblocks;          /* prod(nblocks(mesh)), checked against the mesh */
+} tb_partition;
+
+/* Stored basis weights, the BasisWeightArray layout of the reference
+ * (src/Basis/basis_weight.jl:345-358,413-432): w is Array{T,4}(3,3,3,n) (2D:
+ * (3,3,n)), grad_w is Array{Vec{dim,T}}(3,3,3,n) (AoS, dim per node), window is
+ * the CartesianIndices{dim} per particle as (start_1, stop_1, start_2, stop_2, ...)
+ * 1-based inclusive Int64 (an empty window is start = 1, stop = 0). Values at
+ * local slots outside a truncated window are left as zero. */
+typedef struct tb_weights {
+    void* w;
+    void* grad_w;
+    int64_t* window;
+} tb_weights;
+
+/* Scalars of the recognised step (README.md:71-87, docs/src/gpu.md:296-331). */
+typedef struct tb_step_params {
+    double dt;
+    double mass;        /* per-particle mass when particles.m == NULL */
+    double V0;          /* initial volume when particles.V0 == NULL */
+    double mu;          /* Lame mu when particles.mu == NULL */
+    double lambda;      /* Lame lambda when particles.lambda == NULL */
+    double gravity[3];  /* body acceleration added to f as w m g */
+    double gimp_l;      /* uGIMP particle length when particles.l == NULL */
+    double flip_alpha;  /* FLIP blend: v_p = sum w ((1-a) v_i + a (v_p + v_i - vn_i)); 1 = README FLIP */
+    int32_t basis;      /* enum tb_basis_kind */
+    int32_t transfer;   /* enum tb_transfer_kind */
+    int32_t material;   /* 0 = Neo-Hookean (README.md:85), 1 = weakly compressible fluid p = -K(J-1) with K = lambda */
+    int32_t wall_mask;  /* slip walls: bit 2d = low face of axis d, bit 2d+1 = high face */
+    int32_t wall_layers;/* node layers next to each walled face whose normal velocity is zeroed */
+    int32_t reserved;
+} tb_step_params;
+
+typedef struct tb_ctx tb_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context bound to `device` and `stream` (a cudaStream_t, NULL = the
+ * legacy default stream). One context per stream; a context is not re-entrant. */
+tb_ctx* tb_create(int32_t device, void* stream);
+void tb_destroy(tb_ctx* ctx);
+const char* tb_last_error(const tb_ctx* ctx);
+int32_t tb_set_stream(tb_ctx* ctx, void* stream);
+int32_t tb_synchronize(tb_ctx* ctx);
+/* Number of this library's kernel launches issued through ctx so far. */
+int64_t tb_launch_count(const tb_ctx* ctx);
+
+/* ---- basis weights: update!(weights, particles, mesh) -----------------
+ * reference: src/Basis/basis_weight.jl:714-752 (GPU kernel :686-689). */
+int32_t tb_update_weights_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                              const tb_step_params* params, tb_weights* weights);
+int32_t tb_update_weights_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                              const tb_step_params* params, tb_weights* weights);
+
+/* ---- binning: update!(partition::GPUBlockStrategy, particles.x) ---------
+ * reference: src/Parallel/gpu_block_strategy.jl:142-166. Synchronises the
+ * stream once and returns the totals (the reference's one readback, :161-164). */
+int32_t tb_bin_particles_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                             tb_partition* partition, int64_t* nactive, int64_t* nassigned);
+int32_t tb_bin_particles_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                             tb_partition* partition, int64_t* nactive, int64_t* nassigned);
+
+/* ---- @P2G scatter half: m, mv, f (assigned targets are zeroed first) ----
+ * reference: src/Transfer/gpu.jl:196-223 (block-scheduled) with the sums of
+ * README.md:72-74 plus gravity f += w m g (test/transfer.jl:96). Requires a
+ * partition from tb_bin_particles_* for the same positions. Asynchronous. */
+int32_t tb_p2g_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                   const tb_partition* partition, tb_grid* grid, const tb_step_params* params);
+int32_t tb_p2g_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                   const tb_partition* partition, tb_grid* grid, const tb_step_params* params);
+
+/* ---- @P2G grid half: vn = mv/m, v = vn + dt f/m (guarded), slip walls ----
+ * reference: foreach_loop -> gpukernel_foreach (src/Transfer/foreach.jl:276-339),
+ * equations docs/src/gpu.md:309-316. Asynchronous. */
+int32_t tb_grid_update_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_grid* grid, const tb_step_params* params);
+int32_t tb_grid_update_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_grid* grid, const tb_step_params* params);
+
+/* ---- @G2P gather + particle update (FLIP or APIC, Neo-Hookean) ----------
+ * reference: src/Transfer/gpu.jl:226-232 with README.md:79-86. Asynchronous. */
+int32_t tb_g2p_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_grid* grid, tb_particles* particles,
+                   const tb_step_params* params);
+int32_t tb_g2p_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_grid* grid, tb_particles* particles,
+                   const tb_step_params* params);
+
+/* ---- fused step: bin -> P2G -> grid update -> G2P, `nsteps` times --------
+ * The canonical loop of README.md:66-87 / docs/src/gpu.md:296-331 on device
+ * data, with no host synchronisation between steps. */
+int32_t tb_step_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                    tb_grid* grid, const tb_step_params* params, int32_t nsteps);
+int32_t tb_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                    tb_grid* grid, const tb_step_params* params, int32_t nsteps);
+
+/* ---- host-buffer rollout (end-to-end form of tb_step_*) ----------------
+ * `host` holds HOST pointers (pinned memory recommended) for the particle state;
+ * the context stages it into its own device buffers, runs `nsteps` steps and
+ * copies the state back. Grid and partition live in context-owned device memory.
+ * Synchronous. This is the call a host program without device arrays makes. */
+int32_t tb_rollout_host_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
+                            const tb_step_params* params, int32_t nsteps);
+int32_t tb_rollout_host_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
+                            const tb_step_params* params, int32_t nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TESSERAE_B200_H */

@@ -1,0 +1,683 @@
+// tb_oracle.hpp -- CPU restatement of Tesserae.jl's explicit MPM step.
+//
+// TEST INFRASTRUCTURE ONLY. This header is the parity oracle for the CUDA
+// kernels of libtesserae_b200.so and the timed CPU baseline of bench.py. Only
+// tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs
+// load it. The product library never links it.
+//
+// It restates, templated on the dimension D and the state scalar T (F is
+// always double, as in the mixed FP32 form), the reference's algorithm:
+//   mesh / findblock / support windows   src/Mesh/cartesian.jl:146-285
+//   quadratic B-spline, fast and nodewise src/Basis/bspline.jl:28-184
+//   uGIMP                                 src/Basis/gimp.jl:16-40
+//   WLS (MLS-MPM)                         src/Basis/wls.jl:22-84, polynomials.jl:28-29
+//   stable block partition                src/Parallel/cpu_block_strategy.jl:62-190
+//   P2G / grid update / G2P               README.md:71-87, docs/src/gpu.md:296-331,
+//                                         test/transfer.jl:85-136
+//   APIC                                  docs/src/transfer.md:166-186
+//   colour-phased parallel scatter        src/Parallel/region.jl:212-256
+//
+// Parity of this restatement against the reference itself is pinned only by the
+// reference's known-answer tests and doctests (Julia is not available to run the
+// reference); see tests/golden/.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "../include/tesserae_b200.h"
+
+namespace tbo {
+
+// ---------------------------------------------------------------------------
+// mesh
+// ---------------------------------------------------------------------------
+
+template <int D, class T>
+struct Mesh {
+    int64_t n[3];
+    int64_t nb[3];
+    T xmin[3];
+    T h, h_inv;
+    double xmin64[3], h64;  // FP64 originals for node coordinates
+    int L;
+    int64_t nnodes, nblocks;
+};
+
+template <int D, class T>
+inline Mesh<D, T> make_mesh(const tb_mesh& m) {
+    Mesh<D, T> M{};
+    M.L = m.block_log2;
+    M.nnodes = 1;
+    M.nblocks = 1;
+    for (int d = 0; d < 3; ++d) {
+        M.n[d] = d < D ? m.n_nodes[d] : 1;
+        // nblocks: ((n - 1) >> L) + 1 (src/Mesh/cartesian.jl:241-242)
+        M.nb[d] = d < D ? ((M.n[d] - 1) >> M.L) + 1 : 1;
+        M.xmin[d] = T(m.xmin[d]);
+        M.xmin64[d] = m.xmin[d];
+        M.nnodes *= M.n[d];
+        M.nblocks *= M.nb[d];
+    }
+    // The Float32 form casts h and h_inv separately (src/adapt.jl:53-57).
+    M.h = T(m.h);
+    M.h_inv = T(m.h_inv);
+    M.h64 = m.h;
+    return M;
+}
+
+// Node coordinate on axis d, as the scalar type of the mesh axes. The reference
+// stores axes as Vector{T}(range(xmin; step=h, length=n)) (cartesian.jl:86-101),
+// xmin + i*h evaluated in Julia's TwicePrecision and rounded once; here it is
+// xmin + i*h in FP64 (unfused), which agrees exactly when h is a power of two and
+// to one ulp otherwise. The CUDA kernels use the same FP64 expression.
+template <int D, class T>
+inline T node_coord(const Mesh<D, T>& M, int d, int64_t i) {
+    double x = M.xmin64[d] + double(i) * M.h64;
+    return T(x);
+}
+
+template <int D>
+inline int64_t node_linear(const int64_t* n, const int64_t* idx) {
+    int64_t lin = idx[D - 1];
+    for (int d = D - 2; d >= 0; --d) lin = lin * n[d] + idx[d];
+    return lin;
+}
+
+// findblock: 1-based linear block id, 0 when outside (src/Mesh/cartesian.jl:271-285,
+// gpu_block_strategy.jl:46-53 sub2ind). cell0 = trunc(floor((x - xmin) * h_inv)),
+// inside iff 0 <= cell0 <= n - 2 on every axis.
+template <int D, class T>
+inline int32_t findblock(const Mesh<D, T>& M, const T* x) {
+    int64_t b[3] = {0, 0, 0};
+    for (int d = 0; d < D; ++d) {
+        T c = std::floor((x[d] - M.xmin[d]) * M.h_inv);
+        if (!(c >= T(0) && c <= T(M.n[d] - 2))) return 0;
+        b[d] = int64_t(c) >> M.L;
+    }
+    int64_t lin = b[D - 1];
+    for (int d = D - 2; d >= 0; --d) lin = lin * M.nb[d] + b[d];
+    return int32_t(lin + 1);
+}
+
+// ---------------------------------------------------------------------------
+// basis
+// ---------------------------------------------------------------------------
+
+constexpr int NW3 = 27;
+
+template <int D>
+constexpr int nwin() { return D == 3 ? 27 : 9; }
+
+template <int D, class T>
+struct Weights {
+    int64_t lo[3];   // 0-based first node per axis
+    int64_t cnt[3];  // nodes per axis (0 = empty window)
+    bool empty;
+    T w[27];         // local slot s = i + 3 j + 9 k (column-major 3^D storage)
+    T dw[27][3];
+};
+
+// 1-D jet of BSpline(Quadratic()) (src/Basis/bspline.jl:180-184, derivative by
+// forward-mode AD through abs()). Known answer: jet(0) = (0.75, 0.0) (test/basis.jl:311).
+template <class T>
+inline void jet_bspline_quadratic(T xi, T& val, T& der) {
+    T s = std::signbit(xi) ? T(-1) : T(1);
+    T a = std::fabs(xi);
+    if (a < T(0.5)) {
+        val = (T(3) - T(4) * (a * a)) / T(4);
+        der = -(T(2) * a) * s;
+    } else if (a < T(1.5)) {
+        T t = T(3) - T(2) * a;
+        val = (t * t) / T(8);
+        der = -(t / T(2)) * s;
+    } else {
+        val = T(0);
+        der = T(0);
+    }
+}
+
+// 1-D jet of uGIMP with l normalised by h (src/Basis/gimp.jl:28-33).
+template <class T>
+inline void jet_ugimp(T xi, T l, T& val, T& der) {
+    T s = std::signbit(xi) ? T(-1) : T(1);
+    T a = std::fabs(xi);
+    if (a < l / T(2)) {
+        val = T(1) - (T(4) * (a * a) + l * l) / (T(4) * l);
+        der = -(T(2) * a / l) * s;
+    } else if (a < T(1) - l / T(2)) {
+        val = T(1) - a;
+        der = -s;
+    } else if (a < T(1) + l / T(2)) {
+        T t = T(1) + l / T(2) - a;
+        val = (t * t) / (T(2) * l);
+        der = -(t / l) * s;
+    } else {
+        val = T(0);
+        der = T(0);
+    }
+}
+
+// Normalised coordinate and the inside test of supportnodes (cartesian.jl:157-163,
+// 227-234: floor(xi) in [0, n-2] on every axis).
+template <int D, class T>
+inline bool normalize_inside(const Mesh<D, T>& M, const T* x, T* xi) {
+    bool inside = true;
+    for (int d = 0; d < D; ++d) {
+        xi[d] = (x[d] - M.xmin[d]) * M.h_inv;
+        T c = std::floor(xi[d]);
+        inside = inside && (c >= T(0) && c <= T(M.n[d] - 2));
+    }
+    return inside;
+}
+
+// Quadratic B-spline window: start = trunc(floor(xi - 1/2)) + 1 (1-based), width 3,
+// clipped to the mesh (src/Basis/bspline.jl:28-40).
+template <int D, class T>
+inline void window_bspline_quadratic(const Mesh<D, T>& M, const T* xi, Weights<D, T>& W) {
+    for (int d = 0; d < 3; ++d) { W.lo[d] = 0; W.cnt[d] = 1; }
+    for (int d = 0; d < D; ++d) {
+        int64_t s = int64_t(std::floor(xi[d] - T(1) / T(2)));
+        int64_t e = s + 2;
+        int64_t lo = std::max<int64_t>(s, 0), hi = std::min<int64_t>(e, M.n[d] - 1);
+        W.lo[d] = lo;
+        W.cnt[d] = hi - lo + 1;
+    }
+}
+
+// uGIMP window: supportnodes(x, 1 + l/2, mesh), start = trunc(floor(xi - r)) + 2,
+// stop = trunc(floor(xi + r)) + 1 (1-based) (src/Mesh/cartesian.jl:190-199, gimp.jl:20-24).
+template <int D, class T>
+inline void window_ugimp(const Mesh<D, T>& M, const T* xi, T lnorm, Weights<D, T>& W) {
+    T r = T(1) + lnorm / T(2);
+    for (int d = 0; d < 3; ++d) { W.lo[d] = 0; W.cnt[d] = 1; }
+    for (int d = 0; d < D; ++d) {
+        int64_t s = int64_t(std::floor(xi[d] - r)) + 1;
+        int64_t e = int64_t(std::floor(xi[d] + r));
+        int64_t lo = std::max<int64_t>(s, 0), hi = std::min<int64_t>(e, M.n[d] - 1);
+        W.lo[d] = lo;
+        W.cnt[d] = hi - lo + 1;
+    }
+}
+
+template <int D, class T>
+inline void zero_weights(Weights<D, T>& W) {
+    for (int s = 0; s < 27; ++s) {
+        W.w[s] = T(0);
+        W.dw[s][0] = W.dw[s][1] = W.dw[s][2] = T(0);
+    }
+}
+
+// Separable nodewise jet at every window node (basis_weight.jl:49-60, 625-632):
+// xi_d = (x_d - X_d(i)) h_inv, w = prod vals, grad_d = (prod with der on axis d) * h_inv.
+template <int D, class T, class Jet>
+inline void nodewise_values(const Mesh<D, T>& M, const T* x, Weights<D, T>& W, Jet jet) {
+    for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+        for (int j = 0; j < W.cnt[1]; ++j)
+            for (int i = 0; i < W.cnt[0]; ++i) {
+                int64_t node[3] = {W.lo[0] + i, W.lo[1] + j, W.lo[2] + k};
+                int loc[3] = {i, j, k};
+                T val[3], der[3];
+                for (int d = 0; d < D; ++d) {
+                    T xid = (x[d] - node_coord(M, d, node[d])) * M.h_inv;
+                    jet(xid, val[d], der[d]);
+                }
+                int s = loc[0] + 3 * loc[1] + (D == 3 ? 9 * loc[2] : 0);
+                T w = val[0];
+                for (int d = 1; d < D; ++d) w = w * val[d];
+                W.w[s] = w;
+                for (int g = 0; g < D; ++g) {
+                    T p = (g == 0 ? der[0] : val[0]);
+                    for (int d = 1; d < D; ++d) p = p * (g == d ? der[d] : val[d]);
+                    W.dw[s][g] = p * M.h_inv;
+                }
+            }
+}
+
+// Full-support fast path (bspline.jl:90-100, 146-170): t = fract(xi - 1/2),
+// node values by Horner on the generated coefficients
+//   N0 = 1/2 - t + t^2/2, N1 = 1/2 + t - t^2, N2 = t^2/2, N' = (-1 + t, 1 - 2t, t).
+template <class T>
+inline void bspline_quadratic_axis(T xi, T* v0, T* v1) {
+    T u = xi - T(0.5);
+    T t = u - std::floor(u);
+    const T half = T(1) / T(2);
+    v0[0] = half + t * (T(-1) + t * half);
+    v0[1] = half + t * (T(1) + t * T(-1));
+    v0[2] = T(0) + t * (T(0) + t * half);
+    v1[0] = T(-1) + t * T(1);
+    v1[1] = T(1) + t * T(-2);
+    v1[2] = T(0) + t * T(1);
+}
+
+template <int D, class T>
+inline void fast_values(const Mesh<D, T>& M, const T* xi, Weights<D, T>& W) {
+    T v0[3][3], v1[3][3];
+    for (int d = 0; d < D; ++d) bspline_quadratic_axis(xi[d], v0[d], v1[d]);
+    for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                int loc[3] = {i, j, k};
+                int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                T w = v0[0][i];
+                for (int d = 1; d < D; ++d) w = w * v0[d][loc[d]];
+                W.w[s] = w;
+                for (int g = 0; g < D; ++g) {
+                    T p = (g == 0 ? v1[0][i] : v0[0][i]);
+                    for (int d = 1; d < D; ++d) p = p * (g == d ? v1[d][loc[d]] : v0[d][loc[d]]);
+                    W.dw[s][g] = p * M.h_inv;
+                }
+            }
+}
+
+// Inverse of a small symmetric matrix by Gauss-Jordan with partial pivoting.
+template <class T, int N>
+inline bool invert(const T (&A)[N][N], T (&Ainv)[N][N]) {
+    T a[N][2 * N];
+    for (int r = 0; r < N; ++r)
+        for (int c = 0; c < 2 * N; ++c) a[r][c] = c < N ? A[r][c] : (c - N == r ? T(1) : T(0));
+    for (int c = 0; c < N; ++c) {
+        int p = c;
+        for (int r = c + 1; r < N; ++r)
+            if (std::fabs(a[r][c]) > std::fabs(a[p][c])) p = r;
+        if (a[p][c] == T(0)) return false;
+        if (p != c)
+            for (int k = 0; k < 2 * N; ++k) std::swap(a[p][k], a[c][k]);
+        T inv = T(1) / a[c][c];
+        for (int k = 0; k < 2 * N; ++k) a[c][k] *= inv;
+        for (int r = 0; r < N; ++r)
+            if (r != c) {
+                T f = a[r][c];
+                for (int k = 0; k < 2 * N; ++k) a[r][k] -= f * a[c][k];
+            }
+    }
+    for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) Ainv[r][c] = a[r][c + N];
+    return true;
+}
+
+// WLS correction (wls.jl:51-84): P = [1; X_i - x_p], wq = w M^-1 P,
+// w_wls = wq[0], grad w_wls = wq[1:D]. Full quadratic B-spline support uses the
+// closed form M^-1 = diag(1, 4/h^2 I) (wls.jl:29-49).
+template <int D, class T>
+inline void wls_correct(const Mesh<D, T>& M, const T* x, Weights<D, T>& W, bool closed_form) {
+    constexpr int N = D + 1;
+    T Minv[N][N];
+    for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) Minv[r][c] = T(0);
+    auto rel = [&](int s, int64_t* node, T* P) {
+        P[0] = T(1);
+        for (int d = 0; d < D; ++d) P[d + 1] = node_coord(M, d, node[d]) - x[d];
+    };
+    if (closed_form) {
+        Minv[0][0] = T(1);
+        T c = T(4) / (M.h * M.h);
+        for (int d = 1; d < N; ++d) Minv[d][d] = c;
+    } else {
+        T Mm[N][N];
+        for (int r = 0; r < N; ++r)
+            for (int c = 0; c < N; ++c) Mm[r][c] = T(0);
+        for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+            for (int j = 0; j < W.cnt[1]; ++j)
+                for (int i = 0; i < W.cnt[0]; ++i) {
+                    int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                    int64_t node[3] = {W.lo[0] + i, W.lo[1] + j, W.lo[2] + k};
+                    T P[N];
+                    rel(s, node, P);
+                    for (int r = 0; r < N; ++r)
+                        for (int c = 0; c < N; ++c) Mm[r][c] += W.w[s] * P[r] * P[c];
+                }
+        if (!invert<T, N>(Mm, Minv)) {
+            zero_weights(W);
+            return;
+        }
+    }
+    for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+        for (int j = 0; j < W.cnt[1]; ++j)
+            for (int i = 0; i < W.cnt[0]; ++i) {
+                int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                int64_t node[3] = {W.lo[0] + i, W.lo[1] + j, W.lo[2] + k};
+                T P[N];
+                rel(s, node, P);
+                T wq[N];
+                for (int r = 0; r < N; ++r) {
+                    T acc = T(0);
+                    for (int c = 0; c < N; ++c) acc += Minv[r][c] * P[c];
+                    wq[r] = W.w[s] * acc;
+                }
+                W.w[s] = wq[0];
+                for (int d = 0; d < D; ++d) W.dw[s][d] = wq[d + 1];
+            }
+}
+
+// update_basis_weight! for one particle (basis_weight.jl:638-642).
+template <int D, class T>
+inline void compute_weights(const Mesh<D, T>& M, int basis, const T* x, T l_abs, Weights<D, T>& W) {
+    zero_weights(W);
+    T xi[3] = {0, 0, 0};
+    bool inside = normalize_inside(M, x, xi);
+    if (!inside) {
+        W.empty = true;
+        for (int d = 0; d < 3; ++d) { W.lo[d] = 0; W.cnt[d] = 0; }
+        return;
+    }
+    W.empty = false;
+    bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    T lnorm = gimp ? l_abs / M.h : T(0);
+    if (gimp) window_ugimp(M, xi, lnorm, W);
+    else window_bspline_quadratic(M, xi, W);
+    bool full = true;
+    for (int d = 0; d < D; ++d) full = full && (W.cnt[d] == 3);
+    if (basis == TB_BSPLINE_QUADRATIC) {
+        if (full) fast_values(M, xi, W);
+        else nodewise_values(M, x, W, [](T a, T& v, T& g) { jet_bspline_quadratic(a, v, g); });
+    } else if (basis == TB_WLS_BSPLINE_QUADRATIC) {
+        nodewise_values(M, x, W, [](T a, T& v, T& g) { jet_bspline_quadratic(a, v, g); });
+        wls_correct(M, x, W, full);
+    } else {
+        nodewise_values(M, x, W, [lnorm](T a, T& v, T& g) { jet_ugimp(a, lnorm, v, g); });
+        if (basis == TB_WLS_UGIMP) wls_correct(M, x, W, false);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// particle / grid views
+// ---------------------------------------------------------------------------
+
+template <class T>
+inline T* P(void* p) { return static_cast<T*>(p); }
+template <class T>
+inline const T* CP(const void* p) { return static_cast<const T*>(p); }
+
+template <int D>
+constexpr int nsym() { return D == 3 ? 6 : 3; }
+template <int D>
+inline int symidx(int r, int c) {
+    if (r < c) std::swap(r, c);
+    return c * D - c * (c - 1) / 2 + (r - c);
+}
+
+// ---------------------------------------------------------------------------
+// partition (stable counting sort)
+// ---------------------------------------------------------------------------
+
+template <int D, class T>
+inline void bin(const Mesh<D, T>& M, const tb_particles& p, tb_partition& part, int64_t* nactive,
+                int64_t* nassigned) {
+    const int64_t n = p.n;
+    std::vector<int32_t> cursor(M.nblocks, 0);
+    std::fill(part.counts, part.counts + M.nblocks, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        T x[3] = {0, 0, 0};
+        for (int d = 0; d < D; ++d) x[d] = CP<T>(p.x[d])[i];
+        int32_t b = findblock(M, x);
+        part.blockids[i] = b;
+        if (b) part.counts[b - 1] += 1;
+    }
+    int64_t acc = 0, na = 0;
+    for (int64_t b = 0; b < M.nblocks; ++b) {
+        part.offsets[b] = int32_t(acc);
+        cursor[b] = int32_t(acc);
+        if (part.counts[b]) part.blocklist[na++] = int32_t(b + 1);
+        acc += part.counts[b];
+    }
+    part.offsets[M.nblocks] = int32_t(acc);
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t b = part.blockids[i];
+        if (b) part.particleindices[cursor[b - 1]++] = int32_t(i + 1);
+    }
+    *nactive = na;
+    *nassigned = acc;
+}
+
+// ---------------------------------------------------------------------------
+// P2G / grid update / G2P
+// ---------------------------------------------------------------------------
+
+template <class T>
+inline T opt(const void* arr, int64_t i, double dflt) {
+    return arr ? CP<T>(arr)[i] : T(dflt);
+}
+
+template <int D, class T>
+struct ParticleIn {
+    T x[3], v[3], V, m, l;
+    T sig[3][3];
+    T B[3][3];
+};
+
+template <int D, class T>
+inline void load_particle(const tb_particles& p, const tb_step_params& prm, int64_t i, ParticleIn<D, T>& q) {
+    for (int d = 0; d < 3; ++d) { q.x[d] = T(0); q.v[d] = T(0); }
+    for (int d = 0; d < D; ++d) {
+        q.x[d] = CP<T>(p.x[d])[i];
+        q.v[d] = CP<T>(p.v[d])[i];
+    }
+    q.V = CP<T>(p.V)[i];
+    q.m = opt<T>(p.m, i, prm.mass);
+    q.l = opt<T>(p.l, i, prm.gimp_l);
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) {
+            q.sig[r][c] = CP<T>(p.sigma[symidx<D>(r, c)])[i];
+            q.B[r][c] = (prm.transfer == TB_TRANSFER_APIC) ? CP<T>(p.B[r + c * D])[i] : T(0);
+        }
+}
+
+// Scatter of one particle into the grid fields (README.md:72-74, test/transfer.jl:96-97,
+// docs/src/transfer.md:176-178).
+template <int D, class T, class Acc>
+inline void p2g_particle(const Mesh<D, T>& M, const tb_step_params& prm, const ParticleIn<D, T>& q,
+                         T* gm, T* const* gmv, T* const* gf) {
+    Weights<D, T> W;
+    compute_weights(M, prm.basis, q.x, q.l, W);
+    if (W.empty) return;
+    const T dinv = T(4) / (M.h * M.h);  // D_p^-1 = inv(h^2/4 I) for the quadratic B-spline
+    for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+        for (int j = 0; j < W.cnt[1]; ++j)
+            for (int i = 0; i < W.cnt[0]; ++i) {
+                int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                int64_t node[3] = {W.lo[0] + i, W.lo[1] + j, W.lo[2] + k};
+                int64_t I = node_linear<D>(M.n, node);
+                T w = W.w[s];
+                T wm = w * q.m;
+                gm[I] += wm;
+                T vv[3];
+                for (int d = 0; d < D; ++d) vv[d] = q.v[d];
+                if (prm.transfer == TB_TRANSFER_APIC) {
+                    T dx[3];
+                    for (int d = 0; d < D; ++d) dx[d] = node_coord(M, d, node[d]) - q.x[d];
+                    for (int r = 0; r < D; ++r) {
+                        T a = T(0);
+                        for (int c = 0; c < D; ++c) a += q.B[r][c] * dinv * dx[c];
+                        vv[r] += a;
+                    }
+                }
+                for (int d = 0; d < D; ++d) gmv[d][I] += wm * vv[d];
+                for (int r = 0; r < D; ++r) {
+                    T a = T(0);
+                    for (int c = 0; c < D; ++c) a += (-q.V * q.sig[r][c]) * W.dw[s][c];
+                    gf[r][I] += a + wm * T(prm.gravity[r]);
+                }
+            }
+}
+
+template <int D, class T>
+inline void zero_p2g_targets(const Mesh<D, T>& M, tb_grid& g) {
+    std::fill(P<T>(g.m), P<T>(g.m) + M.nnodes, T(0));
+    for (int d = 0; d < D; ++d) {
+        std::fill(P<T>(g.mv[d]), P<T>(g.mv[d]) + M.nnodes, T(0));
+        std::fill(P<T>(g.f[d]), P<T>(g.f[d]) + M.nnodes, T(0));
+    }
+}
+
+template <int D, class T>
+inline void p2g(const Mesh<D, T>& M, const tb_particles& p, tb_grid& g, const tb_step_params& prm) {
+    zero_p2g_targets(M, g);
+    T* gmv[3] = {nullptr, nullptr, nullptr};
+    T* gf[3] = {nullptr, nullptr, nullptr};
+    for (int d = 0; d < D; ++d) { gmv[d] = P<T>(g.mv[d]); gf[d] = P<T>(g.f[d]); }
+    for (int64_t i = 0; i < p.n; ++i) {
+        ParticleIn<D, T> q;
+        load_particle<D, T>(p, prm, i, q);
+        p2g_particle<D, T, void>(M, prm, q, P<T>(g.m), gmv, gf);
+    }
+}
+
+// Grid half of @P2G (docs/src/gpu.md:309-310, guarded by !iszero(m)) and the
+// slip-wall slices (gpu.md:313-316).
+template <int D, class T>
+inline void grid_update_node(const Mesh<D, T>& M, tb_grid& g, const tb_step_params& prm, int64_t I) {
+    T m = P<T>(g.m)[I];
+    T dt = T(prm.dt);
+    for (int d = 0; d < D; ++d) {
+        T vn = T(0), v = T(0);
+        if (m != T(0)) {
+            vn = P<T>(g.mv[d])[I] / m;
+            v = vn + (dt * P<T>(g.f[d])[I]) / m;
+        }
+        P<T>(g.vn[d])[I] = vn;
+        P<T>(g.v[d])[I] = v;
+    }
+    if (prm.wall_mask) {
+        int64_t idx[3], r = I;
+        for (int d = 0; d < D; ++d) { idx[d] = r % M.n[d]; r /= M.n[d]; }
+        for (int d = 0; d < D; ++d) {
+            bool lo = (prm.wall_mask >> (2 * d)) & 1, hi = (prm.wall_mask >> (2 * d + 1)) & 1;
+            if ((lo && idx[d] < prm.wall_layers) || (hi && idx[d] >= M.n[d] - prm.wall_layers)) {
+                P<T>(g.vn[d])[I] = T(0);
+                P<T>(g.v[d])[I] = T(0);
+            }
+        }
+    }
+}
+
+template <int D, class T>
+inline void grid_update(const Mesh<D, T>& M, tb_grid& g, const tb_step_params& prm) {
+    for (int64_t I = 0; I < M.nnodes; ++I) grid_update_node(M, g, prm, I);
+}
+
+// One particle of @G2P (README.md:79-86, test/transfer.jl:112-136, transfer.md:180-184):
+// FLIP/PIC blend or APIC, then F = (I + dt grad v) F in FP64, J = det F,
+// Neo-Hookean sigma = (mu (F F^T - I) + lambda log J I) / J, V = V0 J.
+template <int D, class T>
+inline void g2p_particle(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p, const tb_step_params& prm,
+                         int64_t i) {
+    T x[3] = {0, 0, 0}, vp[3] = {0, 0, 0};
+    for (int d = 0; d < D; ++d) { x[d] = P<T>(p.x[d])[i]; vp[d] = P<T>(p.v[d])[i]; }
+    T l = opt<T>(p.l, i, prm.gimp_l);
+    Weights<D, T> W;
+    compute_weights(M, prm.basis, x, l, W);
+    T vpic[3] = {0, 0, 0}, dvflip[3] = {0, 0, 0}, gv[3][3] = {}, dx[3] = {0, 0, 0}, Bn[3][3] = {};
+    const T dt = T(prm.dt);
+    if (!W.empty) {
+        for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+            for (int j = 0; j < W.cnt[1]; ++j)
+                for (int ii = 0; ii < W.cnt[0]; ++ii) {
+                    int s = ii + 3 * j + (D == 3 ? 9 * k : 0);
+                    int64_t node[3] = {W.lo[0] + ii, W.lo[1] + j, W.lo[2] + k};
+                    int64_t I = node_linear<D>(M.n, node);
+                    T w = W.w[s];
+                    T vi[3], vni[3];
+                    for (int d = 0; d < D; ++d) {
+                        vi[d] = CP<T>(g.v[d])[I];
+                        vni[d] = CP<T>(g.vn[d])[I];
+                    }
+                    for (int d = 0; d < D; ++d) {
+                        vpic[d] += w * vi[d];
+                        dvflip[d] += w * (vi[d] - vni[d]);
+                        dx[d] += (w * vi[d]) * dt;
+                    }
+                    for (int r = 0; r < D; ++r)
+                        for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * W.dw[s][c];
+                    if (prm.transfer == TB_TRANSFER_APIC) {
+                        T rel[3];
+                        for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, node[d]) - x[d];
+                        for (int r = 0; r < D; ++r)
+                            for (int c = 0; c < D; ++c) Bn[r][c] += (w * vi[r]) * rel[c];
+                    }
+                }
+    }
+    if (prm.transfer == TB_TRANSFER_APIC) {
+        for (int d = 0; d < D; ++d) P<T>(p.v[d])[i] = vpic[d];
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) P<T>(p.B[r + c * D])[i] = Bn[r][c];
+    } else {
+        const T a = T(prm.flip_alpha);
+        for (int d = 0; d < D; ++d) {
+            T vflip = vp[d] + dvflip[d];
+            P<T>(p.v[d])[i] = (a == T(1)) ? vflip : (T(1) - a) * vpic[d] + a * vflip;
+        }
+    }
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) P<T>(p.grad_v[r + c * D])[i] = gv[r][c];
+    for (int d = 0; d < D; ++d) P<T>(p.x[d])[i] = x[d] + dx[d];
+
+    // FP64 kinematics and constitutive update.
+    double F[3][3], Fn[3][3];
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) F[r][c] = CP<double>(p.F[r + c * D])[i];
+    const double dtd = prm.dt;
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) {
+            double a = 0.0;
+            for (int k = 0; k < D; ++k) {
+                double Ark = (r == k ? 1.0 : 0.0) + double(gv[r][k]) * dtd;
+                a += Ark * F[k][c];
+            }
+            Fn[r][c] = a;
+        }
+    double J;
+    if (D == 3)
+        J = Fn[0][0] * (Fn[1][1] * Fn[2][2] - Fn[1][2] * Fn[2][1]) -
+            Fn[0][1] * (Fn[1][0] * Fn[2][2] - Fn[1][2] * Fn[2][0]) +
+            Fn[0][2] * (Fn[1][0] * Fn[2][1] - Fn[1][1] * Fn[2][0]);
+    else
+        J = Fn[0][0] * Fn[1][1] - Fn[0][1] * Fn[1][0];
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) P<double>(p.F[r + c * D])[i] = Fn[r][c];
+    const double mu = p.mu ? double(CP<T>(p.mu)[i]) : prm.mu;
+    const double lam = p.lambda ? double(CP<T>(p.lambda)[i]) : prm.lambda;
+    double sig[3][3] = {};
+    if (prm.material == 1) {
+        for (int d = 0; d < D; ++d) sig[d][d] = lam * (J - 1.0);
+    } else {
+        const double lj = std::log(J);
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double b = 0.0;
+                for (int k = 0; k < D; ++k) b += Fn[r][k] * Fn[c][k];
+                sig[r][c] = (mu * (b - (r == c ? 1.0 : 0.0)) + (r == c ? lam * lj : 0.0)) / J;
+            }
+    }
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c <= r; ++c) P<T>(p.sigma[symidx<D>(r, c)])[i] = T(sig[r][c]);
+    const double V0 = p.V0 ? double(CP<T>(p.V0)[i]) : prm.V0;
+    P<T>(p.V)[i] = T(V0 * J);
+}
+
+template <int D, class T>
+inline void g2p(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p, const tb_step_params& prm) {
+    for (int64_t i = 0; i < p.n; ++i) g2p_particle(M, g, p, prm, i);
+}
+
+// ---------------------------------------------------------------------------
+// colour-phased multithreaded step (src/Parallel/region.jl:212-256 with the
+// CPUBlockStrategy partition): blocks of one colour share no support node
+// because the block width (4 cells) exceeds the window reach, so the blocks of
+// a colour scatter in parallel without atomics.
+// ---------------------------------------------------------------------------
+
+template <int D, class T>
+inline int block_colour(const Mesh<D, T>& M, int64_t b0) {
+    int col = 0;
+    for (int d = 0; d < D; ++d) {
+        col |= int(b0 % M.nb[d] & 1) << d;
+        b0 /= M.nb[d];
+    }
+    return col;
+}
+
+}  // namespace tbo

@@ -1,0 +1,579 @@
+// tb_abi.cu -- the extern "C" boundary of libtesserae_b200.so (include/tesserae_b200.h).
+//
+// Argument checks mirror the reference's (Tesserae.jl src/Transfer/runtime.jl:177-229,
+// src/Parallel/gpu_block_strategy.jl:142-150): particle and block counts must fit
+// Int32, the support window must fit the block tile, only 2D/3D meshes. Errors are
+// returned as status codes with a message; no exception crosses the boundary.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "tb_launch.cuh"
+
+using namespace tb;
+
+struct tb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    long long launches = 0;
+    std::string error;
+    int* d_err = nullptr;            // device status word (ERR_* bits)
+    int* d_totals = nullptr;         // [2] nactive, nassigned
+    int* h_totals = nullptr;         // pinned mirror
+    // scratch (grow-only)
+    int* cursors = nullptr;
+    long long cursors_cap = 0;
+    int* perm_tmp = nullptr;
+    long long perm_tmp_cap = 0;
+    unsigned long long* partials = nullptr;
+    long long partials_cap = 0;
+    unsigned long long* sort_scratch = nullptr;
+    long long sort_scratch_cap = 0;
+    // context-owned state for tb_rollout_host_*
+    void* roll_buf = nullptr;
+    size_t roll_cap = 0;
+};
+
+namespace {
+
+int fail(tb_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->error = buf;
+    return code;
+}
+
+int cuda_fail(tb_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, TB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <class P>
+cudaError_t grow(P*& ptr, long long& cap, long long need) {
+    if (need <= cap) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&ptr, sizeof(P) * size_t(need > 0 ? need : 1));
+    if (e == cudaSuccess) cap = need;
+    return e;
+}
+
+int check_ctx(tb_ctx* c) {
+    if (!c) return TB_ERR_ARG;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    return TB_OK;
+}
+
+int check_mesh(tb_ctx* c, const tb_mesh* m) {
+    if (!m) return fail(c, TB_ERR_ARG, "mesh is NULL");
+    if (m->dim != 2 && m->dim != 3) return fail(c, TB_ERR_UNSUPPORTED, "mesh dim %d: only 2D and 3D are supported", m->dim);
+    const int bw = 1 << m->block_log2;
+    if (!((m->dim == 3 && m->block_log2 == 2) || (m->dim == 2 && (m->block_log2 == 2 || m->block_log2 == 3))))
+        return fail(c, TB_ERR_UNSUPPORTED, "block_size_log2 %d in %dD: supported are 2 (3D) and 2 or 3 (2D)",
+                    m->block_log2, m->dim);
+    long long nn = 1, nb = 1;
+    for (int d = 0; d < m->dim; ++d) {
+        if (m->n_nodes[d] < 2) return fail(c, TB_ERR_ARG, "mesh axis %d has %lld nodes (< 2)", d, (long long)m->n_nodes[d]);
+        nn *= m->n_nodes[d];
+        nb *= ((m->n_nodes[d] - 1) >> m->block_log2) + 1;
+    }
+    if (nb > 0x7fffffffll) return fail(c, TB_ERR_CAPACITY, "block count %lld exceeds Int32 capacity", nb);
+    if (!(m->h > 0) || !(m->h_inv > 0)) return fail(c, TB_ERR_ARG, "mesh spacing must be positive");
+    (void)bw;
+    (void)nn;
+    return TB_OK;
+}
+
+long long mesh_nblocks(const tb_mesh* m) {
+    long long nb = 1;
+    for (int d = 0; d < m->dim; ++d) nb *= ((m->n_nodes[d] - 1) >> m->block_log2) + 1;
+    return nb;
+}
+
+// The support of every hot-path basis is 3 nodes wide; the reference checks the
+// window against the block width (src/Transfer/runtime.jl:192-229).
+int check_params(tb_ctx* c, const tb_step_params* p) {
+    if (!p) return fail(c, TB_ERR_ARG, "params is NULL");
+    if (p->basis < TB_BSPLINE_QUADRATIC || p->basis > TB_WLS_UGIMP)
+        return fail(c, TB_ERR_ARG, "unknown basis kind %d", p->basis);
+    if (p->transfer != TB_TRANSFER_FLIP && p->transfer != TB_TRANSFER_APIC)
+        return fail(c, TB_ERR_ARG, "unknown transfer kind %d", p->transfer);
+    if (p->material != 0 && p->material != 1) return fail(c, TB_ERR_ARG, "unknown material %d", p->material);
+    return TB_OK;
+}
+
+template <class T>
+int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool apic, PView<T>& P) {
+    if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
+    if (p->n < 0 || p->n > 0x7fffffffll)
+        return fail(c, TB_ERR_CAPACITY, "particle count %lld exceeds the partition's Int32 capacity", (long long)p->n);
+    std::memset(&P, 0, sizeof P);
+    P.n = p->n;
+    for (int d = 0; d < dim; ++d) {
+        P.x[d] = static_cast<T*>(p->x[d]);
+        P.v[d] = static_cast<T*>(p->v[d]);
+        if (p->n && !P.x[d]) return fail(c, TB_ERR_ARG, "particles.x[%d] is NULL", d);
+        if (need_state && p->n && !P.v[d]) return fail(c, TB_ERR_ARG, "particles.v[%d] is NULL", d);
+    }
+    P.V = static_cast<T*>(p->V);
+    P.m = static_cast<const T*>(p->m);
+    P.l = static_cast<const T*>(p->l);
+    for (int k = 0; k < dim * dim; ++k) {
+        P.gv[k] = static_cast<T*>(p->grad_v[k]);
+        P.F[k] = static_cast<double*>(p->F[k]);
+        P.B[k] = static_cast<T*>(p->B[k]);
+        if (need_state && p->n && (!P.gv[k] || !P.F[k]))
+            return fail(c, TB_ERR_ARG, "particles.grad_v/F component %d is NULL", k);
+        if (apic && p->n && !P.B[k]) return fail(c, TB_ERR_ARG, "APIC transfer needs particles.B[%d]", k);
+    }
+    for (int k = 0; k < (dim == 3 ? 6 : 3); ++k) {
+        P.sig[k] = static_cast<T*>(p->sigma[k]);
+        if (need_state && p->n && !P.sig[k]) return fail(c, TB_ERR_ARG, "particles.sigma[%d] is NULL", k);
+    }
+    if (need_state && p->n && !P.V) return fail(c, TB_ERR_ARG, "particles.V is NULL");
+    P.V0 = static_cast<const T*>(p->V0);
+    P.mu = static_cast<const T*>(p->mu);
+    P.lam = static_cast<const T*>(p->lambda);
+    return TB_OK;
+}
+
+template <class T>
+int make_gview(tb_ctx* c, const tb_grid* g, int dim, GView<T>& G) {
+    if (!g) return fail(c, TB_ERR_ARG, "grid is NULL");
+    std::memset(&G, 0, sizeof G);
+    G.m = static_cast<T*>(g->m);
+    if (!G.m) return fail(c, TB_ERR_ARG, "grid.m is NULL");
+    for (int d = 0; d < dim; ++d) {
+        G.mv[d] = static_cast<T*>(g->mv[d]);
+        G.f[d] = static_cast<T*>(g->f[d]);
+        G.v[d] = static_cast<T*>(g->v[d]);
+        G.vn[d] = static_cast<T*>(g->vn[d]);
+        if (!G.mv[d] || !G.f[d] || !G.v[d] || !G.vn[d]) return fail(c, TB_ERR_ARG, "grid component %d is NULL", d);
+    }
+    return TB_OK;
+}
+
+int bin_buffers(tb_ctx* c, const tb_partition* part, long long n, long long nb, BinBuffers& B) {
+    if (!part) return fail(c, TB_ERR_ARG, "partition is NULL");
+    if (part->nblocks != nb)
+        return fail(c, TB_ERR_ARG, "partition.nblocks %lld does not match the mesh (%lld)", (long long)part->nblocks, nb);
+    if (!part->counts || !part->offsets || !part->blocklist || (n && (!part->blockids || !part->particleindices)))
+        return fail(c, TB_ERR_ARG, "partition array is NULL");
+    cudaError_t e;
+    if ((e = grow(c->cursors, c->cursors_cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc cursors");
+    if ((e = grow(c->perm_tmp, c->perm_tmp_cap, n)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc perm_tmp");
+    if ((e = grow(c->partials, c->partials_cap, scan_tiles(int(nb)))) != cudaSuccess)
+        return cuda_fail(c, e, "cudaMalloc partials");
+    if ((e = grow(c->sort_scratch, c->sort_scratch_cap, 2 * n)) != cudaSuccess)
+        return cuda_fail(c, e, "cudaMalloc sort scratch");
+    B.blockids = part->blockids;
+    B.counts = part->counts;
+    B.offsets = part->offsets;
+    B.blocklist = part->blocklist;
+    B.perm = part->particleindices;
+    B.cursors = c->cursors;
+    B.perm_tmp = c->perm_tmp;
+    B.partials = c->partials;
+    B.sort_scratch = c->sort_scratch;
+    B.totals = c->d_totals;
+    return TB_OK;
+}
+
+LaunchCfg cfg_of(tb_ctx* c) { return LaunchCfg{c->stream, c->num_sms, &c->launches, c->d_err}; }
+
+// Reads and clears the device status word (synchronises the stream).
+int check_device_status(tb_ctx* c) {
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device status readback");
+    if (h) {
+        cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+        std::string why;
+        if (h & ERR_TILE_RANGE) why += " support window outside its block tile;";
+        if (h & ERR_GIMP_LENGTH) why += " uGIMP requires 0 <= l <= spacing(mesh);";
+        if (h & ERR_WLS_SINGULAR) why += " singular WLS moment matrix;";
+        return fail(c, TB_ERR_DEVICE, "kernel reported:%s", why.c_str());
+    }
+    return TB_OK;
+}
+
+template <int D, class T, int BW>
+int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+             const tb_step_params* prm, int nsteps, bool do_bin, bool do_p2g, bool do_grid, bool do_g2p) {
+    auto M = make_dmesh<D, T>(*m);
+    auto S = make_scalars<T>(*prm);
+    PView<T> P;
+    GView<T> G;
+    int rc;
+    if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    BinBuffers B;
+    if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    const T* xs[3] = {P.x[0], P.x[1], D == 3 ? P.x[2] : P.x[1]};
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
+        if (do_bin) e = launch_bin<D, T>(M, xs, P.n, B, cfg);
+        if (e == cudaSuccess && do_p2g) e = launch_p2g<D, T, BW>(M, P, G, S, B, cfg);
+        if (e == cudaSuccess && do_grid) e = launch_grid_update<D, T>(M, G, S, cfg);
+        if (e == cudaSuccess && do_g2p) e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg);
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return TB_OK;
+}
+
+template <class T>
+int dispatch_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                  const tb_step_params* prm, int nsteps, bool b, bool p2g, bool gr, bool g2p) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    if ((rc = check_params(c, prm)) != TB_OK) return rc;
+    if (nsteps < 0) return fail(c, TB_ERR_ARG, "nsteps must be >= 0");
+    if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
+    if (m->block_log2 == 3) return run_step<2, T, 8>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
+    return run_step<2, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
+}
+
+template <class T>
+int do_bin_only(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part, int64_t* nactive,
+                int64_t* nassigned) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    PView<T> P;
+    if ((rc = make_pview<T>(c, p, m->dim, false, false, P)) != TB_OK) return rc;
+    BinBuffers B;
+    if ((rc = bin_buffers(c, part, P.n, mesh_nblocks(m), B)) != TB_OK) return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    const T* xs[3] = {P.x[0], P.x[1], m->dim == 3 ? P.x[2] : P.x[1]};
+    cudaError_t e = (m->dim == 3) ? launch_bin<3, T>(make_dmesh<3, T>(*m), xs, P.n, B, cfg)
+                                  : launch_bin<2, T>(make_dmesh<2, T>(*m), xs, P.n, B, cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "binning launch");
+    e = cudaMemcpyAsync(c->h_totals, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "binning totals readback");
+    if (nactive) *nactive = c->h_totals[0];
+    if (nassigned) *nassigned = c->h_totals[1];
+    return TB_OK;
+}
+
+template <class T>
+int do_weights(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step_params* prm, tb_weights* w) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    if ((rc = check_params(c, prm)) != TB_OK) return rc;
+    if (!w || (p && p->n && (!w->w || !w->grad_w || !w->window))) return fail(c, TB_ERR_ARG, "weights array is NULL");
+    PView<T> P;
+    if ((rc = make_pview<T>(c, p, m->dim, false, false, P)) != TB_OK) return rc;
+    auto S = make_scalars<T>(*prm);
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e;
+    if (m->dim == 3)
+        e = launch_update_weights<3, T>(make_dmesh<3, T>(*m), P, S, static_cast<T*>(w->w), static_cast<T*>(w->grad_w),
+                                        reinterpret_cast<long long*>(w->window), cfg);
+    else
+        e = launch_update_weights<2, T>(make_dmesh<2, T>(*m), P, S, static_cast<T*>(w->w), static_cast<T*>(w->grad_w),
+                                        reinterpret_cast<long long*>(w->window), cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "update_weights launch");
+    return TB_OK;
+}
+
+template <class T>
+int do_g2p_direct(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p, const tb_step_params* prm) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
+        return rc;
+    PView<T> P;
+    GView<T> G;
+    if ((rc = make_pview<T>(c, p, m->dim, true, prm->transfer == TB_TRANSFER_APIC, P)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, m->dim, G)) != TB_OK) return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e = (m->dim == 3) ? launch_g2p_direct<3, T>(make_dmesh<3, T>(*m), G, P, make_scalars<T>(*prm), cfg)
+                                  : launch_g2p_direct<2, T>(make_dmesh<2, T>(*m), G, P, make_scalars<T>(*prm), cfg);
+    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "g2p launch");
+}
+
+// Host-buffer rollout: stage the particle state into a context-owned device
+// block, run the steps on a context-owned grid and partition, copy back.
+template <class T>
+int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm, int nsteps) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    if ((rc = check_params(c, prm)) != TB_OK) return rc;
+    if (!host) return fail(c, TB_ERR_ARG, "particles is NULL");
+    const int D = m->dim;
+    const long long n = host->n;
+    if (n < 0 || n > 0x7fffffffll) return fail(c, TB_ERR_CAPACITY, "particle count exceeds Int32 capacity");
+    const bool apic = prm->transfer == TB_TRANSFER_APIC;
+    long long nn = 1;
+    for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
+    const long long nb = mesh_nblocks(m);
+    // Fields moved: x, v, V, grad_v, sigma (T); F (double); optional m, l, B, V0, mu, lambda (T).
+    struct Field {
+        void** host_slot;
+        size_t elem;
+        bool inout;
+    };
+    std::vector<Field> fields;
+    auto add = [&](void** slot, size_t elem, bool inout) {
+        if (*slot) fields.push_back({slot, elem, inout});
+    };
+    for (int d = 0; d < D; ++d) add(&host->x[d], sizeof(T), true);
+    for (int d = 0; d < D; ++d) add(&host->v[d], sizeof(T), true);
+    add(&host->V, sizeof(T), true);
+    for (int k = 0; k < D * D; ++k) add(&host->grad_v[k], sizeof(T), true);
+    for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&host->sigma[k], sizeof(T), true);
+    for (int k = 0; k < D * D; ++k) add(&host->F[k], sizeof(double), true);
+    if (apic)
+        for (int k = 0; k < D * D; ++k) add(&host->B[k], sizeof(T), true);
+    add(&host->m, sizeof(T), false);
+    add(&host->l, sizeof(T), false);
+    add(&host->V0, sizeof(T), false);
+    add(&host->mu, sizeof(T), false);
+    add(&host->lambda, sizeof(T), false);
+    auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+    size_t bytes = 0;
+    for (auto& f : fields) bytes += align(f.elem * size_t(n));
+    const size_t grid_bytes = align(sizeof(T) * size_t(nn)) * size_t(1 + 4 * D);
+    const size_t part_bytes = align(sizeof(int) * size_t(n)) * 2 + align(sizeof(int) * size_t(nb)) * 2 +
+                              align(sizeof(int) * size_t(nb + 1));
+    const size_t total = bytes + grid_bytes + part_bytes;
+    if (total > c->roll_cap) {
+        if (c->roll_buf) cudaFree(c->roll_buf);
+        c->roll_buf = nullptr;
+        c->roll_cap = 0;
+        cudaError_t e = cudaMalloc(&c->roll_buf, total);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc rollout state");
+        c->roll_cap = total;
+        e = cudaMemsetAsync(c->roll_buf, 0, total, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemsetAsync rollout state");
+    }
+    char* base = static_cast<char*>(c->roll_buf);
+    tb_particles dev = *host;
+    size_t off = 0;
+    std::vector<void*> dptr(fields.size());
+    for (size_t i = 0; i < fields.size(); ++i) {
+        dptr[i] = base + off;
+        off += align(fields[i].elem * size_t(n));
+    }
+    // device particle struct mirrors host with device pointers
+    {
+        size_t i = 0;
+        auto remap = [&](void** hs) {
+            for (size_t k = 0; k < fields.size(); ++k)
+                if (fields[k].host_slot == hs) return dptr[k];
+            return (void*)nullptr;
+        };
+        for (int d = 0; d < D; ++d) dev.x[d] = remap(&host->x[d]);
+        for (int d = 0; d < D; ++d) dev.v[d] = remap(&host->v[d]);
+        dev.V = remap(&host->V);
+        for (int k = 0; k < D * D; ++k) dev.grad_v[k] = remap(&host->grad_v[k]);
+        for (int k = 0; k < (D == 3 ? 6 : 3); ++k) dev.sigma[k] = remap(&host->sigma[k]);
+        for (int k = 0; k < D * D; ++k) dev.F[k] = remap(&host->F[k]);
+        for (int k = 0; k < D * D; ++k) dev.B[k] = apic ? remap(&host->B[k]) : nullptr;
+        dev.m = remap(&host->m);
+        dev.l = remap(&host->l);
+        dev.V0 = remap(&host->V0);
+        dev.mu = remap(&host->mu);
+        dev.lambda = remap(&host->lambda);
+        (void)i;
+    }
+    tb_grid g{};
+    g.m = base + off;
+    off += align(sizeof(T) * size_t(nn));
+    for (int d = 0; d < D; ++d) {
+        g.mv[d] = base + off;
+        off += align(sizeof(T) * size_t(nn));
+        g.f[d] = base + off;
+        off += align(sizeof(T) * size_t(nn));
+        g.v[d] = base + off;
+        off += align(sizeof(T) * size_t(nn));
+        g.vn[d] = base + off;
+        off += align(sizeof(T) * size_t(nn));
+    }
+    tb_partition part{};
+    part.blockids = reinterpret_cast<int32_t*>(base + off);
+    off += align(sizeof(int) * size_t(n));
+    part.particleindices = reinterpret_cast<int32_t*>(base + off);
+    off += align(sizeof(int) * size_t(n));
+    part.counts = reinterpret_cast<int32_t*>(base + off);
+    off += align(sizeof(int) * size_t(nb));
+    part.blocklist = reinterpret_cast<int32_t*>(base + off);
+    off += align(sizeof(int) * size_t(nb));
+    part.offsets = reinterpret_cast<int32_t*>(base + off);
+    part.nblocks = nb;
+    cudaError_t e = cudaSuccess;
+    for (size_t i = 0; i < fields.size() && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(dptr[i], *fields[i].host_slot, fields[i].elem * size_t(n), cudaMemcpyHostToDevice,
+                            c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "rollout H2D");
+    rc = dispatch_step<T>(c, m, &dev, &part, &g, prm, nsteps, true, true, true, true);
+    if (rc != TB_OK) return rc;
+    for (size_t i = 0; i < fields.size() && e == cudaSuccess; ++i)
+        if (fields[i].inout)
+            e = cudaMemcpyAsync(*fields[i].host_slot, dptr[i], fields[i].elem * size_t(n), cudaMemcpyDeviceToHost,
+                                c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "rollout D2H");
+    return check_device_status(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+tb_ctx* tb_create(int32_t device, void* stream) {
+    tb_ctx* c = new (std::nothrow) tb_ctx();
+    if (!c) return nullptr;
+    c->device = device;
+    c->stream = static_cast<cudaStream_t>(stream);
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_totals, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&c->h_totals, 2 * sizeof(int)) != cudaSuccess) {
+        tb_destroy(c);
+        return nullptr;
+    }
+    cudaMemset(c->d_err, 0, sizeof(int));
+    cudaMemset(c->d_totals, 0, 2 * sizeof(int));
+    return c;
+}
+
+void tb_destroy(tb_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_err);
+    cudaFree(c->d_totals);
+    if (c->h_totals) cudaFreeHost(c->h_totals);
+    cudaFree(c->cursors);
+    cudaFree(c->perm_tmp);
+    cudaFree(c->partials);
+    cudaFree(c->sort_scratch);
+    cudaFree(c->roll_buf);
+    delete c;
+}
+
+const char* tb_last_error(const tb_ctx* c) { return c ? c->error.c_str() : "null context"; }
+
+int32_t tb_set_stream(tb_ctx* c, void* stream) {
+    if (!c) return TB_ERR_ARG;
+    c->stream = static_cast<cudaStream_t>(stream);
+    return TB_OK;
+}
+
+int32_t tb_synchronize(tb_ctx* c) {
+    int rc = check_ctx(c);
+    if (rc != TB_OK) return rc;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamSynchronize");
+    return check_device_status(c);
+}
+
+int64_t tb_launch_count(const tb_ctx* c) { return c ? c->launches : 0; }
+
+int32_t tb_update_weights_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step_params* prm,
+                              tb_weights* w) {
+    return do_weights<double>(c, m, p, prm, w);
+}
+int32_t tb_update_weights_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step_params* prm,
+                              tb_weights* w) {
+    return do_weights<float>(c, m, p, prm, w);
+}
+
+int32_t tb_bin_particles_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part,
+                             int64_t* nactive, int64_t* nassigned) {
+    return do_bin_only<double>(c, m, p, part, nactive, nassigned);
+}
+int32_t tb_bin_particles_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part,
+                             int64_t* nactive, int64_t* nassigned) {
+    return do_bin_only<float>(c, m, p, part, nactive, nassigned);
+}
+
+int32_t tb_p2g_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_partition* part, tb_grid* g,
+                   const tb_step_params* prm) {
+    return dispatch_step<double>(c, m, const_cast<tb_particles*>(p), const_cast<tb_partition*>(part), g, prm, 1,
+                                 false, true, false, false);
+}
+int32_t tb_p2g_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_partition* part, tb_grid* g,
+                   const tb_step_params* prm) {
+    return dispatch_step<float>(c, m, const_cast<tb_particles*>(p), const_cast<tb_partition*>(part), g, prm, 1,
+                                false, true, false, false);
+}
+
+int32_t tb_grid_update_f64(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params* prm) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
+        return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e;
+    if (m->dim == 3) {
+        GView<double> G;
+        if ((rc = make_gview<double>(c, g, 3, G)) != TB_OK) return rc;
+        e = launch_grid_update<3, double>(make_dmesh<3, double>(*m), G, make_scalars<double>(*prm), cfg);
+    } else {
+        GView<double> G;
+        if ((rc = make_gview<double>(c, g, 2, G)) != TB_OK) return rc;
+        e = launch_grid_update<2, double>(make_dmesh<2, double>(*m), G, make_scalars<double>(*prm), cfg);
+    }
+    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "grid update launch");
+}
+int32_t tb_grid_update_f32(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params* prm) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
+        return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e;
+    if (m->dim == 3) {
+        GView<float> G;
+        if ((rc = make_gview<float>(c, g, 3, G)) != TB_OK) return rc;
+        e = launch_grid_update<3, float>(make_dmesh<3, float>(*m), G, make_scalars<float>(*prm), cfg);
+    } else {
+        GView<float> G;
+        if ((rc = make_gview<float>(c, g, 2, G)) != TB_OK) return rc;
+        e = launch_grid_update<2, float>(make_dmesh<2, float>(*m), G, make_scalars<float>(*prm), cfg);
+    }
+    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "grid update launch");
+}
+
+int32_t tb_g2p_f64(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p, const tb_step_params* prm) {
+    return do_g2p_direct<double>(c, m, g, p, prm);
+}
+int32_t tb_g2p_f32(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p, const tb_step_params* prm) {
+    return do_g2p_direct<float>(c, m, g, p, prm);
+}
+
+int32_t tb_step_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                    const tb_step_params* prm, int32_t nsteps) {
+    return dispatch_step<double>(c, m, p, part, g, prm, nsteps, true, true, true, true);
+}
+int32_t tb_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                    const tb_step_params* prm, int32_t nsteps) {
+    return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true);
+}
+
+int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
+                            int32_t nsteps) {
+    return do_rollout<double>(c, m, host, prm, nsteps);
+}
+int32_t tb_rollout_host_f32(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
+                            int32_t nsteps) {
+    return do_rollout<float>(c, m, host, prm, nsteps);
+}
+
+}  // extern "C"

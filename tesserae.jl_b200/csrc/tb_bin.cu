@@ -1,0 +1,313 @@
+// tb_bin.cu -- particle binning into grid blocks: the device counterpart of
+// update!(::GPUBlockStrategy, x) (Tesserae.jl src/Parallel/gpu_block_strategy.jl:142-166),
+// producing the block order of the reference CPU strategy bit for bit: block id
+// ascending, particle id ascending inside a block (cpu_block_strategy.jl:174-190).
+//
+//   count    one thread per particle: findblock, warp-aggregated count atomics
+//   scan     3 launches over packed (count | nonempty << 32) 64-bit sums: tile
+//            reduce, single-CTA spine, tile rescan writing offsets, cursors,
+//            the compacted block list and the totals [nactive, nassigned]
+//   scatter  one thread per particle: a warp reserves one run per distinct
+//            block with a single atomic and writes its particles in lane order
+//   fixup    one CTA per non-empty block: the block's segment is a set of runs,
+//            one per warp (32 consecutive particle ids), each ascending; the
+//            runs are sorted by warp id (bitonic, shared memory, or a global
+//            scratch region for segments above 2048 runs) and copied in order.
+// The result is deterministic regardless of atomic order.
+#include "tb_launch.cuh"
+
+namespace tb {
+
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(256) bin_count_kernel(DMesh<D, T> M, const T* __restrict__ x0,
+                                                        const T* __restrict__ x1, const T* __restrict__ x2,
+                                                        long long n, int* __restrict__ blockids,
+                                                        int* __restrict__ counts) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int b = -1;
+    if (p < n) {
+        T x[3];
+        x[0] = x0[p];
+        x[1] = x1[p];
+        if constexpr (D == 3) x[2] = x2[p];
+        b = findblock<D, T>(M, x);
+        blockids[p] = b;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int leader = __ffs(peers) - 1;
+    if (b > 0 && int(threadIdx.x & 31) == leader) atomicAdd(&counts[b - 1], __popc(peers));
+}
+
+__device__ __forceinline__ unsigned long long pack_count(int c) {
+    return (unsigned long long)(unsigned)c | ((unsigned long long)(c != 0) << 32);
+}
+
+// Inclusive block scan of one 64-bit value per thread (blockDim = 256).
+__device__ __forceinline__ unsigned long long block_incl_scan(unsigned long long v, unsigned long long* warp_tot,
+                                                              unsigned long long& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_tot[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned long long w = lane < nw ? warp_tot[lane] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    total = warp_tot[nw - 1];
+    unsigned long long r = v + (wid > 0 ? warp_tot[wid - 1] : 0ull);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) scan_reduce_kernel(const int* __restrict__ counts, int nb,
+                                                          unsigned long long* __restrict__ partials) {
+    __shared__ unsigned long long wt[8];
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (base + k < nb) s += pack_count(counts[base + k]);
+    unsigned long long total;
+    block_incl_scan(s, wt, total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+// Exclusive scan of the tile partials in place (one CTA).
+__global__ void __launch_bounds__(256) scan_spine_kernel(unsigned long long* partials, int ntiles) {
+    __shared__ unsigned long long wt[8];
+    unsigned long long carry = 0;
+    for (int c = 0; c < ntiles; c += 256) {
+        const int i = c + threadIdx.x;
+        unsigned long long v = i < ntiles ? partials[i] : 0ull;
+        unsigned long long total;
+        unsigned long long incl = block_incl_scan(v, wt, total);
+        if (i < ntiles) partials[i] = carry + incl - v;
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(256) scan_finalize_kernel(const int* __restrict__ counts, int nb,
+                                                            const unsigned long long* __restrict__ partials,
+                                                            int* __restrict__ offsets, int* __restrict__ cursors,
+                                                            int* __restrict__ blocklist, int* __restrict__ totals) {
+    __shared__ unsigned long long wt[8];
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+    int c[4];
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        c[k] = (base + k < nb) ? counts[base + k] : 0;
+        s += pack_count(c[k]);
+    }
+    unsigned long long total;
+    unsigned long long incl = block_incl_scan(s, wt, total);
+    unsigned long long run = partials[blockIdx.x] + incl - s;  // exclusive prefix of this thread
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int b = base + k;
+        if (b < nb) {
+            const int start = int(run & 0xffffffffull);
+            offsets[b] = start;
+            cursors[b] = start;
+            if (c[k] != 0) blocklist[int(run >> 32)] = b + 1;
+            run += pack_count(c[k]);
+            if (b == nb - 1) {
+                offsets[nb] = int(run & 0xffffffffull);
+                totals[0] = int(run >> 32);
+                totals[1] = int(run & 0xffffffffull);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) bin_scatter_kernel(const int* __restrict__ blockids, long long n,
+                                                          int* __restrict__ cursors, int* __restrict__ perm_tmp) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = p < n ? blockids[p] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    const int rank = __popc(peers & lanemask_lt());
+    int base = 0;
+    if (b > 0 && lane == leader) base = atomicAdd(&cursors[b - 1], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (b > 0) perm_tmp[base + rank] = int(p);
+}
+
+constexpr int FIX_THREADS = 128;
+constexpr int FIX_SMEM_KEYS = 2048;
+
+__device__ __forceinline__ int next_pow2(int v) {
+    int k = 1;
+    while (k < v) k <<= 1;
+    return k;
+}
+
+__global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __restrict__ totals,
+                                                                const int* __restrict__ blocklist,
+                                                                const int* __restrict__ offsets,
+                                                                const int* __restrict__ counts,
+                                                                const int* __restrict__ S, int* __restrict__ perm,
+                                                                unsigned long long* __restrict__ gscratch) {
+    __shared__ unsigned long long sbuf[FIX_SMEM_KEYS];
+    __shared__ int kcount;
+    __shared__ int wsum[FIX_THREADS / 32];
+    const int nactive = totals[0];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        const int b = blocklist[bi] - 1;
+        const int s = offsets[b];
+        const int n = counts[b];
+        const int* seg = S + s;
+        int* out = perm + s;
+        // Run heads: the first element, and every element whose warp id differs
+        // from its predecessor's. Key = (warp id << 32) | position in segment.
+        // First count them to pick the buffer: shared memory when the padded key
+        // count fits, else the block's own region [2s, 2s + 2n) of the global
+        // scratch (next_pow2(k) <= 2n, and segments are disjoint).
+        if (tid == 0) kcount = 0;
+        __syncthreads();
+        int myheads = 0;
+        for (int j = tid; j < n; j += FIX_THREADS)
+            myheads += (j == 0) || ((seg[j - 1] >> 5) != (seg[j] >> 5));
+        if (myheads) atomicAdd(&kcount, myheads);
+        __syncthreads();
+        const int k = kcount;
+        const int K = next_pow2(k);
+        unsigned long long* buf = (K <= FIX_SMEM_KEYS) ? sbuf : gscratch + 2ll * s;
+        __syncthreads();
+        if (tid == 0) kcount = 0;
+        __syncthreads();
+        for (int j = tid; j < n; j += FIX_THREADS) {
+            const int v = seg[j];
+            const bool head = (j == 0) || ((seg[j - 1] >> 5) != (v >> 5));
+            if (head) {
+                const int idx = atomicAdd(&kcount, 1);
+                buf[idx] = ((unsigned long long)(unsigned)(v >> 5) << 32) | (unsigned)j;
+            }
+        }
+        __syncthreads();
+        for (int t = k + tid; t < K; t += FIX_THREADS) buf[t] = ~0ull;
+        __syncthreads();
+        // Bitonic sort of the K keys (ascending).
+        for (int size = 2; size <= K; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int i = tid; i < (K >> 1); i += FIX_THREADS) {
+                    const int lo = (i / stride) * 2 * stride + (i % stride);
+                    const int hi = lo + stride;
+                    const bool asc = (lo & size) == 0;
+                    const unsigned long long a = buf[lo], c = buf[hi];
+                    if ((a > c) == asc) {
+                        buf[lo] = c;
+                        buf[hi] = a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // Copy the runs in sorted order; each run is at most 32 long.
+        int base = 0;
+        for (int c0 = 0; c0 < k; c0 += FIX_THREADS) {
+            const int r = c0 + tid;
+            int len = 0, j0 = 0;
+            if (r < k) {
+                const unsigned long long e = buf[r];
+                j0 = int(e & 0xffffffffull);
+                const int w = int(e >> 32);
+                len = 1;
+                while (j0 + len < n && (seg[j0 + len] >> 5) == w) ++len;
+            }
+            // block exclusive scan of len
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane == 31) wsum[wid] = incl;
+            __syncthreads();
+            int wprefix = 0, total = 0;
+#pragma unroll
+            for (int q = 0; q < FIX_THREADS / 32; ++q) {
+                if (q < wid) wprefix += wsum[q];
+                total += wsum[q];
+            }
+            const int excl = base + wprefix + incl - len;
+            for (int t = 0; t < len; ++t) out[excl + t] = seg[j0 + t] + 1;
+            base += total;
+            __syncthreads();
+        }
+    }
+}
+
+inline unsigned grid_for(long long n, int threads) { return unsigned((n + threads - 1) / threads); }
+
+}  // namespace
+
+template <int D, class T>
+cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,
+                             const LaunchCfg& cfg) {
+    cudaError_t e = cudaMemsetAsync(b.counts, 0, sizeof(int) * size_t(M.nblocks), cfg.stream);
+    if (e != cudaSuccess) return e;
+    if (n > 0) {
+        bin_count_kernel<D, T><<<grid_for(n, 256), 256, 0, cfg.stream>>>(M, x[0], x[1], D == 3 ? x[2] : x[1], n,
+                                                                         b.blockids, b.counts);
+        ++*cfg.launches;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_rest(int nb, long long n, const BinBuffers& b, const LaunchCfg& cfg) {
+    const int nt = scan_tiles(nb);
+    scan_reduce_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials);
+    scan_spine_kernel<<<1, 256, 0, cfg.stream>>>(b.partials, nt);
+    scan_finalize_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials, b.offsets, b.cursors, b.blocklist,
+                                                     b.totals);
+    *cfg.launches += 3;
+    if (n > 0) {
+        bin_scatter_kernel<<<grid_for(n, 256), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors, b.perm_tmp);
+        const int grid = std::min(nb, cfg.num_sms * 16);
+        bin_fixup_kernel<<<grid, FIX_THREADS, 0, cfg.stream>>>(b.totals, b.blocklist, b.offsets, b.counts,
+                                                               b.perm_tmp, b.perm, b.sort_scratch);
+        *cfg.launches += 2;
+    }
+    return cudaGetLastError();
+}
+
+template <int D, class T>
+cudaError_t launch_bin(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,
+                       const LaunchCfg& cfg, bool) {
+    cudaError_t e = launch_bin_count<D, T>(M, x, n, b, cfg);
+    if (e != cudaSuccess) return e;
+    return launch_bin_rest(M.nblocks, n, b, cfg);
+}
+
+#define TB_INST_BIN(D, T)                                                                                     \
+    template cudaError_t launch_bin<D, T>(const DMesh<D, T>&, const T* const*, long long, const BinBuffers&, \
+                                          const LaunchCfg&, bool);                                            \
+    template cudaError_t launch_bin_count<D, T>(const DMesh<D, T>&, const T* const*, long long,              \
+                                                const BinBuffers&, const LaunchCfg&);
+TB_INST_BIN(3, double)
+TB_INST_BIN(3, float)
+TB_INST_BIN(2, double)
+TB_INST_BIN(2, float)
+
+}  // namespace tb

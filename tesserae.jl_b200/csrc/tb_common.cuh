@@ -1,0 +1,469 @@
+// tb_common.cuh -- device-side data views and basis math shared by the kernels
+// of libtesserae_b200.so (sm_100a).
+//
+// Mesh, window and weight rules follow the reference:
+//   findblock / windows    Tesserae.jl src/Mesh/cartesian.jl:146-285
+//   quadratic B-spline     src/Basis/bspline.jl:28-184 (fast full-support path and
+//                          the nodewise path for truncated windows)
+//   uGIMP                  src/Basis/gimp.jl:16-40
+//   WLS (MLS-MPM)          src/Basis/wls.jl:22-84
+// The basis values are evaluated inside the transfers ("deferred" weights,
+// src/Transfer/runtime.jl:55-130), so no weight array crosses HBM.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/tesserae_b200.h"
+
+namespace tb {
+
+// Error bits a kernel raises in the context's device status word.
+enum : int {
+    ERR_TILE_RANGE = 1,   // a support window left its block tile
+    ERR_GIMP_LENGTH = 2,  // uGIMP requires 0 <= l <= h (gimp.jl:22)
+    ERR_WLS_SINGULAR = 4  // WLS moment matrix not invertible
+};
+
+template <int D, class T>
+struct DMesh {
+    int n[3];      // nodes per axis
+    int nb[3];     // blocks per axis
+    int L;         // block_log2
+    int nblocks;
+    long long nnodes;
+    T xmin[3];
+    T h, h_inv;
+    double xmin64[3], h64;
+};
+
+template <int D, class T>
+inline DMesh<D, T> make_dmesh(const tb_mesh& m) {
+    DMesh<D, T> M{};
+    M.L = m.block_log2;
+    M.nblocks = 1;
+    M.nnodes = 1;
+    for (int d = 0; d < 3; ++d) {
+        M.n[d] = d < D ? int(m.n_nodes[d]) : 1;
+        M.nb[d] = d < D ? ((M.n[d] - 1) >> M.L) + 1 : 1;
+        M.xmin[d] = T(m.xmin[d]);
+        M.xmin64[d] = m.xmin[d];
+        M.nblocks *= M.nb[d];
+        M.nnodes *= M.n[d];
+    }
+    M.h = T(m.h);          // the Float32 form casts h and h_inv separately (src/adapt.jl:53-57)
+    M.h_inv = T(m.h_inv);
+    M.h64 = m.h;
+    return M;
+}
+
+// Particle SoA views. T is the state scalar; F is always double.
+template <class T>
+struct PView {
+    long long n;
+    T* x[3];
+    T* v[3];
+    T* V;
+    const T* m;
+    const T* l;
+    T* gv[9];
+    T* sig[6];
+    double* F[9];
+    T* B[9];
+    const T* V0;
+    const T* mu;
+    const T* lam;
+};
+
+template <class T>
+struct GView {
+    T* m;
+    T* mv[3];
+    T* f[3];
+    T* v[3];
+    T* vn[3];
+};
+
+// Step scalars, converted once to the state type.
+template <class T>
+struct Scalars {
+    T dt, mass, V0, g[3], gimp_l, alpha;
+    double dt64, V0_64, mu, lam;
+    int basis, transfer, material, wall_mask, wall_layers;
+};
+
+template <class T>
+inline Scalars<T> make_scalars(const tb_step_params& p) {
+    Scalars<T> s{};
+    s.dt = T(p.dt);
+    s.mass = T(p.mass);
+    s.V0 = T(p.V0);
+    for (int d = 0; d < 3; ++d) s.g[d] = T(p.gravity[d]);
+    s.gimp_l = T(p.gimp_l);
+    s.alpha = T(p.flip_alpha);
+    s.dt64 = p.dt;
+    s.V0_64 = p.V0;
+    s.mu = p.mu;
+    s.lam = p.lambda;
+    s.basis = p.basis;
+    s.transfer = p.transfer;
+    s.material = p.material;
+    s.wall_mask = p.wall_mask;
+    s.wall_layers = p.wall_layers;
+    return s;
+}
+
+template <int D>
+__host__ __device__ constexpr int nsym() { return D == 3 ? 6 : 3; }
+
+// Index of (r, c) in Tensorial's symmetric independent-component order.
+template <int D>
+__host__ __device__ constexpr int symidx(int r, int c) {
+    return (r >= c) ? (c * D - c * (c - 1) / 2 + (r - c)) : (r * D - r * (r - 1) / 2 + (c - r));
+}
+
+// Node coordinate X_d(i) = xmin + i h, rounded once in FP64 and cast to T
+// (the reference stores the axes as Vector{T}(range(xmin; step=h, length=n))).
+template <int D, class T>
+__device__ __forceinline__ T node_coord(const DMesh<D, T>& M, int d, int i) {
+    return T(__dadd_rn(M.xmin64[d], __dmul_rn(double(i), M.h64)));
+}
+
+// 1-based linear block id (0 = outside), cartesian.jl:271-285 + sub2ind.
+template <int D, class T>
+__device__ __forceinline__ int findblock(const DMesh<D, T>& M, const T* x) {
+    int lin = 0;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+        T c = floor((x[d] - M.xmin[d]) * M.h_inv);
+        if (!(c >= T(0) && c <= T(M.n[d] - 2))) return 0;
+        lin = lin * M.nb[d] + (int(c) >> M.L);
+    }
+    return lin + 1;
+}
+
+// Per-axis basis data of one particle: window start/count and the 1-D jets.
+template <class T>
+struct Axis {
+    int lo, cnt;
+    T val[3], der[3];
+};
+
+// 1-D jets, forward-mode derivative through abs() as in the reference's AD.
+template <class T>
+__device__ __forceinline__ void jet_bspline_quadratic(T xi, T& val, T& der) {
+    T s = signbit(xi) ? T(-1) : T(1);
+    T a = fabs(xi);
+    if (a < T(0.5)) {
+        val = (T(3) - T(4) * (a * a)) / T(4);
+        der = -(T(2) * a) * s;
+    } else if (a < T(1.5)) {
+        T t = T(3) - T(2) * a;
+        val = (t * t) / T(8);
+        der = -(t / T(2)) * s;
+    } else {
+        val = T(0);
+        der = T(0);
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void jet_ugimp(T xi, T l, T& val, T& der) {
+    T s = signbit(xi) ? T(-1) : T(1);
+    T a = fabs(xi);
+    if (a < l / T(2)) {
+        val = T(1) - (T(4) * (a * a) + l * l) / (T(4) * l);
+        der = -(T(2) * a / l) * s;
+    } else if (a < T(1) - l / T(2)) {
+        val = T(1) - a;
+        der = -s;
+    } else if (a < T(1) + l / T(2)) {
+        T t = T(1) + l / T(2) - a;
+        val = (t * t) / (T(2) * l);
+        der = -(t / l) * s;
+    } else {
+        val = T(0);
+        der = T(0);
+    }
+}
+
+// Fast full-support axis values (bspline.jl:90-100): t = fract(xi - 1/2),
+// N = (1/2 - t + t^2/2, 1/2 + t - t^2, t^2/2), N' = (t - 1, 1 - 2t, t).
+template <class T>
+__device__ __forceinline__ void bspline_quadratic_axis(T xi, T* v0, T* v1) {
+    T u = xi - T(0.5);
+    T t = u - floor(u);
+    const T half = T(0.5);
+    v0[0] = half + t * (T(-1) + t * half);
+    v0[1] = half + t * (T(1) + t * T(-1));
+    v0[2] = t * (t * half);
+    v1[0] = T(-1) + t;
+    v1[1] = T(1) + t * T(-2);
+    v1[2] = t;
+}
+
+// Window and 1-D jets of one particle for B-spline / uGIMP kernels (the
+// kernel part of WLS too). Returns false when the particle is outside the mesh
+// (empty window, cartesian.jl:190-199). `full` reports a 3^D window.
+template <int D, class T>
+__device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, const T* x, T lnorm, Axis<T>* ax,
+                                             bool& full) {
+    T xi[3];
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        xi[d] = (x[d] - M.xmin[d]) * M.h_inv;
+        T c = floor(xi[d]);
+        inside = inside && (c >= T(0) && c <= T(M.n[d] - 2));
+    }
+    if (!inside) return false;
+    const bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    full = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        int s, e;
+        if (gimp) {
+            T r = T(1) + lnorm / T(2);
+            s = int(floor(xi[d] - r)) + 1;
+            e = int(floor(xi[d] + r));
+        } else {
+            s = int(floor(xi[d] - T(0.5)));
+            e = s + 2;
+        }
+        int lo = max(s, 0), hi = min(e, M.n[d] - 1);
+        ax[d].lo = lo;
+        ax[d].cnt = hi - lo + 1;
+        full = full && (ax[d].cnt == 3);
+    }
+    if (basis == TB_BSPLINE_QUADRATIC && full) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) bspline_quadratic_axis(xi[d], ax[d].val, ax[d].der);
+        return true;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ax[d].val[k] = T(0);
+            ax[d].der[k] = T(0);
+            if (k < ax[d].cnt) {
+                T xn = (x[d] - node_coord(M, d, ax[d].lo + k)) * M.h_inv;
+                if (gimp) jet_ugimp(xn, lnorm, ax[d].val[k], ax[d].der[k]);
+                else jet_bspline_quadratic(xn, ax[d].val[k], ax[d].der[k]);
+            }
+        }
+    }
+    return true;
+}
+
+// Kernel value and gradient at window slot (i, j, k), product order of
+// bspline.jl:133-142 / basis_weight.jl:49-60.
+template <int D, class T>
+__device__ __forceinline__ void node_weight(const DMesh<D, T>& M, const Axis<T>* ax, int i, int j, int k, T& w,
+                                            T* dw) {
+    if constexpr (D == 3) {
+        T vx = ax[0].val[i], vy = ax[1].val[j], vz = ax[2].val[k];
+        w = (vx * vy) * vz;
+        dw[0] = ((ax[0].der[i] * vy) * vz) * M.h_inv;
+        dw[1] = ((vx * ax[1].der[j]) * vz) * M.h_inv;
+        dw[2] = ((vx * vy) * ax[2].der[k]) * M.h_inv;
+    } else {
+        T vx = ax[0].val[i], vy = ax[1].val[j];
+        w = vx * vy;
+        dw[0] = (ax[0].der[i] * vy) * M.h_inv;
+        dw[1] = (vx * ax[1].der[j]) * M.h_inv;
+    }
+}
+
+// WLS moment-matrix inverse (wls.jl:51-68); the closed form diag(1, 4/h^2) for a
+// full quadratic B-spline support (wls.jl:29-49). Returns false if singular.
+template <int D, class T>
+__device__ __forceinline__ bool wls_minv(const DMesh<D, T>& M, const Axis<T>* ax, const T* x, bool closed,
+                                         T (&Mi)[D + 1][D + 1]) {
+    constexpr int N = D + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < N; ++c) Mi[r][c] = T(0);
+    if (closed) {
+        Mi[0][0] = T(1);
+        T cval = T(4) / (M.h * M.h);
+#pragma unroll
+        for (int d = 1; d < N; ++d) Mi[d][d] = cval;
+        return true;
+    }
+    T A[N][2 * N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < 2 * N; ++c) A[r][c] = (c - N == r) ? T(1) : T(0);
+#pragma unroll
+    for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                T w, dw[3];
+                node_weight<D, T>(M, ax, i, j, D == 3 ? k : 0, w, dw);
+                T P[N];
+                P[0] = T(1);
+                P[1] = node_coord(M, 0, ax[0].lo + i) - x[0];
+                P[2] = node_coord(M, 1, ax[1].lo + j) - x[1];
+                if constexpr (D == 3) P[3] = node_coord(M, 2, ax[2].lo + k) - x[2];
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+#pragma unroll
+                    for (int c = 0; c < N; ++c) A[r][c] += w * P[r] * P[c];
+            }
+    // Gauss-Jordan with partial pivoting on [M | I].
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        int p = c;
+#pragma unroll
+        for (int r = c + 1; r < N; ++r)
+            if (fabs(A[r][c]) > fabs(A[p][c])) p = r;
+        if (A[p][c] == T(0)) return false;
+        if (p != c) {
+#pragma unroll
+            for (int k = 0; k < 2 * N; ++k) {
+                T t = A[p][k];
+                A[p][k] = A[c][k];
+                A[c][k] = t;
+            }
+        }
+        T inv = T(1) / A[c][c];
+#pragma unroll
+        for (int k = 0; k < 2 * N; ++k) A[c][k] *= inv;
+#pragma unroll
+        for (int r = 0; r < N; ++r)
+            if (r != c) {
+                T f = A[r][c];
+#pragma unroll
+                for (int k = 0; k < 2 * N; ++k) A[r][k] -= f * A[c][k];
+            }
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < N; ++c) Mi[r][c] = A[r][c + N];
+    return true;
+}
+
+// Basis state of one particle, ready for per-node evaluation in a transfer.
+template <int D, class T>
+struct Basis {
+    Axis<T> ax[D];
+    T Mi[D + 1][D + 1];
+    bool wls;
+};
+
+// Prepare the basis of one particle. Returns false for an empty window.
+template <int D, class T, bool ALLOW_WLS = true>
+__device__ __forceinline__ bool prepare_basis(const DMesh<D, T>& M, int basis, const T* x, T l_abs,
+                                              Basis<D, T>& B, int* err) {
+    T lnorm = T(0);
+    if (basis == TB_UGIMP || basis == TB_WLS_UGIMP) {
+        lnorm = l_abs / M.h;
+        if (!(lnorm >= T(0) && lnorm <= T(1))) {
+            atomicOr(err, ERR_GIMP_LENGTH);
+            return false;
+        }
+    }
+    bool full = false;
+    if (!axis_weights<D, T>(M, basis, x, lnorm, B.ax, full)) return false;
+    B.wls = ALLOW_WLS && (basis == TB_WLS_BSPLINE_QUADRATIC || basis == TB_WLS_UGIMP);
+    if constexpr (ALLOW_WLS) if (B.wls) {
+        bool closed = (basis == TB_WLS_BSPLINE_QUADRATIC) && full;
+        if (!wls_minv<D, T>(M, B.ax, x, closed, B.Mi)) {
+            atomicOr(err, ERR_WLS_SINGULAR);
+            return false;
+        }
+    }
+    return true;
+}
+
+// w and grad w at window slot (i, j, k); `rel` = X_i - x_p per axis.
+template <int D, class T>
+__device__ __forceinline__ void eval_node(const DMesh<D, T>& M, const Basis<D, T>& B, int i, int j, int k,
+                                          const T* rel, T& w, T* dw) {
+    node_weight<D, T>(M, B.ax, i, j, k, w, dw);
+    if (B.wls) {
+        constexpr int N = D + 1;
+        T P[N];
+        P[0] = T(1);
+#pragma unroll
+        for (int d = 0; d < D; ++d) P[d + 1] = rel[d];
+        T wq[N];
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            T acc = T(0);
+#pragma unroll
+            for (int c = 0; c < N; ++c) acc += B.Mi[r][c] * P[c];
+            wq[r] = w * acc;
+        }
+        w = wq[0];
+#pragma unroll
+        for (int d = 0; d < D; ++d) dw[d] = wq[d + 1];
+    }
+}
+
+// FP64 particle kinematics and constitutive update (README.md:82-86):
+// F = (I + dt grad_v) F, J = det F, sigma by Neo-Hookean or the weakly
+// compressible fluid p = -K (J - 1), V = V0 J. F, J and log J stay in FP64.
+template <int D, class T>
+__device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars<T>& s, long long p,
+                                                const T (&gv)[3][3]) {
+    double F[3][3], Fn[3][3];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) F[r][c] = P.F[r + c * D][p];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            double a = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                double Ark = (r == k ? 1.0 : 0.0) + double(gv[r][k]) * s.dt64;
+                a += Ark * F[k][c];
+            }
+            Fn[r][c] = a;
+        }
+    double J;
+    if constexpr (D == 3)
+        J = Fn[0][0] * (Fn[1][1] * Fn[2][2] - Fn[1][2] * Fn[2][1]) -
+            Fn[0][1] * (Fn[1][0] * Fn[2][2] - Fn[1][2] * Fn[2][0]) +
+            Fn[0][2] * (Fn[1][0] * Fn[2][1] - Fn[1][1] * Fn[2][0]);
+    else
+        J = Fn[0][0] * Fn[1][1] - Fn[0][1] * Fn[1][0];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) P.F[r + c * D][p] = Fn[r][c];
+    const double mu = P.mu ? double(P.mu[p]) : s.mu;
+    const double lam = P.lam ? double(P.lam[p]) : s.lam;
+    if (s.material == 1) {
+        const double pr = lam * (J - 1.0);
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c <= r; ++c) P.sig[symidx<D>(r, c)][p] = T(r == c ? pr : 0.0);
+    } else {
+        const double lj = log(J);
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c <= r; ++c) {
+                double b = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) b += Fn[r][k] * Fn[c][k];
+                double sg = (mu * (b - (r == c ? 1.0 : 0.0)) + (r == c ? lam * lj : 0.0)) / J;
+                P.sig[symidx<D>(r, c)][p] = T(sg);
+            }
+    }
+    const double V0 = P.V0 ? double(P.V0[p]) : s.V0_64;
+    P.V[p] = T(V0 * J);
+}
+
+}  // namespace tb

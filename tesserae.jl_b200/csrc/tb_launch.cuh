@@ -1,0 +1,67 @@
+// tb_launch.cuh -- host-side launchers shared between the kernel files and the
+// C-ABI layer of libtesserae_b200.so.
+#pragma once
+
+#include "tb_common.cuh"
+
+namespace tb {
+
+// Device buffers of one binning pass (GPUBlockStrategy arrays plus scratch).
+struct BinBuffers {
+    int* blockids;        // [n] caller
+    int* counts;          // [nb] caller
+    int* offsets;         // [nb+1] caller
+    int* blocklist;       // [nb] caller
+    int* perm;            // [n] caller, 1-based particle ids
+    int* cursors;         // [nb] scratch
+    int* perm_tmp;        // [n] scratch, 0-based ids in warp-run order
+    unsigned long long* partials;  // [ntiles] scratch
+    unsigned long long* sort_scratch;  // [2n] scratch for large blocks
+    int* totals;          // [2] device: nactive, nassigned
+};
+
+constexpr int SCAN_TILE = 1024;  // blocks per scan tile (256 threads x 4)
+
+inline int scan_tiles(int nb) { return (nb + SCAN_TILE - 1) / SCAN_TILE; }
+
+struct LaunchCfg {
+    cudaStream_t stream;
+    int num_sms;
+    long long* launches;  // incremented per kernel launch
+    int* err;             // device status word
+};
+
+template <int D, class T>
+cudaError_t launch_bin(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,
+                       const LaunchCfg& cfg, bool count_only_done = false);
+
+// Count kernel alone (positions -> blockids, counts); the rest of the pass in
+// launch_bin_rest. Split so a fused step can count inside G2P.
+template <int D, class T>
+cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,
+                             const LaunchCfg& cfg);
+cudaError_t launch_bin_rest(int nblocks, long long n, const BinBuffers& b, const LaunchCfg& cfg);
+
+template <int D, class T, int BW>
+cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                       const BinBuffers& b, const LaunchCfg& cfg);
+
+template <int D, class T>
+cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s, const LaunchCfg& cfg);
+
+template <int D, class T>
+cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const LaunchCfg& cfg);
+
+template <int D, class T, int BW>
+cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                       const BinBuffers& b, const LaunchCfg& cfg);
+
+template <int D, class T>
+cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                              const LaunchCfg& cfg);
+
+template <int D, class T>
+cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* grad_w,
+                                  long long* window, const LaunchCfg& cfg);
+
+}  // namespace tb

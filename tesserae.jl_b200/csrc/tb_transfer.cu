@@ -1,0 +1,408 @@
+// tb_transfer.cu -- grid update and G2P kernels of the explicit MPM step.
+//
+// (P2G is in tb_p2g.cu.)
+// grid (src/Transfer/foreach.jl:276-339, docs/src/gpu.md:309-316): vn = mv/m,
+//      v = vn + dt f / m guarded by m != 0, then the slip-wall slices.
+// G2P  (src/Transfer/gpu.jl:226-232, README.md:79-86): one CTA per non-empty
+//      block stages the block's (v, v - vn) tile in shared memory and gathers
+//      for each particle of the block; particles outside the mesh (empty window)
+//      are updated by a particle-parallel pass.
+#include "tb_launch.cuh"
+
+namespace tb {
+
+namespace {
+
+template <int D, int BW>
+struct Tile {
+    static constexpr int TS = BW + 3;
+    static constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
+};
+
+template <int D, class T>
+__device__ __forceinline__ void load_x(const PView<T>& P, long long p, T* x) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(256) grid_zero_kernel(GView<T> G, long long nn) {
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < nn; I += (long long)gridDim.x * blockDim.x) {
+        G.m[I] = T(0);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            G.mv[d][I] = T(0);
+            G.f[d][I] = T(0);
+        }
+    }
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(256) grid_update_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s) {
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < M.nnodes;
+         I += (long long)gridDim.x * blockDim.x) {
+        const T m = G.m[I];
+        int idx[3];
+        long long r = I;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            idx[d] = int(r % M.n[d]);
+            r /= M.n[d];
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            T vn = T(0), v = T(0);
+            if (m != T(0)) {
+                vn = G.mv[d][I] / m;
+                v = vn + (s.dt * G.f[d][I]) / m;
+            }
+            if (s.wall_mask) {
+                const bool lo = (s.wall_mask >> (2 * d)) & 1, hi = (s.wall_mask >> (2 * d + 1)) & 1;
+                if ((lo && idx[d] < s.wall_layers) || (hi && idx[d] >= M.n[d] - s.wall_layers)) {
+                    vn = T(0);
+                    v = T(0);
+                }
+            }
+            G.vn[d][I] = vn;
+            G.v[d][I] = v;
+        }
+    }
+}
+
+// Final per-particle writes of @G2P and the FP64 constitutive update.
+template <int D, class T>
+__device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& s, long long p, const T* x,
+                                           const T* vp, const T* vpic, const T* dvf, const T (&gv)[3][3],
+                                           const T* dxs, const T (&Bn)[3][3]) {
+    if (s.transfer == TB_TRANSFER_APIC) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) P.v[d][p] = vpic[d];
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) P.B[r + c * D][p] = Bn[r][c];
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const T vflip = vp[d] + dvf[d];
+            P.v[d][p] = (s.alpha == T(1)) ? vflip : (T(1) - s.alpha) * vpic[d] + s.alpha * vflip;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) P.gv[r + c * D][p] = gv[r][c];
+#pragma unroll
+    for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
+    particle_update<D, T>(P, s, p, gv);
+}
+
+template <int D, class T, int BW, bool GEN>
+__global__ void __launch_bounds__(128) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
+                                                       const int* __restrict__ totals,
+                                                       const int* __restrict__ blocklist,
+                                                       const int* __restrict__ offsets,
+                                                       const int* __restrict__ perm, int* err) {
+    constexpr int TS = Tile<D, BW>::TS, TN = Tile<D, BW>::TN;
+    __shared__ T tv[D * TN];
+    __shared__ T tdv[D * TN];
+    const int nactive = totals[0];
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const bool apic = s.transfer == TB_TRANSFER_APIC;
+    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        int b = blocklist[bi] - 1;
+        int org[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            org[d] = (b % M.nb[d]) * BW - 1;
+            b /= M.nb[d];
+        }
+        b = blocklist[bi] - 1;
+        for (int t = tid; t < TN; t += nth) {
+            int node[3], rem = t;
+            bool inside = true;
+            long long lin = 0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                node[d] = org[d] + rem % TS;
+                rem /= TS;
+                inside = inside && node[d] >= 0 && node[d] < M.n[d];
+            }
+#pragma unroll
+            for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + (inside ? node[d] : 0);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const T vi = inside ? G.v[d][lin] : T(0);
+                const T vni = inside ? G.vn[d][lin] : T(0);
+                tv[d * TN + t] = vi;
+                tdv[d * TN + t] = vi - vni;
+            }
+        }
+        __syncthreads();
+        const int s0 = offsets[b], s1 = offsets[b + 1];
+        for (int j = s0 + tid; j < s1; j += nth) {
+            const long long p = perm[j] - 1;
+            T x[3], vp[3];
+            load_x<D, T>(P, p, x);
+#pragma unroll
+            for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
+            const T l = P.l ? P.l[p] : s.gimp_l;
+            T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
+            T gv[3][3] = {}, Bn[3][3] = {};
+            Basis<D, T> B;
+            if (prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) {
+                const bool need_rel = GEN && (B.wls || apic);
+#pragma unroll
+                for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            const int idx[3] = {i, jj, k};
+                            int t = 0;
+                            bool ok = true;
+#pragma unroll
+                            for (int d = D - 1; d >= 0; --d) {
+                                const int q = B.ax[d].lo + idx[d] - org[d];
+                                ok = ok && (q >= 0 && q < TS);
+                                t = t * TS + q;
+                            }
+                            if (!ok) {
+                                atomicOr(err, ERR_TILE_RANGE);
+                                continue;
+                            }
+                            T rel[3] = {T(0), T(0), T(0)};
+                            if (need_rel) {
+#pragma unroll
+                                for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
+                            }
+                            T w, dw[3];
+                            eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
+                            T vi[3];
+#pragma unroll
+                            for (int d = 0; d < D; ++d) {
+                                vi[d] = tv[d * TN + t];
+                                vpic[d] += w * vi[d];
+                                dvf[d] += w * tdv[d * TN + t];
+                                dxs[d] += (w * vi[d]) * s.dt;
+                            }
+#pragma unroll
+                            for (int r = 0; r < D; ++r)
+#pragma unroll
+                                for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * dw[c];
+                            if (GEN && apic) {
+#pragma unroll
+                                for (int r = 0; r < D; ++r)
+#pragma unroll
+                                    for (int c = 0; c < D; ++c) Bn[r][c] += (w * vi[r]) * rel[c];
+                            }
+                        }
+            }
+            g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn);
+        }
+        __syncthreads();
+    }
+}
+
+// Particle-parallel G2P reading the grid from global memory: the reference's own
+// G2P schedule (one thread per particle, gpu.jl:226-232); needs no partition.
+template <int D, class T>
+__global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
+                                                         int* err) {
+    const bool apic = s.transfer == TB_TRANSFER_APIC;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        T x[3], vp[3];
+        load_x<D, T>(P, p, x);
+#pragma unroll
+        for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
+        const T l = P.l ? P.l[p] : s.gimp_l;
+        T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
+        T gv[3][3] = {}, Bn[3][3] = {};
+        Basis<D, T> B;
+        if (prepare_basis<D, T>(M, s.basis, x, l, B, err)) {
+            const bool need_rel = B.wls || apic;
+#pragma unroll
+            for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const int idx[3] = {i, jj, k};
+                        long long lin = 0;
+                        bool valid = true;
+#pragma unroll
+                        for (int d = D - 1; d >= 0; --d) {
+                            valid = valid && idx[d] < B.ax[d].cnt;
+                            lin = lin * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
+                        }
+                        T rel[3] = {T(0), T(0), T(0)};
+                        if (need_rel) {
+#pragma unroll
+                            for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
+                        }
+                        T w, dw[3];
+                        eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
+                        T vi[3];
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            vi[d] = valid ? __ldg(G.v[d] + lin) : T(0);
+                            const T dv = valid ? vi[d] - __ldg(G.vn[d] + lin) : T(0);
+                            vpic[d] += w * vi[d];
+                            dvf[d] += w * dv;
+                            dxs[d] += (w * vi[d]) * s.dt;
+                        }
+#pragma unroll
+                        for (int r = 0; r < D; ++r)
+#pragma unroll
+                            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * dw[c];
+                        if (apic) {
+#pragma unroll
+                            for (int r = 0; r < D; ++r)
+#pragma unroll
+                                for (int c = 0; c < D; ++c) Bn[r][c] += (w * vi[r]) * rel[c];
+                        }
+                    }
+        }
+        g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn);
+    }
+}
+
+// Particles outside the mesh (block id 0): empty window, so only the particle
+// equations run (v and x keep their values under FLIP).
+template <int D, class T>
+__global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T> s, const int* __restrict__ blockids) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        if (blockids[p] != 0) continue;
+        T x[3], vp[3], z[3] = {T(0), T(0), T(0)};
+        T gv[3][3] = {}, Bn[3][3] = {};
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            x[d] = P.x[d][p];
+            vp[d] = P.v[d][p];
+        }
+        g2p_finish<D, T>(P, s, p, x, vp, z, z, gv, z, Bn);
+    }
+}
+
+// update!(weights, particles, mesh) with stored values (basis_weight.jl:714-752):
+// w in (3,3,3,n) column-major, grad_w as Vec{D} per slot, window as 1-based
+// (start, stop) Int64 pairs; slots outside a truncated window are zeroed.
+template <int D, class T>
+__global__ void __launch_bounds__(128) update_weights_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s, T* w_out,
+                                                             T* gw_out, long long* win_out, int* err) {
+    constexpr int NW = (D == 3) ? 27 : 9;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        T x[3];
+        load_x<D, T>(P, p, x);
+        const T l = P.l ? P.l[p] : s.gimp_l;
+        Basis<D, T> B;
+        const bool ok = prepare_basis<D, T>(M, s.basis, x, l, B, err);
+        for (int slot = 0; slot < NW; ++slot) {
+            const int i = slot % 3, jj = (slot / 3) % 3, k = slot / 9;
+            T w = T(0), dw[3] = {T(0), T(0), T(0)};
+            if (ok && i < B.ax[0].cnt && jj < B.ax[1].cnt && (D == 2 || k < B.ax[D - 1].cnt)) {
+                const int idx[3] = {i, jj, k};
+                T rel[3] = {T(0), T(0), T(0)};
+                if (B.wls) {
+#pragma unroll
+                    for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
+                }
+                eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
+            }
+            w_out[p * NW + slot] = w;
+#pragma unroll
+            for (int d = 0; d < D; ++d) gw_out[(p * NW + slot) * D + d] = dw[d];
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            win_out[p * 2 * D + 2 * d] = ok ? B.ax[d].lo + 1 : 1;
+            win_out[p * 2 * D + 2 * d + 1] = ok ? B.ax[d].lo + B.ax[d].cnt : 0;
+        }
+    }
+}
+
+template <class K>
+int occupancy_grid(K kernel, int threads, int num_sms) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    return num_sms * (per_sm > 0 ? per_sm : 1);
+}
+
+}  // namespace
+
+template <int D, class T>
+cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const LaunchCfg& cfg) {
+    const long long nn = M.nnodes;
+    const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
+    grid_zero_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(G, nn);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T>
+cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s, const LaunchCfg& cfg) {
+    const long long nn = M.nnodes;
+    const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
+    grid_update_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(M, G, s);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T, int BW>
+cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                       const BinBuffers& b, const LaunchCfg& cfg) {
+    if (P.n == 0) return cudaSuccess;
+    const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
+    auto kern = gen ? g2p_tile_kernel<D, T, BW, true> : g2p_tile_kernel<D, T, BW, false>;
+    const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), M.nblocks);
+    kern<<<grid, 128, 0, cfg.stream>>>(M, G, P, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
+    g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids);
+    *cfg.launches += 2;
+    return cudaGetLastError();
+}
+
+template <int D, class T>
+cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                              const LaunchCfg& cfg) {
+    if (P.n == 0) return cudaSuccess;
+    const int grid = int(std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 32));
+    g2p_direct_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, G, P, s, cfg.err);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T>
+cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* gw,
+                                  long long* win, const LaunchCfg& cfg) {
+    if (P.n == 0) return cudaSuccess;
+    const int grid = int(std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 16));
+    update_weights_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, P, s, w, gw, win, cfg.err);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+#define TB_INST_T(D, T)                                                                                      \
+    template cudaError_t launch_grid_update<D, T>(const DMesh<D, T>&, const GView<T>&, const Scalars<T>&,   \
+                                                  const LaunchCfg&);                                         \
+    template cudaError_t launch_grid_zero<D, T>(const DMesh<D, T>&, const GView<T>&, const LaunchCfg&);     \
+    template cudaError_t launch_update_weights<D, T>(const DMesh<D, T>&, const PView<T>&, const Scalars<T>&, \
+                                                     T*, T*, long long*, const LaunchCfg&);                  \
+    template cudaError_t launch_g2p_direct<D, T>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,       \
+                                                 const Scalars<T>&, const LaunchCfg&);
+#define TB_INST_TB(D, T, BW)                                                                                 \
+    template cudaError_t launch_g2p<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,         \
+                                              const Scalars<T>&, const BinBuffers&, const LaunchCfg&);
+
+TB_INST_T(3, double)
+TB_INST_T(3, float)
+TB_INST_T(2, double)
+TB_INST_T(2, float)
+TB_INST_TB(3, double, 4)
+TB_INST_TB(3, float, 4)
+TB_INST_TB(2, double, 8)
+TB_INST_TB(2, float, 8)
+TB_INST_TB(2, double, 4)
+TB_INST_TB(2, float, 4)
+
+}  // namespace tb

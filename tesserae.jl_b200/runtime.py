@@ -1,0 +1,152 @@
+"""Device API: the reference's hot-path verbs on torch device arrays, through the
+C ABI of libtesserae_b200.so.
+
+  update(weights, particles, mesh, params)      update!(weights, particles, mesh)      basis_weight.jl:714
+  update(partition, particles, mesh, ctx)       update!(partition, particles.x)         gpu_block_strategy.jl:142
+  P2G(grid, particles, partition, mesh, params) @P2G (m, mv, f sums + grid half)        p2g.jl:66, gpu.jl:196
+  G2P(grid, particles, mesh, params)            @G2P (FLIP/APIC + Neo-Hookean)          g2p.jl:71, gpu.jl:226
+  step(...)                                     the whole README.md:66-87 loop body, n times
+
+The precision form follows the particle dtype: float64 -> the plain `_f64`
+entry points, float32 (F float64) -> the mixed `_f32` ones. Every call raises
+RuntimeError with the library's message on a non-zero status; there is no
+fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .state import BasisWeights, CartesianMesh, Grid, Particles, Partition
+
+
+def _suffix(dtype) -> str:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return "f64"
+    if dt == np.float32:
+        return "f32"
+    raise TypeError(f"unsupported scalar type {dt}")
+
+
+class Context:
+    """A tb_ctx bound to one device and stream (default: torch's current stream)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+        self.lib = _abi.load_library()
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream or 0)
+        self.ptr = self.lib.tb_create(int(device), C.c_void_p(handle))
+        if not self.ptr:
+            raise RuntimeError("tb_create failed (no CUDA device?)")
+        self.device = device
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.lib.tb_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int, what: str):
+        if rc != _abi.TB_OK:
+            msg = self.lib.tb_last_error(self.ptr)
+            raise RuntimeError(f"{what}: status {rc}: {msg.decode() if msg else ''}")
+
+    def synchronize(self):
+        self.check(self.lib.tb_synchronize(self.ptr), "tb_synchronize")
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.tb_launch_count(self.ptr))
+
+    def fn(self, name: str, dtype):
+        return getattr(self.lib, f"{name}_{_suffix(dtype)}")
+
+
+def _ref(s):
+    return C.byref(s)
+
+
+def update(target, particles: Particles, mesh: CartesianMesh, params=None, ctx: Context | None = None):
+    """update!(weights, particles, mesh) or update!(partition, particles.x)."""
+    ctx = ctx or _default()
+    if isinstance(target, BasisWeights):
+        if params is None:
+            raise ValueError("update(weights, ...) needs step params (basis kind, uGIMP length)")
+        rc = ctx.fn("tb_update_weights", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                          _ref(params), _ref(target.struct()))
+        ctx.check(rc, "update!(weights)")
+        return target
+    if isinstance(target, Partition):
+        na, nass = C.c_int64(), C.c_int64()
+        rc = ctx.fn("tb_bin_particles", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                         _ref(target.struct()), C.byref(na), C.byref(nass))
+        ctx.check(rc, "update!(partition)")
+        target.nactive, target.nassigned = na.value, nass.value
+        return target
+    raise TypeError(f"update: unsupported target {type(target).__name__}")
+
+
+def P2G(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+        grid_half: bool = True, ctx: Context | None = None):
+    """The recognised @P2G body: m = sum w m_p, mv = sum w m_p v_p (APIC: + B D^-1 (x_i - x_p)),
+    f = sum -V sigma grad w + w m_p g; with `grid_half`, vn = mv/m and v = vn + dt f/m."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_p2g", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                           _ref(partition.struct()), _ref(grid.struct()), _ref(params))
+    ctx.check(rc, "@P2G")
+    if grid_half:
+        rc = ctx.fn("tb_grid_update", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(grid.struct()),
+                                                       _ref(params))
+        ctx.check(rc, "@P2G grid half")
+    return grid
+
+
+def G2P(grid: Grid, particles: Particles, mesh: CartesianMesh, params, ctx: Context | None = None):
+    """The recognised @G2P body (README.md:79-86 / APIC)."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_g2p", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(grid.struct()),
+                                           _ref(particles.struct()), _ref(params))
+    ctx.check(rc, "@G2P")
+    return particles
+
+
+def step(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params, nsteps: int = 1,
+         ctx: Context | None = None):
+    """`nsteps` fused steps (bin -> P2G -> grid update -> G2P) without host sync."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_step", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                            _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                            int(nsteps))
+    ctx.check(rc, "step")
+
+
+def rollout_host(particles: Particles, mesh: CartesianMesh, params, nsteps: int, ctx: Context | None = None):
+    """Host-buffer rollout: `particles` holds numpy arrays; state is copied in,
+    advanced `nsteps` steps on the device and copied back (synchronous)."""
+    ctx = ctx or _default()
+    if particles.backend != "numpy":
+        raise TypeError("rollout_host takes host (numpy) particles")
+    rc = ctx.fn("tb_rollout_host", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                    _ref(params), int(nsteps))
+    ctx.check(rc, "rollout_host")
+
+
+_ctx = None
+
+
+def _default() -> Context:
+    global _ctx
+    if _ctx is None:
+        _ctx = Context()
+    return _ctx

@@ -1,0 +1,206 @@
+"""Seeded synthetic scenes for the five workloads of the explicit MPM path.
+
+Every scene is generated on the host in FP64 with numpy's PCG64 generator from a
+fixed seed, using the reference's GridSampling rule (src/particles.jl:9-16,
+26-31: points at xmin + l/2 + k*l with l = spacing*h, kept in column-major
+order, then filtered). No public dataset is involved.
+
+Scenes:
+  readme2d   2D two-disk collision of README.md:44-96 (100x100 cells, ~10k particles)
+  cube3d     3D unit cube 256^3, centre cube of side 0.5, 2^3 per cell (16 777 216 particles)
+  clusters3d 3D 512^3, 64 Gaussian clusters, lognormal masses (32M particles)
+  sphere3d   3D 64^3 sphere r=0.3, jittered 4^3 per cell (the differentiable rollout)
+  dambreak3d 3D 384^3 column [0,0.4]x[0,1]x[0,0.8], 2^3 per cell, WLS(uGIMP) + APIC fluid
+Each takes a `scale` that shrinks the mesh (cells per axis divided by `scale`,
+spacing kept) so tests run the same physics at sizes the oracle finishes fast.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from .state import CartesianMesh, Particles, lame, step_params
+
+SEEDS = {"readme2d": 0, "cube3d": 20260001, "clusters3d": 20260002, "sphere3d": 20260003,
+         "dambreak3d": 20260004}
+
+
+@dataclass
+class Scene:
+    name: str
+    mesh: CartesianMesh
+    particles: Particles          # host FP64
+    params: _abi.tb_step_params
+    nsteps: int
+    meta: dict
+
+
+def grid_sampling_axis(xmin: float, xmax: float, h: float, spacing: float = 0.5) -> np.ndarray:
+    """Axis of GridSampling points: (xmin + l/2):l:xmax with l = spacing*h."""
+    l = spacing * h
+    n = int(np.floor((xmax - (xmin + l / 2)) / l + 1e-9)) + 1
+    return xmin + (2.0 * np.arange(n) + 1.0) * (l / 2.0)
+
+
+def _lattice(axes: list[np.ndarray]) -> np.ndarray:
+    """Column-major (first axis fastest) lattice points, shape (dim, n)."""
+    grids = np.meshgrid(*axes, indexing="ij")
+    return np.stack([g.reshape(-1, order="F") for g in grids])
+
+
+def readme2d(scale: int = 1) -> Scene:
+    """README.md:44-96: unit square, h = 0.01, two disks r = 0.2, E = 500, nu = 0.3,
+    rho0 = 1e3, dt = 1e-3; V0 = volume / N before the disk filter (README.md:57)."""
+    h = 0.01
+    L = 1.0 / scale
+    mesh = CartesianMesh(h, (0.0, L), (0.0, L))
+    ax = grid_sampling_axis(0.0, L, h)
+    pts = _lattice([ax, ax])
+    npre = pts.shape[1]
+    V0 = (L * L) / npre
+    rho0, E, nu = 1e3, 500.0, 0.3
+    r = 0.2 * L
+    keep = (np.hypot(pts[0] - r, pts[1] - r) < r) | (np.hypot(pts[0] - (L - r), pts[1] - (L - r)) < r)
+    pts = pts[:, keep]
+    n = pts.shape[1]
+    P = Particles(n, 2, np.float64)
+    P.x[...] = pts
+    s = np.where(pts[0] > 0.5 * L, -0.1, 0.1)
+    P.v[0] = s
+    P.v[1] = s
+    P.V[...] = V0
+    mu, lam = lame(E, nu)
+    prm = step_params(1e-3, mass=rho0 * V0, V0=V0, mu=mu, lam=lam)
+    return Scene("readme2d", mesh, P, prm, 1000, {"n_before_filter": npre, "E": E, "nu": nu, "rho0": rho0})
+
+
+def cube3d(scale: int = 1, seed: int | None = None) -> Scene:
+    """Unit cube 256^3 cells (h = 1/256), centre cube [1/4, 3/4]^3 at 2 particles
+    per cell per axis, v ~ U[-0.5, 0.5]^3, Neo-Hookean E = 1e6, nu = 0.3,
+    rho0 = 1e3, gravity -9.81 z, 100 steps. The stated dt = 1e-4 puts the P-wave
+    CFL number c dt / h at 0.94 (c = sqrt((lambda + 2 mu) / rho0) = 36.7 m/s), and the
+    FP64 oracle goes to NaN within 20 steps; dt = 5e-5 (CFL 0.47) is used instead."""
+    cells = 256 // scale
+    h = 1.0 / 256
+    L = cells * h
+    mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
+    lpart = h / 2
+    k = np.arange(cells // 2, 3 * cells // 2)  # particles per axis inside [L/4, 3L/4]
+    ax = (2.0 * k + 1.0) * (lpart / 2.0)
+    pts = _lattice([ax, ax, ax])
+    n = pts.shape[1]
+    rng = np.random.default_rng(SEEDS["cube3d"] if seed is None else seed)
+    P = Particles(n, 3, np.float64)
+    P.x[...] = pts
+    P.v[...] = rng.uniform(-0.5, 0.5, size=(3, n))
+    V0 = lpart ** 3
+    P.V[...] = V0
+    rho0, E, nu = 1e3, 1e6, 0.3
+    mu, lam = lame(E, nu)
+    prm = step_params(5e-5, mass=rho0 * V0, V0=V0, mu=mu, lam=lam, gravity=(0.0, 0.0, -9.81))
+    return Scene("cube3d", mesh, P, prm, 100, {"E": E, "nu": nu, "rho0": rho0, "cells": cells})
+
+
+def _sort_by_block(mesh: CartesianMesh, pts: np.ndarray) -> np.ndarray:
+    """Stable order by reference block id: the particle order `reorder_particles!`
+    establishes (src/Parallel/gpu_block_strategy.jl:173-238)."""
+    L = mesh.block_size_log2
+    nb = mesh.nblocks()
+    b = np.zeros(pts.shape[1], dtype=np.int64)
+    for d in reversed(range(mesh.dim)):
+        c = np.floor((pts[d] - mesh.xmin[d]) * mesh.h_inv).astype(np.int64) >> L
+        b = b * nb[d] + np.clip(c, 0, nb[d] - 1)
+    return np.argsort(b, kind="stable")
+
+
+def clusters3d(scale: int = 1, n_total: int = 32 * 1024 * 1024, seed: int | None = None) -> Scene:
+    """512^3 cells (h = 1/512), n_total particles from 64 Gaussian clusters
+    (sigma = 0.02, centres U[0.2, 0.8]^3), masses rho0 V0 lognormal(0, 0.5),
+    Neo-Hookean E = 1e5, nu = 0.35, 50 steps. Points outside [0.01, 0.99]^3 of the
+    (scaled) domain are redrawn. Particles are stored block-ordered."""
+    cells = 512 // scale
+    h = 1.0 / 512
+    L = cells * h
+    mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
+    rng = np.random.default_rng(SEEDS["clusters3d"] if seed is None else seed)
+    n = n_total // (scale ** 3)
+    centres = rng.uniform(0.2 * L, 0.8 * L, size=(64, 3))
+    which = rng.integers(0, 64, size=n)
+    sig = 0.02 * L
+    pts = centres[which].T + rng.normal(0.0, sig, size=(3, n))
+    redrawn = 0
+    while True:
+        bad = np.any((pts < 0.01 * L) | (pts > 0.99 * L), axis=0)
+        nbad = int(bad.sum())
+        if nbad == 0:
+            break
+        redrawn += nbad
+        pts[:, bad] = centres[which[bad]].T + rng.normal(0.0, sig, size=(3, nbad))
+    order = _sort_by_block(mesh, pts)
+    pts = pts[:, order]
+    P = Particles(n, 3, np.float64, optional=("m",))
+    P.x[...] = pts
+    V0 = (h / 2) ** 3
+    rho0, E, nu = 1e3, 1e5, 0.35
+    P.m[...] = rho0 * V0 * rng.lognormal(0.0, 0.5, size=n)
+    P.V[...] = V0
+    mu, lam = lame(E, nu)
+    prm = step_params(5e-5, mass=rho0 * V0, V0=V0, mu=mu, lam=lam, gravity=(0.0, 0.0, -9.81))
+    return Scene("clusters3d", mesh, P, prm, 50, {"E": E, "nu": nu, "rho0": rho0, "redrawn": redrawn})
+
+
+def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
+    """64^3 cells (h = 1/64), sphere r = 0.3 at (0.5, 0.5, 0.5), 4 particles per cell
+    per axis on a lattice jittered by U[-l/4, l/4], per-particle log E = log(1e5) +
+    N(0, 0.1), nu = 0.3, rho0 = 1e3, dt = 5e-4, 200 steps."""
+    cells = 64 // scale
+    h = 1.0 / 64
+    L = cells * h
+    mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
+    rng = np.random.default_rng(SEEDS["sphere3d"] if seed is None else seed)
+    ax = grid_sampling_axis(0.0, L, h, spacing=0.25)
+    pts = _lattice([ax, ax, ax])
+    c, r = 0.5 * L, 0.3 * L
+    keep = np.sum((pts - c) ** 2, axis=0) < r * r
+    pts = pts[:, keep]
+    lp = h / 4
+    pts = pts + rng.uniform(-lp / 4, lp / 4, size=pts.shape)
+    n = pts.shape[1]
+    P = Particles(n, 3, np.float64, optional=("mu", "lam"))
+    P.x[...] = pts
+    V0 = lp ** 3
+    P.V[...] = V0
+    logE = np.log(1e5) + rng.normal(0.0, 0.1, size=n)
+    mu, lam = lame(np.exp(logE), 0.3)
+    P.mu[...] = mu
+    P.lam[...] = lam
+    prm = step_params(5e-4, mass=1e3 * V0, V0=V0, mu=float(np.mean(mu)), lam=float(np.mean(lam)))
+    return Scene("sphere3d", mesh, P, prm, 200, {"nu": 0.3, "rho0": 1e3, "target": (0.5 * L, 0.5 * L, 0.8 * L)})
+
+
+def dambreak3d(scale: int = 1) -> Scene:
+    """384^3 cells (h = 1/384), column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell,
+    weakly compressible fluid p = -K (J - 1) with K = 2e6, rho0 = 1e3, WLS(uGIMP)
+    basis with l = h/2, APIC transfer, slip walls on every face, dt = 5e-5, 100 steps."""
+    cells = 384 // scale
+    h = 1.0 / 384
+    L = cells * h
+    mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
+    axx = grid_sampling_axis(0.0, L, h)
+    pts = _lattice([axx[axx < 0.4 * L], axx, axx[axx < 0.8 * L]])
+    n = pts.shape[1]
+    P = Particles(n, 3, np.float64, optional=("B",))
+    P.x[...] = pts
+    V0 = (h / 2) ** 3
+    P.V[...] = V0
+    K = 2e6
+    prm = step_params(5e-5, mass=1e3 * V0, V0=V0, mu=0.0, lam=K, gravity=(0.0, 0.0, -9.81),
+                      gimp_l=h / 2, basis=_abi.TB_WLS_UGIMP, transfer=_abi.TB_TRANSFER_APIC,
+                      material=_abi.MATERIAL_FLUID, wall_mask=0b111111, wall_layers=2)
+    return Scene("dambreak3d", mesh, P, prm, 100, {"K": K, "rho0": 1e3})
+
+
+SCENES = {"readme2d": readme2d, "cube3d": cube3d, "clusters3d": clusters3d, "sphere3d": sphere3d,
+          "dambreak3d": dambreak3d}

@@ -1,0 +1,339 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Binning is compared bit for bit; floating-point fields within the tolerances
+written in each test: FP64 to 1e-12 of the field's scale per kernel (1e-9 after
+several steps), FP32 per kernel to 1e-5 of the scale, and the FP32 rollout to
+1e-5 relative L2 against the FP64 oracle on displacement and velocity.
+"""
+import numpy as np
+import pytest
+
+from helpers import basis_kind, max_rel, reference_partition, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(P):
+    return P.to("torch", device="cuda")
+
+
+def host(P):
+    return P.to("numpy")
+
+
+def bin_both(tb, oracle, ctx, mesh, P):
+    from tesserae_b200 import runtime
+    n = P.n
+    part_o = tb.Partition(mesh, n)
+    na_o, nass_o = oracle.bin(mesh, P, part_o)
+    Pd = dev(P)
+    part_d = tb.Partition(mesh, n, backend="torch", device="cuda")
+    runtime.update(part_d, Pd, mesh, ctx=ctx)
+    return part_o, part_d, (na_o, nass_o)
+
+
+def assert_same_partition(part_o, part_d, totals):
+    na, nass = totals
+    d = part_d.numpy()
+    assert (part_d.nactive, part_d.nassigned) == (na, nass)
+    assert np.array_equal(d["blockids"], part_o.blockids)
+    assert np.array_equal(d["counts"], part_o.counts)
+    assert np.array_equal(d["offsets"], part_o.offsets)
+    assert np.array_equal(d["blocklist"][:na], part_o.blocklist[:na])
+    assert np.array_equal(d["particleindices"][:nass], part_o.particleindices[:nass])
+
+
+# ---------------------------------------------------------------------------
+# binning: bit-exact
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_bin_cube(tb, oracle, ctx, dtype):
+    sc = tb.scenes.cube3d(scale=8)
+    P = sc.particles.to("numpy", dtype=dtype)
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, sc.mesh, P)
+    assert_same_partition(part_o, part_d, tot)
+    bid, counts, offsets, blocklist, perm = reference_partition(sc.mesh, P.x)
+    assert np.array_equal(part_o.particleindices[:tot[1]], perm)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_bin_random_with_outside(tb, oracle, ctx, dtype):
+    rng = np.random.default_rng(7)
+    mesh = tb.CartesianMesh(1 / 64, (0.0, 1.0), (0.0, 0.5), (0.0, 0.75))
+    n = 200_003
+    P = tb.Particles(n, 3, dtype)
+    P.x[...] = rng.uniform(-0.05, 1.05, size=(3, n)).astype(dtype)
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, mesh, P)
+    assert tot[1] < n  # some particles are outside
+    assert_same_partition(part_o, part_d, tot)
+
+
+@pytest.mark.parametrize("count", [1500, 70_000, 100_000])
+def test_bin_one_crowded_block(tb, oracle, ctx, count):
+    """Shuffled particles crowded into one block: every warp (32 consecutive ids)
+    contributes one run to it, so the fix-up sorts ~n/32 runs: in shared memory
+    up to 2048 runs, in the block's global scratch region above that."""
+    rng = np.random.default_rng(count)
+    mesh = tb.CartesianMesh(1 / 32, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    n = count + 5000
+    P = tb.Particles(n, 3)
+    P.x[...] = rng.uniform(0.0, 1.0, size=(3, n))
+    P.x[:, :count] = rng.uniform(4 / 32, 8 / 32 - 1e-9, size=(3, count))  # block (2,2,2)
+    perm = rng.permutation(n)
+    P.x[...] = P.x[:, perm]
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, mesh, P)
+    assert_same_partition(part_o, part_d, tot)
+    assert part_o.counts.max() >= count
+
+
+def test_bin_2d_and_empty(tb, oracle, ctx):
+    sc = tb.scenes.readme2d()
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, sc.mesh, sc.particles)
+    assert_same_partition(part_o, part_d, tot)
+    P0 = tb.Particles(0, 3)
+    mesh = tb.CartesianMesh(0.25, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, mesh, P0)
+    assert tot == (0, 0) and part_d.nactive == 0 and part_d.nassigned == 0
+    Pout = tb.Particles(100, 3)
+    Pout.x[...] = 5.0
+    part_o, part_d, tot = bin_both(tb, oracle, ctx, mesh, Pout)
+    assert tot == (0, 0)
+    assert np.all(part_d.numpy()["blockids"] == 0)
+
+
+# ---------------------------------------------------------------------------
+# basis weights
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("basis", ["bspline_quadratic", "ugimp", "wls_bspline_quadratic", "wls_ugimp"])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 2e-5)])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_update_weights(tb, oracle, ctx, basis, dtype, tol, dim):
+    from tesserae_b200 import runtime
+    rng = np.random.default_rng(11)
+    mesh = tb.CartesianMesh(0.1, *[(0.0, 1.0)] * dim)
+    n = 4000
+    P = tb.Particles(n, dim, dtype)
+    P.x[...] = rng.uniform(-0.02, 1.02, size=(dim, n)).astype(dtype)  # interior, boundary and outside
+    prm = tb.step_params(1.0, gimp_l=0.05, basis=basis_kind(tb._abi, basis))
+    Wo = tb.generate_basis_weights(dim, n, dtype)
+    oracle.update_weights(mesh, P, prm, Wo)
+    Wd = tb.generate_basis_weights(dim, n, dtype, backend="torch", device="cuda")
+    runtime.update(Wd, dev(P), mesh, prm, ctx=ctx)
+    ctx.synchronize()
+    assert np.array_equal(Wd.window.cpu().numpy(), Wo.window)
+    scale_w = np.abs(Wo.w).max()
+    scale_g = np.abs(Wo.grad_w).max()
+    assert np.max(np.abs(Wd.w.cpu().numpy() - Wo.w)) <= tol * scale_w
+    assert np.max(np.abs(Wd.grad_w.cpu().numpy() - Wo.grad_w)) <= tol * scale_g
+
+
+# ---------------------------------------------------------------------------
+# P2G / grid update / G2P
+# ---------------------------------------------------------------------------
+
+def small_scene(tb, name, dtype):
+    if name == "cube":
+        sc = tb.scenes.cube3d(scale=8)
+    elif name == "readme2d":
+        sc = tb.scenes.readme2d()
+    elif name == "clusters":
+        sc = tb.scenes.clusters3d(scale=8)
+    elif name == "dambreak":
+        sc = tb.scenes.dambreak3d(scale=8)
+    elif name == "sphere":
+        sc = tb.scenes.sphere3d(scale=2)
+    else:
+        raise ValueError(name)
+    P = sc.particles
+    rng = np.random.default_rng(5)
+    # Non-trivial stress, velocity gradient and APIC matrix so every term is exercised.
+    D = P.dim
+    P.sigma[...] = rng.normal(0.0, 1e3, size=P.sigma.shape)
+    if P.B is not None:
+        P.B[...] = rng.normal(0.0, 0.5, size=P.B.shape)
+    if name == "readme2d":
+        pass
+    return sc, P.to("numpy", dtype=dtype)
+
+
+def grid_fields(G):
+    g = G.numpy() if not isinstance(G.m, np.ndarray) else {k: getattr(G, k) for k in ("m", "mv", "f", "v", "vn")}
+    return g
+
+
+SCENES = ["cube", "readme2d", "clusters", "dambreak", "sphere"]
+
+
+@pytest.mark.parametrize("name", SCENES)
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_p2g(tb, oracle, ctx, name, dtype, tol):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, name, dtype)
+    mesh, prm = sc.mesh, sc.params
+    Go = tb.generate_grid(mesh, dtype)
+    oracle.p2g(mesh, P, Go, prm)
+    Pd = dev(P)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    runtime.update(part, Pd, mesh, ctx=ctx)
+    Gd = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+    runtime.P2G(Gd, Pd, part, mesh, prm, grid_half=False, ctx=ctx)
+    ctx.synchronize()
+    g = Gd.numpy()
+    for k in ("m", "mv", "f"):
+        ref = getattr(Go, k)
+        scale = np.abs(ref).max()
+        if scale == 0:
+            assert np.abs(g[k]).max() == 0, k
+            continue
+        err = np.max(np.abs(g[k] - ref)) / scale
+        assert err <= tol, (k, err)
+    if name in ("cube", "clusters", "sphere"):
+        # no particle near the mesh boundary: every window is full, so the
+        # partition of unity makes P2G conserve mass up to rounding
+        mass = (P.m.astype(np.float64).sum() if P.m is not None else P.n * prm.mass)
+        assert abs(g["m"].sum(dtype=np.float64) - mass) <= 10 * tol * mass
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_grid_update_bitexact(tb, oracle, ctx, dtype):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", dtype)
+    mesh = sc.mesh
+    prm = sc.params
+    prm.wall_mask = 0b100111
+    prm.wall_layers = 3
+    Go = tb.generate_grid(mesh, dtype)
+    oracle.p2g(mesh, P, Go, prm)
+    Gd = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+    for k in ("m", "mv", "f"):
+        getattr(Gd, k).copy_(torch.from_numpy(getattr(Go, k)))
+    oracle.grid_update(mesh, Go, prm)
+    lib = ctx.fn("tb_grid_update", dtype)
+    import ctypes
+    ctx.check(lib(ctx.ptr, ctypes.byref(mesh.struct()), ctypes.byref(Gd.struct()), ctypes.byref(prm)), "grid")
+    ctx.synchronize()
+    g = Gd.numpy()
+    assert np.array_equal(g["v"], Go.v) and np.array_equal(g["vn"], Go.vn)
+
+
+@pytest.mark.parametrize("name", SCENES)
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_g2p_direct(tb, oracle, ctx, name, dtype, tol):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, name, dtype)
+    mesh, prm = sc.mesh, sc.params
+    Go = tb.generate_grid(mesh, dtype)
+    oracle.p2g(mesh, P, Go, prm)
+    oracle.grid_update(mesh, Go, prm)
+    Gd = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+    for k in ("m", "mv", "f", "v", "vn"):
+        getattr(Gd, k).copy_(torch.from_numpy(getattr(Go, k)))
+    Pd = dev(P)
+    oracle.g2p(mesh, Go, P, prm)
+    runtime.G2P(Gd, Pd, mesh, prm, ctx=ctx)
+    ctx.synchronize()
+    got = Pd.numpy()
+    ref = P.numpy()
+    for k in ("x", "v", "grad_v", "F", "sigma", "V") + (("B",) if P.B is not None else ()):
+        scale = np.abs(ref[k]).max()
+        if scale == 0:
+            assert np.abs(got[k]).max() == 0, k
+            continue
+        err = np.max(np.abs(got[k] - ref[k])) / scale
+        assert err <= (tol if k not in ("sigma",) else 50 * tol), (k, err)
+
+
+@pytest.mark.parametrize("name,nsteps", [("cube", 10), ("readme2d", 20), ("dambreak", 5), ("sphere", 10),
+                                         ("clusters", 5)])
+def test_step_fp64(tb, oracle, ctx, name, nsteps):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, name, np.float64)
+    P.sigma[...] = 0.0  # start from the scene's natural (stress-free, B = 0) state
+    if P.B is not None:
+        P.B[...] = 0.0
+    mesh, prm = sc.mesh, sc.params
+    Pd = dev(P)
+    Go = tb.generate_grid(mesh)
+    oracle.step(mesh, P, Go, prm, nsteps)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, backend="torch", device="cuda")
+    runtime.step(Gd, Pd, part, mesh, prm, nsteps, ctx=ctx)
+    ctx.synchronize()
+    got, ref = Pd.numpy(), P.numpy()
+    for k in ("x", "v", "F", "V"):
+        assert rel_l2(got[k], ref[k]) <= 1e-9, k
+    g = Gd.numpy()
+    for k in ("m", "mv", "v"):
+        assert rel_l2(g[k], getattr(Go, k)) <= 1e-9, k
+
+
+def test_step_fp32_vs_fp64_oracle(tb, oracle, ctx):
+    """The mixed FP32 form after 100 steps against the FP64 oracle: relative L2
+    error of the state (positions, velocities) <= 1e-5. Displacements are held to
+    1e-3 only: FP32 positions near 0.5 round at ulp = 6e-8 every step, against
+    ~2.5e-3 of total displacement."""
+    from tesserae_b200 import runtime
+    sc = tb.scenes.cube3d(scale=8)
+    mesh, prm = sc.mesh, sc.params
+    P64 = sc.particles
+    x0 = P64.x.copy()
+    P32 = dev(P64.to("numpy", dtype=np.float32))
+    Go = tb.generate_grid(mesh)
+    oracle.step(mesh, P64, Go, prm, 100)
+    part = tb.Partition(mesh, P64.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+    runtime.step(Gd, P32, part, mesh, prm, 100, ctx=ctx)
+    ctx.synchronize()
+    got = P32.numpy()
+    err_x = rel_l2(got["x"], P64.x)
+    err_v = rel_l2(got["v"], P64.v)
+    err_u = rel_l2(got["x"].astype(np.float64) - x0, P64.x - x0)
+    assert err_x <= 1e-5 and err_v <= 1e-5, (err_x, err_v)
+    assert err_u <= 1e-3, err_u
+
+
+def test_rollout_host_matches_device_step(tb, ctx):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", np.float32)
+    P.sigma[...] = 0.0
+    mesh, prm = sc.mesh, sc.params
+    Pd = dev(P)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+    runtime.step(Gd, Pd, part, mesh, prm, 3, ctx=ctx)
+    ctx.synchronize()
+    runtime.rollout_host(P, mesh, prm, 3, ctx=ctx)
+    got = Pd.numpy()
+    for k in ("x", "v", "F", "sigma", "V"):
+        assert rel_l2(getattr(P, k), got[k]) <= 1e-6, k
+
+
+def test_error_statuses(tb, ctx):
+    """Argument errors come back as status codes with a message (no fault)."""
+    import ctypes
+    from tesserae_b200 import runtime
+    mesh = tb.CartesianMesh(0.25, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    P = dev(tb.Particles(10, 3))
+    part = tb.Partition(mesh, 10, backend="torch", device="cuda")
+    bad = part.struct()
+    bad.nblocks = 7
+    rc = ctx.lib.tb_bin_particles_f64(ctx.ptr, ctypes.byref(mesh.struct()), ctypes.byref(P.struct()),
+                                      ctypes.byref(bad), None, None)
+    assert rc == tb._abi.TB_ERR_ARG and b"nblocks" in ctx.lib.tb_last_error(ctx.ptr)
+    m1 = mesh.struct()
+    m1.dim = 1
+    rc = ctx.lib.tb_bin_particles_f64(ctx.ptr, ctypes.byref(m1), ctypes.byref(P.struct()),
+                                      ctypes.byref(part.struct()), None, None)
+    assert rc == tb._abi.TB_ERR_UNSUPPORTED
+    # uGIMP length beyond the spacing is reported by the kernel's status word
+    prm = tb.step_params(1.0, gimp_l=0.3, basis=tb._abi.TB_UGIMP)
+    P.x.fill_(0.5)
+    W = tb.generate_basis_weights(3, 10, backend="torch", device="cuda")
+    runtime.update(W, P, mesh, prm, ctx=ctx)
+    with pytest.raises(RuntimeError, match="uGIMP"):
+        ctx.synchronize()
+    ctx.synchronize()  # status cleared
