@@ -1,0 +1,375 @@
+"""Benchmark of the explicit MPM step (bin -> P2G -> grid update -> G2P).
+
+Workload: the 3D cube scene (unit cube 256^3 cells, centre cube of side 0.5 at
+2^3 particles per cell = 16 777 216 particles, Neo-Hookean E = 1e6, nu = 0.3,
+gravity), seeded synthetic data. One bench "step" = one MPM step over all
+particles. The headline form is the mixed FP32 step (FP32 state, FP64 F/J/log J,
+FP64-accumulated P2G tiles); the plain FP64 step is measured beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). N > 1 (torchrun): every rank runs its own
+replica of the workload (weak scaling, no data exchange); time = max over ranks.
+`--impl reference` times the reference's CPU algorithm (the OpenMP restatement
+in oracle/, FP64, all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+METRIC = "particle-steps/s, 1 B200: FP32 fused vs FP64 plain @<=1e-5 rel err; adj/fwd"
+
+
+def load_package():
+    if "tesserae_b200" in sys.modules:
+        return sys.modules["tesserae_b200"]
+    pkg = ROOT / "tesserae.jl_b200"
+    spec = importlib.util.spec_from_file_location("tesserae_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["tesserae_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle(tb):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as oracle_mod  # noqa: E402  (CPU baseline / reference arm only)
+    return oracle_mod
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic bytes per particle and per active node of each kernel family,
+# mixed FP32 form (F FP64) and plain FP64 form: the scatter/gather reads and
+# writes of the reference's equations (weights evaluated in the kernels).
+def algorithmic_bytes(kind: str, dtype) -> tuple[int, int]:
+    s = np.dtype(dtype).itemsize
+    per_p = {
+        # x, v, V, sigma(6) read
+        "p2g": (3 + 3 + 1 + 6) * s,
+        # x, v, F(9 x 8) read; x, v, grad_v(9), F, sigma(6), V written
+        "g2p": (3 + 3) * s + 72 + (3 + 3 + 9 + 6 + 1) * s + 72,
+        # x read, block id written
+        "bin_count": 3 * s + 4,
+    }[kind]
+    per_n = {
+        "p2g": 7 * s,       # m, mv, f written once per active node
+        "g2p": 6 * s,       # v, vn read once per active node
+        "bin_count": 0,
+    }[kind]
+    return per_p, per_n
+
+
+def active_nodes(mesh, particles_np) -> int:
+    """Nodes inside the support of at least one particle (quadratic B-spline)."""
+    x = particles_np
+    n = mesh.n_nodes
+    lo = [np.floor((x[d] - mesh.xmin[d]) * mesh.h_inv - 0.5).astype(np.int64) for d in range(3)]
+    mask = np.zeros(n[::-1], dtype=bool)  # z, y, x
+    mins = [int(l.min()) for l in lo]
+    maxs = [int(l.max()) + 2 for l in lo]
+    # the cube scene fills a box of cells densely: the active nodes are that box
+    for d in range(3):
+        mins[d], maxs[d] = max(mins[d], 0), min(maxs[d], n[d] - 1)
+    mask[mins[2]:maxs[2] + 1, mins[1]:maxs[1] + 1, mins[0]:maxs[0] + 1] = True
+    return int(mask.sum())
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    tb = load_package()
+    om = load_oracle(tb)
+    oracle = om.Oracle(tb._abi)
+    sc = tb.scenes.cube3d(scale=args.scale)
+    mesh, prm = sc.mesh, sc.params
+    P = sc.particles
+    G = tb.generate_grid(mesh)
+    threads = om.cores()
+    for _ in range(args.warmup):
+        oracle.step_parallel(mesh, P, G, prm, 1, threads)
+    t0 = time.perf_counter()
+    phases = oracle.step_parallel(mesh, P, G, prm, args.steps, threads)
+    dt = time.perf_counter() - t0
+    value = P.n * args.steps / dt
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded cube3d scene)",
+        "config": {"workload": "cube3d: 256^3 cells, 16,777,216 particles, one MPM step per step",
+                   "n_particles": P.n, "scale": args.scale, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"full workload, {args.steps} MPM steps after {args.warmup} warm-up, FP64, "
+                                   "OpenMP colour-phased restatement of the reference CPU path",
+                         "phase_s": dict(zip(["bin", "p2g", "grid", "g2p"], phases))},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scale", type=int, default=1, help="shrink the cube scene (cells per axis / scale)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    tb = load_package()
+    from tesserae_b200 import runtime
+    ctx = runtime.Context(local)
+
+    sc = tb.scenes.cube3d(scale=args.scale)
+    mesh, prm = sc.mesh, sc.params
+    host64 = sc.particles
+    n = host64.n
+    x0 = host64.x.copy()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(P, G, part, K):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        l0 = ctx.launches
+        e0.record()
+        runtime.step(G, P, part, mesh, prm, K, ctx=ctx)
+        e1.record()
+        barrier()
+        return e0.elapsed_time(e1), ctx.launches - l0
+
+    results = {}
+    for name, dtype in (("f32", np.float32), ("f64", np.float64)):
+        P = host64.to("torch", device="cuda", dtype=dtype)
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, P, part, mesh, prm, args.warmup, ctx=ctx)
+        ctx.synchronize()
+        with ClockSampler(local) as clk:
+            ms, launches = timed_steps(P, G, part, args.steps)
+        ms = max_over_ranks(ms)
+        # per-kernel device time, profiled separately (events add launch gaps)
+        ctx.profile(True)
+        runtime.step(G, P, part, mesh, prm, 3, ctx=ctx)
+        kt = ctx.profile_read()
+        ctx.profile(False)
+        results[name] = {"ms": ms, "launches": launches, "kernels": kt, "clocks": clk.summary()}
+        del P, part, G
+        torch.cuda.empty_cache()
+
+    # FP32 vs FP64 after 100 steps of the same scene (both on the device).
+    acc = {}
+    Ps = {}
+    for name, dtype in (("f32", np.float32), ("f64", np.float64)):
+        P = host64.to("torch", device="cuda", dtype=dtype)
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, P, part, mesh, prm, sc.nsteps, ctx=ctx)
+        ctx.synchronize()
+        Ps[name] = {k: getattr(P, k).double().cpu().numpy() for k in ("x", "v")}
+        del P, part, G
+        torch.cuda.empty_cache()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    acc = {"steps": sc.nsteps, "rel_err_x": rel(Ps["f32"]["x"], Ps["f64"]["x"]),
+           "rel_err_v": rel(Ps["f32"]["v"], Ps["f64"]["v"]),
+           "rel_err_displacement": rel(Ps["f32"]["x"] - x0, Ps["f64"]["x"] - x0),
+           "against": "plain FP64 form on the device (parity-tested against the FP64 oracle)"}
+    del Ps
+
+    # End to end through the host-buffer C-ABI call: pinned host state in,
+    # S MPM steps, state out, every call.
+    S = 10
+    calls = max(2, args.steps // S)
+    hostp = host64.to("pinned", dtype=np.float32)
+    runtime.rollout_host(hostp, mesh, prm, S, ctx=ctx)  # allocates the context's device state
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        runtime.rollout_host(hostp, mesh, prm, S, ctx=ctx)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    fbytes = hostp.x.nbytes + hostp.v.nbytes + hostp.V.nbytes + hostp.grad_v.nbytes + hostp.sigma.nbytes + \
+        hostp.F.nbytes
+    e2e = {"value": world * n * S * calls / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": fbytes,
+           "d2h_bytes_per_step": fbytes, "mpm_steps_per_call": S,
+           "note": "one bench step = one tb_rollout_host_f32 call on pinned host buffers (H2D, S steps, D2H)"}
+    del hostp
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # Roofline of the dominant kernel (mixed FP32 form).
+    kt = results["f32"]["kernels"]
+    dom = max(("p2g", "g2p"), key=lambda k: kt.get(k, (0, 0.0))[1])
+    launches_dom, ms_dom = kt[dom]
+    per_p, per_n = algorithmic_bytes(dom, np.float32)
+    nact = active_nodes(mesh, host64.x)
+    alg_bytes = n * per_p + nact * per_n
+    achieved = alg_bytes / (ms_dom / launches_dom * 1e-3) / 1e9
+    peak, peak_src = measured_peaks()
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic_cube3d.json"
+    if tfile.exists():
+        tj = json.loads(tfile.read_text())
+        if dom in tj:
+            traffic = tj[dom]["dram_bytes_per_particle"] * n
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        om = load_oracle(tb)
+        oracle = om.Oracle(tb._abi)
+        cores = om.cores()
+        Pc = host64.to("numpy")
+        Gc = tb.generate_grid(mesh)
+        oracle.step_parallel(mesh, Pc, Gc, prm, 1, cores)
+        t0 = time.perf_counter()
+        nst = 2
+        oracle.step_parallel(mesh, Pc, Gc, prm, nst, cores)
+        dt = time.perf_counter() - t0
+        cpu = {"value": n * nst / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+               "sample": f"cube3d full workload ({n} particles), {nst} MPM steps after 1 warm-up, FP64 "
+                         "OpenMP colour-phased restatement of the reference CPU path"}
+
+    f32, f64 = results["f32"], results["f64"]
+    out = {
+        "metric": METRIC,
+        "value": world * n * args.steps / (f32["ms"] * 1e-3),
+        "unit": "particle-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": f32["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded cube3d scene, numpy PCG64)",
+        "config": {"workload": "cube3d: unit cube 256^3 cells, centre cube side 0.5 at 2^3 particles/cell, "
+                               "Neo-Hookean E=1e6 nu=0.3, gravity, dt=5e-5; one MPM step per bench step",
+                   "n_particles": n, "scale": args.scale, "form": "mixed FP32 (FP64 F, det F, log J; FP64 tiles)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (2.7 GB particle state per replica)"},
+        "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
+        "accuracy": acc,
+        "adjoint_over_forward": None,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_active_node": per_n,
+                     "active_nodes": nact},
+        "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(kt.items())},
+        "kernels_ms_per_step_f64": {k: v[1] / 3 for k, v in sorted(f64["kernels"].items())},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": f32["launches"],
+        "clocks": f32["clocks"],
+    }
+    print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

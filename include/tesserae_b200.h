@@ -14,8 +14,9 @@
  * Precision forms (the `_f64` / `_f32` suffix):
  *   _f64  "plain": every array is double. Drop-in for `gpu_preserve` data.
  *   _f32  "mixed": every array is float EXCEPT the deformation gradient F,
- *         which stays double; weights, P2G and G2P run in FP32, the P2G tile
- *         uses compensated (two-term) sums, and F update, det F and log J run in
+ *         which stays double; weights, P2G and G2P run in FP32, the P2G
+ *         shared-memory tiles accumulate the FP32 contributions in FP64
+ *         (compensated accumulation), and F update, det F and log J run in
  *         FP64. Drop-in for `gpu` (Float32-cast) data plus an FP64 F array.
  *
  * Index conventions follow the reference (Julia, column-major, 1-based):
@@ -156,6 +157,20 @@ int32_t tb_set_stream(tb_ctx* ctx, void* stream);
 int32_t tb_synchronize(tb_ctx* ctx);
 /* Number of this library's kernel launches issued through ctx so far. */
 int64_t tb_launch_count(const tb_ctx* ctx);
+
+/* Per-kernel device time: while enabled, every launch of this library through
+ * ctx is bracketed by CUDA events on ctx's stream (the per-phase timer table of
+ * the reference's tutorials, docs/literate/tutorials/taylor_impact.jl:107-185). */
+typedef struct tb_kernel_time {
+    char name[32];     /* kernel family: bin_count, bin_scan, bin_scatter, bin_fixup,
+                          grid_mark, grid_zero, p2g, grid_update, g2p, g2p_outside, ... */
+    int64_t launches;
+    double ms;         /* summed device time */
+} tb_kernel_time;
+int32_t tb_profile_enable(tb_ctx* ctx, int32_t on);
+/* Synchronises, writes up to `cap` entries accumulated since the last read,
+ * sets *count to the number of kernel families, and resets the totals. */
+int32_t tb_profile_read(tb_ctx* ctx, tb_kernel_time* out, int32_t cap, int32_t* count);
 
 /* ---- basis weights: update!(weights, particles, mesh) -----------------
  * reference: src/Basis/basis_weight.jl:714-752 (GPU kernel :686-689). */

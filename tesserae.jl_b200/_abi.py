@@ -98,6 +98,10 @@ class tb_step_params(C.Structure):
     ]
 
 
+class tb_kernel_time(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("ms", C.c_double)]
+
+
 P = C.POINTER
 I32 = C.c_int32
 I64 = C.c_int64
@@ -110,6 +114,8 @@ SIGNATURES = [
     ("tb_set_stream", I32, [VP, VP]),
     ("tb_synchronize", I32, [VP]),
     ("tb_launch_count", I64, [VP]),
+    ("tb_profile_enable", I32, [VP, I32]),
+    ("tb_profile_read", I32, [VP, P(tb_kernel_time), I32, P(I32)]),
 ]
 for _p in ("f64", "f32"):
     SIGNATURES += [

@@ -11,10 +11,63 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <map>
 
 #include "tb_launch.cuh"
 
 using namespace tb;
+
+// Per-kernel device timing (tb_profile_enable / tb_profile_read): one pair of
+// CUDA events on the launching stream around every launch of this library.
+struct EventProfiler final : tb::Profiler {
+    struct Span {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Span> spans;
+    const char* cur_name = nullptr;
+    cudaEvent_t cur_a = nullptr;
+    std::map<std::string, std::pair<long long, double>> totals;
+
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(const char* name, cudaStream_t s) override {
+        cur_name = name;
+        cur_a = get();
+        cudaEventRecord(cur_a, s);
+    }
+    void end(cudaStream_t s) override {
+        cudaEvent_t b = get();
+        cudaEventRecord(b, s);
+        spans.push_back({cur_name, cur_a, b});
+    }
+    void collect() {
+        for (auto& sp : spans) {
+            cudaEventSynchronize(sp.b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, sp.a, sp.b);
+            auto& t = totals[sp.name];
+            t.first += 1;
+            t.second += ms;
+            pool.push_back(sp.a);
+            pool.push_back(sp.b);
+        }
+        spans.clear();
+    }
+    ~EventProfiler() override {
+        collect();
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
 
 struct tb_ctx {
     int device = 0;
@@ -34,6 +87,15 @@ struct tb_ctx {
     long long partials_cap = 0;
     unsigned long long* sort_scratch = nullptr;
     long long sort_scratch_cap = 0;
+    // touched node blocks of the last two transfers (sparse grid zero/update)
+    unsigned char* touched_cur = nullptr;
+    unsigned char* touched_prev = nullptr;
+    long long touched_cap = 0;
+    const void* grid_key = nullptr;  // grid.m of the grid the flags describe
+    long long grid_nblocks = 0;
+    bool grid_sparse_ok = false;     // the flags describe every non-zero node of grid_key
+    bool grid_dense_pending = false; // last P2G zeroed densely: the next grid half runs densely too
+    EventProfiler* prof = nullptr;
     // context-owned state for tb_rollout_host_*
     void* roll_buf = nullptr;
     size_t roll_cap = 0;
@@ -188,7 +250,7 @@ int bin_buffers(tb_ctx* c, const tb_partition* part, long long n, long long nb, 
     return TB_OK;
 }
 
-LaunchCfg cfg_of(tb_ctx* c) { return LaunchCfg{c->stream, c->num_sms, &c->launches, c->d_err}; }
+LaunchCfg cfg_of(tb_ctx* c) { return LaunchCfg{c->stream, c->num_sms, &c->launches, c->d_err, c->prof}; }
 
 // Reads and clears the device status word (synchronises the stream).
 int check_device_status(tb_ctx* c) {
@@ -207,6 +269,57 @@ int check_device_status(tb_ctx* c) {
     return TB_OK;
 }
 
+int touched_buffers(tb_ctx* c, long long nb) {
+    cudaError_t e;
+    if (nb > c->touched_cap) {
+        long long cap = c->touched_cap;
+        if ((e = grow(c->touched_cur, cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched flags");
+        cap = c->touched_cap;
+        if ((e = grow(c->touched_prev, cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched flags");
+        c->touched_cap = nb;
+        c->grid_sparse_ok = false;
+    }
+    return TB_OK;
+}
+
+// Zero the P2G targets where this transfer adds, then scatter. The first
+// transfer of an ABI call zeroes every node of the grid (its content is the
+// caller's); the following steps of the same call zero only the node blocks
+// touched by this or the previous step, which are the only ones that can be
+// non-zero, so the grid matches the reference's dense fillzero!
+// (src/Core/zero.jl:100-106) at a fraction of the traffic. Nothing is cached
+// across calls: a later grid may reuse an earlier grid's address.
+template <int D, class T, int BW>
+cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G,
+                          const Scalars<T>& S, const BinBuffers& B, const LaunchCfg& cfg) {
+    const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks;
+    std::swap(c->touched_cur, c->touched_prev);
+    cudaError_t e = cudaMemsetAsync(c->touched_cur, 0, size_t(M.nblocks), cfg.stream);
+    if (e == cudaSuccess && !known) e = cudaMemsetAsync(c->touched_prev, 0, size_t(M.nblocks), cfg.stream);
+    if (e == cudaSuccess) e = launch_mark_touched(D, M.nb, B, c->touched_cur, M.nblocks, cfg);
+    if (e == cudaSuccess)
+        e = known ? launch_sparse_zero<D, T, BW>(M, G, c->touched_cur, c->touched_prev, cfg)
+                  : launch_grid_zero<D, T>(M, G, cfg);
+    if (e == cudaSuccess) e = launch_p2g<D, T, BW>(M, P, G, S, B, cfg);
+    c->grid_key = G.m;
+    c->grid_nblocks = M.nblocks;
+    c->grid_sparse_ok = (e == cudaSuccess);
+    c->grid_dense_pending = !known;
+    return e;
+}
+
+// Grid half: over the touched node blocks when the flags describe this grid
+// (zeroing v and vn of blocks touched only before), else over every node.
+template <int D, class T, int BW>
+cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& S,
+                                        const LaunchCfg& cfg) {
+    const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks &&
+                       !c->grid_dense_pending;
+    c->grid_dense_pending = false;
+    if (known) return launch_sparse_grid_update<D, T, BW>(M, G, S, c->touched_cur, c->touched_prev, cfg);
+    return launch_grid_update<D, T>(M, G, S, cfg);
+}
+
 template <int D, class T, int BW>
 int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
              const tb_step_params* prm, int nsteps, bool do_bin, bool do_p2g, bool do_grid, bool do_g2p) {
@@ -222,10 +335,12 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
     const LaunchCfg cfg = cfg_of(c);
     const T* xs[3] = {P.x[0], P.x[1], D == 3 ? P.x[2] : P.x[1]};
     cudaError_t e = cudaSuccess;
+    if ((do_p2g || do_grid) && (rc = touched_buffers(c, M.nblocks)) != TB_OK) return rc;
+    c->grid_sparse_ok = false;  // the first step of every call runs densely
     for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
         if (do_bin) e = launch_bin<D, T>(M, xs, P.n, B, cfg);
-        if (e == cudaSuccess && do_p2g) e = launch_p2g<D, T, BW>(M, P, G, S, B, cfg);
-        if (e == cudaSuccess && do_grid) e = launch_grid_update<D, T>(M, G, S, cfg);
+        if (e == cudaSuccess && do_p2g) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
+        if (e == cudaSuccess && do_grid) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
         if (e == cudaSuccess && do_g2p) e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
@@ -288,6 +403,25 @@ int do_weights(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step
                                         reinterpret_cast<long long*>(w->window), cfg);
     if (e != cudaSuccess) return cuda_fail(c, e, "update_weights launch");
     return TB_OK;
+}
+
+template <class T>
+int do_grid_update(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params* prm) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
+        return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e;
+    GView<T> G;
+    if ((rc = make_gview<T>(c, g, m->dim, G)) != TB_OK) return rc;
+    c->grid_sparse_ok = false;  // a standalone call cannot know which nodes are non-zero
+    if (m->dim == 3)
+        e = grid_update_sparse_or_dense<3, T, 4>(c, make_dmesh<3, T>(*m), G, make_scalars<T>(*prm), cfg);
+    else if (m->block_log2 == 3)
+        e = grid_update_sparse_or_dense<2, T, 8>(c, make_dmesh<2, T>(*m), G, make_scalars<T>(*prm), cfg);
+    else
+        e = grid_update_sparse_or_dense<2, T, 4>(c, make_dmesh<2, T>(*m), G, make_scalars<T>(*prm), cfg);
+    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "grid update launch");
 }
 
 template <class T>
@@ -466,6 +600,9 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->partials);
     cudaFree(c->sort_scratch);
     cudaFree(c->roll_buf);
+    cudaFree(c->touched_cur);
+    cudaFree(c->touched_prev);
+    delete c->prof;
     delete c;
 }
 
@@ -486,6 +623,39 @@ int32_t tb_synchronize(tb_ctx* c) {
 }
 
 int64_t tb_launch_count(const tb_ctx* c) { return c ? c->launches : 0; }
+
+int32_t tb_profile_enable(tb_ctx* c, int32_t on) {
+    int rc = check_ctx(c);
+    if (rc != TB_OK) return rc;
+    if (on && !c->prof) c->prof = new (std::nothrow) EventProfiler();
+    if (on && !c->prof) return fail(c, TB_ERR_ARG, "out of host memory");
+    if (!on && c->prof) {
+        delete c->prof;
+        c->prof = nullptr;
+    }
+    return TB_OK;
+}
+
+int32_t tb_profile_read(tb_ctx* c, tb_kernel_time* out, int32_t cap, int32_t* count) {
+    int rc = check_ctx(c);
+    if (rc != TB_OK) return rc;
+    if (!c->prof) return fail(c, TB_ERR_ARG, "profiling is not enabled");
+    if (cap < 0 || (cap > 0 && !out)) return fail(c, TB_ERR_ARG, "bad output buffer");
+    c->prof->collect();
+    int32_t k = 0;
+    for (auto& kv : c->prof->totals) {
+        if (k < cap) {
+            std::memset(out[k].name, 0, sizeof out[k].name);
+            std::strncpy(out[k].name, kv.first.c_str(), sizeof out[k].name - 1);
+            out[k].launches = kv.second.first;
+            out[k].ms = kv.second.second;
+        }
+        ++k;
+    }
+    if (count) *count = k;
+    c->prof->totals.clear();
+    return TB_OK;
+}
 
 int32_t tb_update_weights_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step_params* prm,
                               tb_weights* w) {
@@ -517,38 +687,10 @@ int32_t tb_p2g_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_
 }
 
 int32_t tb_grid_update_f64(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params* prm) {
-    int rc;
-    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
-        return rc;
-    const LaunchCfg cfg = cfg_of(c);
-    cudaError_t e;
-    if (m->dim == 3) {
-        GView<double> G;
-        if ((rc = make_gview<double>(c, g, 3, G)) != TB_OK) return rc;
-        e = launch_grid_update<3, double>(make_dmesh<3, double>(*m), G, make_scalars<double>(*prm), cfg);
-    } else {
-        GView<double> G;
-        if ((rc = make_gview<double>(c, g, 2, G)) != TB_OK) return rc;
-        e = launch_grid_update<2, double>(make_dmesh<2, double>(*m), G, make_scalars<double>(*prm), cfg);
-    }
-    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "grid update launch");
+    return do_grid_update<double>(c, m, g, prm);
 }
 int32_t tb_grid_update_f32(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params* prm) {
-    int rc;
-    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_params(c, prm)) != TB_OK)
-        return rc;
-    const LaunchCfg cfg = cfg_of(c);
-    cudaError_t e;
-    if (m->dim == 3) {
-        GView<float> G;
-        if ((rc = make_gview<float>(c, g, 3, G)) != TB_OK) return rc;
-        e = launch_grid_update<3, float>(make_dmesh<3, float>(*m), G, make_scalars<float>(*prm), cfg);
-    } else {
-        GView<float> G;
-        if ((rc = make_gview<float>(c, g, 2, G)) != TB_OK) return rc;
-        e = launch_grid_update<2, float>(make_dmesh<2, float>(*m), G, make_scalars<float>(*prm), cfg);
-    }
-    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "grid update launch");
+    return do_grid_update<float>(c, m, g, prm);
 }
 
 int32_t tb_g2p_f64(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p, const tb_step_params* prm) {

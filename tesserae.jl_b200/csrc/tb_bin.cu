@@ -268,6 +268,7 @@ cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long 
     cudaError_t e = cudaMemsetAsync(b.counts, 0, sizeof(int) * size_t(M.nblocks), cfg.stream);
     if (e != cudaSuccess) return e;
     if (n > 0) {
+        KernelScope ks(cfg, "bin_count");
         bin_count_kernel<D, T><<<grid_for(n, 256), 256, 0, cfg.stream>>>(M, x[0], x[1], D == 3 ? x[2] : x[1], n,
                                                                          b.blockids, b.counts);
         ++*cfg.launches;
@@ -277,14 +278,21 @@ cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long 
 
 cudaError_t launch_bin_rest(int nb, long long n, const BinBuffers& b, const LaunchCfg& cfg) {
     const int nt = scan_tiles(nb);
-    scan_reduce_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials);
-    scan_spine_kernel<<<1, 256, 0, cfg.stream>>>(b.partials, nt);
-    scan_finalize_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials, b.offsets, b.cursors, b.blocklist,
-                                                     b.totals);
+    {
+        KernelScope ks(cfg, "bin_scan");
+        scan_reduce_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials);
+        scan_spine_kernel<<<1, 256, 0, cfg.stream>>>(b.partials, nt);
+        scan_finalize_kernel<<<nt, 256, 0, cfg.stream>>>(b.counts, nb, b.partials, b.offsets, b.cursors, b.blocklist,
+                                                         b.totals);
+    }
     *cfg.launches += 3;
     if (n > 0) {
-        bin_scatter_kernel<<<grid_for(n, 256), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors, b.perm_tmp);
+        {
+            KernelScope ks(cfg, "bin_scatter");
+            bin_scatter_kernel<<<grid_for(n, 256), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors, b.perm_tmp);
+        }
         const int grid = std::min(nb, cfg.num_sms * 16);
+        KernelScope ks(cfg, "bin_fixup");
         bin_fixup_kernel<<<grid, FIX_THREADS, 0, cfg.stream>>>(b.totals, b.blocklist, b.offsets, b.counts,
                                                                b.perm_tmp, b.perm, b.sort_scratch);
         *cfg.launches += 2;

@@ -411,13 +411,18 @@ __device__ __forceinline__ void eval_node(const DMesh<D, T>& M, const Basis<D, T
 // F = (I + dt grad_v) F, J = det F, sigma by Neo-Hookean or the weakly
 // compressible fluid p = -K (J - 1), V = V0 J. F, J and log J stay in FP64.
 template <int D, class T>
-__device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars<T>& s, long long p,
-                                                const T (&gv)[3][3]) {
-    double F[3][3], Fn[3][3];
+__device__ __forceinline__ void load_F(const PView<T>& P, long long p, double (&F)[3][3]) {
 #pragma unroll
     for (int r = 0; r < D; ++r)
 #pragma unroll
         for (int c = 0; c < D; ++c) F[r][c] = P.F[r + c * D][p];
+}
+
+// F is passed in (loaded early by the caller so the load overlaps the gather).
+template <int D, class T>
+__device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars<T>& s, long long p,
+                                                const T (&gv)[3][3], const double (&F)[3][3]) {
+    double Fn[3][3];
 #pragma unroll
     for (int r = 0; r < D; ++r)
 #pragma unroll

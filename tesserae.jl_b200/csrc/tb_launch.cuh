@@ -24,11 +24,31 @@ constexpr int SCAN_TILE = 1024;  // blocks per scan tile (256 threads x 4)
 
 inline int scan_tiles(int nb) { return (nb + SCAN_TILE - 1) / SCAN_TILE; }
 
+// Optional per-kernel timing: CUDA events recorded on the launching stream
+// around every launch while profiling is enabled (tb_profile_enable).
+struct Profiler {
+    virtual void begin(const char* name, cudaStream_t s) = 0;
+    virtual void end(cudaStream_t s) = 0;
+    virtual ~Profiler() = default;
+};
+
 struct LaunchCfg {
     cudaStream_t stream;
     int num_sms;
     long long* launches;  // incremented per kernel launch
     int* err;             // device status word
+    Profiler* prof;       // null unless profiling
+};
+
+// RAII scope naming the kernel launches it encloses.
+struct KernelScope {
+    const LaunchCfg& cfg;
+    KernelScope(const LaunchCfg& c, const char* name) : cfg(c) {
+        if (cfg.prof) cfg.prof->begin(name, cfg.stream);
+    }
+    ~KernelScope() {
+        if (cfg.prof) cfg.prof->end(cfg.stream);
+    }
 };
 
 template <int D, class T>
@@ -42,6 +62,7 @@ cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long 
                              const LaunchCfg& cfg);
 cudaError_t launch_bin_rest(int nblocks, long long n, const BinBuffers& b, const LaunchCfg& cfg);
 
+// P2G scatter into a grid whose m, mv, f are already zero where it will add.
 template <int D, class T, int BW>
 cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
                        const BinBuffers& b, const LaunchCfg& cfg);
@@ -55,6 +76,17 @@ cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const Laun
 template <int D, class T, int BW>
 cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
                        const BinBuffers& b, const LaunchCfg& cfg);
+
+// Sparse grid maintenance over node blocks touched now (cur) or in the previous
+// transfer (prev): see tb_transfer.cu.
+cudaError_t launch_mark_touched(int dim, const int* nbv, const BinBuffers& b, unsigned char* cur, int nblocks,
+                                const LaunchCfg& cfg);
+template <int D, class T, int BW>
+cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const unsigned char* cur,
+                               const unsigned char* prev, const LaunchCfg& cfg);
+template <int D, class T, int BW>
+cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
+                                      const unsigned char* cur, const unsigned char* prev, const LaunchCfg& cfg);
 
 template <int D, class T>
 cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,

@@ -4,81 +4,116 @@
 //
 // One CTA per non-empty grid block (grid-stride over the device block list).
 // The block's particles reach the (BW+3)^D-node halo tile [BW b - 1, BW b + BW + 1]
-// per axis; every support window starts at one of (BW+1)^D tile positions.
+// per axis; every support window starts at one of (BW+1)^D tile positions
+// ("groups"; particles of a group share their window).
 //
-// Per batch of up to NB particles of the block:
-//   1. one thread per particle evaluates the basis once (per-axis values and
-//      derivatives, zero past a truncated window) and writes a compact record
-//      (sources m_p, v_p, -V_p sigma_p; axis jets; for WLS/APIC also x_p, the
-//      moment inverse and B_p) to shared memory, and counting-sorts the batch by
-//      window start ("group");
-//   2. one warp per group maps lanes to the 3^D window nodes (2D: 9 nodes x 3
-//      particle lanes) and streams the group's particles, reading each record by
-//      broadcast and accumulating the node's m, mv, f in registers;
-//   3. each lane adds its node sums into the shared tile once per group. Lanes
-//      of a warp touch distinct nodes, so the only collisions are between warps.
-//      FP32 adds are compensated: atomicAdd returns the old value, the rounding
-//      error of old + x is recovered exactly (two-sum) into a second tile.
-// After the last batch the tile is flushed with one global atomic per non-zero
-// node value (gravity, sum w m g = g sum w m, is added there from the tile mass).
+// Per batch of up to NR particles of the block (one batch for a cube3d block):
+//   1. each thread evaluates the basis of its particles once (per-axis values
+//      and h_inv-scaled derivatives, zero past a truncated window) and writes a
+//      record (m_p, m_p v_p, S = -V_p sigma_p, the axis jets; for WLS/APIC also
+//      x_p, v_p, the moment inverse and B_p) to shared memory, then the batch is
+//      counting-sorted by group;
+//   2. a lane walks a pencil of groups along x (same window start in y, z)
+//      for one (y, z) row of the window and keeps the row's 3 x-nodes in
+//      registers; 9 rows x 3 pencils fill a warp in 3D (3 rows x 10 in 2D).
+//      Per particle and row the factors wy*wz, dy*wz, wy*dz and the force rows
+//      a = S[:,0] wy wz, b = S[:,1] dy wz + S[:,2] wy dz are formed once, so
+//      each of the row's nodes costs w = wx wyz, m += w m_p, mv += w (m_p v_p),
+//      f += dx a + wx b;
+//   3. after each group the x-node the window leaves for good is added to the
+//      shared tile and the row shifts one node (the pencil loop is unrolled, so
+//      the shift is a register rename): a pencil of G groups adds (G + 2) x 9
+//      node sums instead of 27 G. Lanes of a warp touch distinct nodes; only
+//      warps collide.
+// The tile accumulates in FP64 in both forms. For FP32 data this is the
+// compensated accumulation: FP64 holds the exact sum of up to 2^29 FP32 terms of
+// equal exponent, costs the same 8 bytes per value as a (hi, lo) FP32 Kahan pair,
+// and a shared-memory f64 atomic add runs at 1.8x the rate of an FP32 atomic add
+// followed by an exact two-sum of its rounding error (1.50 vs 0.84 T op/s
+// measured on B200). After the last batch the tile is flushed with one global
+// atomic per non-zero node value (gravity, sum w m g = g sum w m, is added there
+// from the tile mass).
 #include "tb_launch.cuh"
 
 namespace tb {
 
 namespace {
 
-__device__ __forceinline__ void tile_add(double* hi, double*, int idx, double x) {
-    if (x != 0.0) atomicAdd(&hi[idx], x);
-}
-
-__device__ __forceinline__ void tile_add(float* hi, float* lo, int idx, float x) {
-    if (x == 0.0f) return;
-    const float old = atomicAdd(&hi[idx], x);
-    const float s = __fadd_rn(old, x);
-    const float bp = __fsub_rn(s, old);
-    const float e = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bp)), __fsub_rn(x, bp));
-    if (e != 0.0f) atomicAdd(&lo[idx], e);
-}
-
-// Record layout (in T words), padded to a multiple of 4:
-//   [0]      m_p            [1..D]   v_p
-//   [4..]    S = -V sigma (symmetric, nsym)   -> 4 .. 4+nsym
-//   [AX..]   per axis d, per slot k: (value, derivative) -> AX + 6 d + 2 k
-//   GEN only: [XP..] x_p (D), [MI..] moment inverse (D+1)^2, [BP..] B_p (D^2)
+// Record layout (in T words):
+//   [0] m_p  [1..3] m_p v_p
+//   [4..9] S = -V sigma (symmetric; 3 used in 2D)
+//   [12..17] x jets (value, derivative * h_inv) per slot, [18..23] y, [24..29] z
+//   GEN: [32..34] x_p  [36..38] v_p  [40..55] moment inverse ((D+1)^2; [40] = -1
+//        marks a plain kernel)  [56..64] B_p (column-major)
+// The record stride is 4 (mod 32) words: the 8 lanes of a quarter warp that
+// store or load 16-byte vectors of 8 consecutive records hit 8 distinct bank
+// groups (a stride of 32 words would put every record in the same banks).
 template <int D, bool GEN>
 struct Rec {
-    static constexpr int NS = (D == 3) ? 6 : 3;
-    static constexpr int AX = 4 + ((NS + 3) / 4) * 4;  // 12 (3D), 8 (2D)
-    static constexpr int XP = AX + 6 * D;
-    static constexpr int MI = XP + 4;
-    static constexpr int BP = MI + (D + 1) * (D + 1);
-    static constexpr int END = GEN ? BP + D * D : XP;
-    static constexpr int SIZE = ((END + 3) / 4) * 4;
+    static constexpr int MV = 1, S = 4, AX = 12, XP = 32, VP = 36, MI = 40, BP = 56;
+    static constexpr int SIZE = GEN ? 68 : (D == 3 ? 36 : 28);
 };
 
-template <int D, class T, int BW, bool GEN, int NB>
-__global__ void __launch_bounds__(NB, 2) p2g_group_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
-                                                       const int* __restrict__ totals,
-                                                       const int* __restrict__ blocklist,
-                                                       const int* __restrict__ offsets,
-                                                       const int* __restrict__ perm, int* err) {
+template <class T>
+struct V4 {
+    T a, b, c, d;
+};
+template <class T>
+struct V2 {
+    T a, b;
+};
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+    const double2 u = *reinterpret_cast<const double2*>(p), w = *reinterpret_cast<const double2*>(p + 2);
+    return {u.x, u.y, w.x, w.y};
+}
+__device__ __forceinline__ V2<float> ld2(const float* p) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    return {v.x, v.y};
+}
+__device__ __forceinline__ V2<double> ld2(const double* p) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    return {v.x, v.y};
+}
+__device__ __forceinline__ void st4(float* p, float a, float b, float c, float d) {
+    *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void st4(double* p, double a, double b, double c, double d) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(c, d);
+}
+
+// Tile bytes rounded up to 16 so the records after it are 16-byte aligned.
+template <int NCTN>
+__host__ __device__ constexpr size_t tile_bytes() {
+    return ((sizeof(double) * NCTN + 15) / 16) * 16;
+}
+
+template <int D, class T, int BW, bool GEN, int NR>
+__global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
+                                                          const int* __restrict__ totals,
+                                                          const int* __restrict__ blocklist,
+                                                          const int* __restrict__ offsets,
+                                                          const int* __restrict__ perm, int* err) {
+    constexpr int NT = 256;
     constexpr int TS = BW + 3;
     constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
     constexpr int NC = 1 + 2 * D;
-    constexpr bool COMP = sizeof(T) == 4;
     constexpr int G1 = BW + 1;  // window starts per axis
     constexpr int NG = (D == 3) ? G1 * G1 * G1 : G1 * G1;
-    constexpr int NSLOT = (D == 3) ? 27 : 9;
-    constexpr int NSUB = 32 / NSLOT;  // particle lanes per slot (1 in 3D, 3 in 2D)
     constexpr int RS = Rec<D, GEN>::SIZE;
-    constexpr int NW = NB / 32;
+    constexpr int NW = NT / 32;
+    constexpr int NJK = (D == 3) ? 9 : 3;  // window rows
+    constexpr int NSUB = 32 / NJK;         // pencils per warp: 3 (3D), 10 (2D)
     using R = Rec<D, GEN>;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* hi = reinterpret_cast<T*>(smem_raw);
-    T* lo = hi + NC * TN;
-    T* rec = lo + (COMP ? NC * TN : 0);
-    int* gcount = reinterpret_cast<int*>(rec + NB * RS);
+    double* tile = reinterpret_cast<double*>(smem_raw);
+    T* rec = reinterpret_cast<T*>(smem_raw + tile_bytes<NC * TN>());
+    int* gcount = reinterpret_cast<int*>(rec + NR * RS);
     int* gstart = gcount + NG;
     int* order = gstart + NG + 1;
 
@@ -86,6 +121,8 @@ __global__ void __launch_bounds__(NB, 2) p2g_group_kernel(DMesh<D, T> M, PView<T
     const int nactive = totals[0];
     const bool apic = s.transfer == TB_TRANSFER_APIC;
     const T dinv = T(4) / (M.h * M.h);
+    const int jk = lane % NJK, sub = lane / NJK;
+    const int sj = jk % 3, sk = (D == 3) ? jk / 3 : 0;
 
     for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
         const int b = blocklist[bi] - 1;
@@ -98,66 +135,83 @@ __global__ void __launch_bounds__(NB, 2) p2g_group_kernel(DMesh<D, T> M, PView<T
                 r /= M.nb[d];
             }
         }
-        for (int t = tid; t < NC * TN; t += NB) {
-            hi[t] = T(0);
-            if constexpr (COMP) lo[t] = T(0);
-        }
+        for (int t = tid; t < NC * TN; t += NT) tile[t] = 0.0;
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0; b0 < s1; b0 += NB) {
-            const int nbat = min(NB, s1 - b0);
-            for (int g = tid; g < NG; g += NB) gcount[g] = 0;
+        for (int b0 = s0; b0 < s1; b0 += NR) {
+            const int nbat = min(NR, s1 - b0);
+            for (int g = tid; g < NG; g += NT) gcount[g] = 0;
             __syncthreads();
             // ---- 1. records + group histogram
-            int grp = -1, rank = 0;
-            if (tid < nbat) {
-                const long long p = perm[b0 + tid] - 1;
+            int grp[NR / NT], rank[NR / NT];
+#pragma unroll
+            for (int u = 0; u < NR / NT; ++u) {
+                const int ti = tid + u * NT;
+                grp[u] = -1;
+                rank[u] = 0;
+                if (ti >= nbat) continue;
+                const long long p = perm[b0 + ti] - 1;
                 T x[3];
 #pragma unroll
                 for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
                 const T l = P.l ? P.l[p] : s.gimp_l;
                 Basis<D, T> B;
-                if (prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) {
-                    int gi = 0;
-                    bool ok = true;
+                if (!prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) continue;
+                int gi = 0;
+                bool ok = true;
 #pragma unroll
-                    for (int d = D - 1; d >= 0; --d) {
-                        const int q = B.ax[d].lo - org[d];
-                        ok = ok && q >= 0 && q < G1;
-                        gi = gi * G1 + q;
-                    }
-                    if (!ok) {
-                        atomicOr(err, ERR_TILE_RANGE);
-                    } else {
-                        grp = gi;
-                        T* r = rec + tid * RS;
-                        const T Vp = P.V[p];
-                        r[0] = P.m ? P.m[p] : s.mass;
-#pragma unroll
-                        for (int d = 0; d < D; ++d) r[1 + d] = P.v[d][p];
-#pragma unroll
-                        for (int k = 0; k < R::NS; ++k) r[4 + k] = (-Vp) * P.sig[k][p];
-#pragma unroll
-                        for (int d = 0; d < D; ++d)
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                r[R::AX + 6 * d + 2 * k] = B.ax[d].val[k];
-                                r[R::AX + 6 * d + 2 * k + 1] = B.ax[d].der[k];
-                            }
-                        if constexpr (GEN) {
-#pragma unroll
-                            for (int d = 0; d < D; ++d) r[R::XP + d] = x[d];
-#pragma unroll
-                            for (int i = 0; i < D + 1; ++i)
-#pragma unroll
-                                for (int j = 0; j < D + 1; ++j)
-                                    r[R::MI + i * (D + 1) + j] = B.wls ? B.Mi[i][j] : T(i == j ? 1 : 0);
-                            r[R::MI + 0] = B.wls ? B.Mi[0][0] : T(-1);  // -1 marks a plain kernel
-#pragma unroll
-                            for (int k = 0; k < D * D; ++k) r[R::BP + k] = apic ? P.B[k][p] : T(0);
-                        }
-                        rank = atomicAdd(&gcount[grp], 1);
-                    }
+                for (int d = D - 1; d >= 0; --d) {
+                    const int q = B.ax[d].lo - org[d];
+                    ok = ok && q >= 0 && q < G1;
+                    gi = gi * G1 + q;
                 }
+                if (!ok) {
+                    atomicOr(err, ERR_TILE_RANGE);
+                    continue;
+                }
+                T* r = rec + ti * RS;
+                const T mp = P.m ? P.m[p] : s.mass;
+                const T Vp = P.V[p];
+                T v[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                for (int d = 0; d < D; ++d) v[d] = P.v[d][p];
+                T Sv[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) Sv[k] = (k < (D == 3 ? 6 : 3)) ? (-Vp) * P.sig[k < 6 ? k : 0][p] : T(0);
+                T ax[18];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        ax[6 * d + 2 * k] = d < D ? B.ax[d < D ? d : 0].val[k] : T(0);
+                        ax[6 * d + 2 * k + 1] = d < D ? B.ax[d < D ? d : 0].der[k] * M.h_inv : T(0);
+                    }
+                st4(r + 0, mp, mp * v[0], mp * v[1], mp * v[2]);
+                st4(r + 4, Sv[0], Sv[1], Sv[2], Sv[3]);
+                st4(r + 8, Sv[4], Sv[5], T(0), T(0));
+                st4(r + 12, ax[0], ax[1], ax[2], ax[3]);
+                st4(r + 16, ax[4], ax[5], ax[6], ax[7]);
+                st4(r + 20, ax[8], ax[9], ax[10], ax[11]);
+                if constexpr (D == 3) {
+                    st4(r + 24, ax[12], ax[13], ax[14], ax[15]);
+                    st4(r + 28, ax[16], ax[17], T(0), T(0));
+                }
+                if constexpr (GEN) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        r[R::XP + d] = d < D ? x[d] : T(0);
+                        r[R::VP + d] = v[d];
+                    }
+#pragma unroll
+                    for (int i = 0; i < D + 1; ++i)
+#pragma unroll
+                        for (int j = 0; j < D + 1; ++j)
+                            r[R::MI + i * (D + 1) + j] = B.wls ? B.Mi[i][j] : T(i == j ? 1 : 0);
+                    r[R::MI] = B.wls ? B.Mi[0][0] : T(-1);
+#pragma unroll
+                    for (int k = 0; k < D * D; ++k) r[R::BP + k] = apic ? P.B[k][p] : T(0);
+                }
+                grp[u] = gi;
+                rank[u] = atomicAdd(&gcount[gi], 1);
             }
             __syncthreads();
             if (warp == 0) {
@@ -177,120 +231,147 @@ __global__ void __launch_bounds__(NB, 2) p2g_group_kernel(DMesh<D, T> M, PView<T
                 if (lane == 0) gstart[NG] = carry;
             }
             __syncthreads();
-            if (grp >= 0) order[gstart[grp] + rank] = tid;
+#pragma unroll
+            for (int u = 0; u < NR / NT; ++u)
+                if (grp[u] >= 0) order[gstart[grp[u]] + rank[u]] = tid + u * NT;
             __syncthreads();
-            // ---- 2. one warp per group, lanes over window nodes
-            const int slot = lane % NSLOT, sub = lane / NSLOT;
-            const int si = slot % 3, sj = (slot / 3) % 3, sk = (D == 3) ? slot / 9 : 0;
-            for (int g = warp; g < NG; g += NW) {
-                const int q0 = gstart[g], q1 = gstart[g + 1];
-                if (q0 == q1) continue;
-                int gl[3];
-                {
-                    int r = g;
+            // ---- 2./3. pencils of groups along x: the NSUB lane sets of a warp
+            //      walk NSUB different pencils, so every lane owns its (pencil, row)
+            //      and adds its sums to the tile without any cross-lane reduction.
+            constexpr int NPENCIL = NG / G1;
+            constexpr int NTASK = (NPENCIL + NSUB - 1) / NSUB;
+            for (int task = warp; task < NTASK; task += NW) {
+                const int pc = task * NSUB + sub;
+                const bool live = sub < NSUB && pc < NPENCIL;
+                const int gy = live ? pc % G1 : 0, gz = (D == 3 && live) ? pc / G1 : 0;
+                const int gbase = G1 * (gy + G1 * gz);
+                T acc[3][NC];
 #pragma unroll
-                    for (int d = 0; d < D; ++d) {
-                        gl[d] = r % G1;
-                        r /= G1;
-                    }
-                }
-                T acc[NC];
+                for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int c = 0; c < NC; ++c) acc[c] = T(0);
-                T X[3] = {T(0), T(0), T(0)};
+                    for (int c = 0; c < NC; ++c) acc[i][c] = T(0);
+                T Y = T(0), Z = T(0);
                 if constexpr (GEN) {
-                    X[0] = node_coord(M, 0, org[0] + gl[0] + si);
-                    X[1] = node_coord(M, 1, org[1] + gl[1] + sj);
-                    if constexpr (D == 3) X[2] = node_coord(M, 2, org[2] + gl[2] + sk);
+                    Y = node_coord(M, 1, org[1] + gy + sj);
+                    if constexpr (D == 3) Z = node_coord(M, 2, org[2] + gz + sk);
                 }
-                if (sub < NSUB) {
-                    for (int q = q0 + sub; q < q1; q += NSUB) {
-                        const T* r = rec + order[q] * RS;
-                        const T mp = r[0];
-                        T v[3], S[6];
 #pragma unroll
-                        for (int d = 0; d < D; ++d) v[d] = r[1 + d];
-#pragma unroll
-                        for (int k = 0; k < R::NS; ++k) S[k] = r[4 + k];
-                        const T wx = r[R::AX + 2 * si], dx = r[R::AX + 2 * si + 1];
-                        const T wy = r[R::AX + 6 + 2 * sj], dy = r[R::AX + 6 + 2 * sj + 1];
-                        T w, gw[3];
-                        if constexpr (D == 3) {
-                            const T wz = r[R::AX + 12 + 2 * sk], dz = r[R::AX + 12 + 2 * sk + 1];
-                            w = (wx * wy) * wz;
-                            gw[0] = ((dx * wy) * wz) * M.h_inv;
-                            gw[1] = ((wx * dy) * wz) * M.h_inv;
-                            gw[2] = ((wx * wy) * dz) * M.h_inv;
-                        } else {
-                            w = wx * wy;
-                            gw[0] = (dx * wy) * M.h_inv;
-                            gw[1] = (wx * dy) * M.h_inv;
-                        }
-                        if constexpr (GEN) {
-                            T rel[3];
-#pragma unroll
-                            for (int d = 0; d < D; ++d) rel[d] = X[d] - r[R::XP + d];
-                            if (r[R::MI] != T(-1)) {  // WLS: wq = w Mi [1; rel]
-                                constexpr int N = D + 1;
-                                T Pv[N];
-                                Pv[0] = T(1);
-#pragma unroll
-                                for (int d = 0; d < D; ++d) Pv[d + 1] = rel[d];
-                                T wq[N];
-#pragma unroll
-                                for (int i = 0; i < N; ++i) {
-                                    T a = T(0);
-#pragma unroll
-                                    for (int j = 0; j < N; ++j) a += r[R::MI + i * N + j] * Pv[j];
-                                    wq[i] = w * a;
-                                }
-                                w = wq[0];
-#pragma unroll
-                                for (int d = 0; d < D; ++d) gw[d] = wq[d + 1];
+                for (int gx = 0; gx < G1 + 2; ++gx) {
+                    if (gx < G1 && live) {
+                        const int q1 = gstart[gbase + gx + 1];
+                        for (int q = gstart[gbase + gx]; q < q1; ++q) {
+                            const T* r = rec + order[q] * RS;
+                            const V4<T> m4 = ld4(r + 0), s4 = ld4(r + 4), x4 = ld4(r + 12);
+                            const V2<T> s2 = ld2(r + 8), x2 = ld2(r + 16), y2 = ld2(r + R::AX + 6 + 2 * sj);
+                            const T mp = m4.a;
+                            const T mv[3] = {m4.b, m4.c, m4.d};
+                            const T S[6] = {s4.a, s4.b, s4.c, s4.d, s2.a, s2.b};
+                            const T wx[3] = {x4.a, x4.c, x2.a}, dx[3] = {x4.b, x4.d, x2.b};
+                            const T wy = y2.a, dy = y2.b;
+                            T wyz, dyz, wdz;
+                            if constexpr (D == 3) {
+                                const V2<T> z2 = ld2(r + R::AX + 12 + 2 * sk);
+                                const T wz = z2.a, dz = z2.b;
+                                wyz = wy * wz;
+                                dyz = dy * wz;
+                                wdz = wy * dz;
+                            } else {
+                                wyz = wy;
+                                dyz = dy;
+                                wdz = T(0);
                             }
-                            if (apic) {
+                            if constexpr (!GEN) {
+                                // f_a = S[a,0] dx wyz + S[a,1] wx dyz + S[a,2] wx wdz
+                                T fa[3], fb[3];
 #pragma unroll
-                                for (int i = 0; i < D; ++i) {
-                                    T a = T(0);
+                                for (int a = 0; a < D; ++a) {
+                                    fa[a] = S[symidx<D>(a, 0)] * wyz;
+                                    fb[a] = S[symidx<D>(a, 1)] * dyz;
+                                    if constexpr (D == 3) fb[a] += S[symidx<D>(a, 2)] * wdz;
+                                }
 #pragma unroll
-                                    for (int j = 0; j < D; ++j) a += r[R::BP + i + j * D] * dinv * rel[j];
-                                    v[i] += a;
+                                for (int i = 0; i < 3; ++i) {
+                                    const T w = wx[i] * wyz;
+                                    acc[i][0] += w * mp;
+#pragma unroll
+                                    for (int d = 0; d < D; ++d) acc[i][1 + d] += w * mv[d];
+#pragma unroll
+                                    for (int a = 0; a < D; ++a) acc[i][1 + D + a] += dx[i] * fa[a] + wx[i] * fb[a];
+                                }
+                            } else {
+#pragma unroll
+                                for (int i = 0; i < 3; ++i) {
+                                    T w = wx[i] * wyz;
+                                    T gw[3] = {dx[i] * wyz, wx[i] * dyz, wx[i] * wdz};
+                                    T rel[3];
+                                    rel[0] = node_coord(M, 0, org[0] + gx + i) - r[R::XP + 0];
+                                    rel[1] = Y - r[R::XP + 1];
+                                    rel[2] = (D == 3) ? Z - r[R::XP + 2] : T(0);
+                                    if (r[R::MI] != T(-1)) {  // WLS: wq = w Mi [1; rel]
+                                        constexpr int N = D + 1;
+                                        T Pv[N];
+                                        Pv[0] = T(1);
+#pragma unroll
+                                        for (int d = 0; d < D; ++d) Pv[d + 1] = rel[d];
+                                        T wq[N];
+#pragma unroll
+                                        for (int a = 0; a < N; ++a) {
+                                            T t = T(0);
+#pragma unroll
+                                            for (int c = 0; c < N; ++c) t += r[R::MI + a * N + c] * Pv[c];
+                                            wq[a] = w * t;
+                                        }
+                                        w = wq[0];
+#pragma unroll
+                                        for (int d = 0; d < D; ++d) gw[d] = wq[d + 1];
+                                    }
+                                    T vv[3];
+#pragma unroll
+                                    for (int d = 0; d < D; ++d) vv[d] = r[R::VP + d];
+                                    if (apic) {
+#pragma unroll
+                                        for (int a = 0; a < D; ++a) {
+                                            T t = T(0);
+#pragma unroll
+                                            for (int c = 0; c < D; ++c) t += r[R::BP + a + c * D] * dinv * rel[c];
+                                            vv[a] += t;
+                                        }
+                                    }
+                                    const T wm = w * mp;
+                                    acc[i][0] += wm;
+#pragma unroll
+                                    for (int d = 0; d < D; ++d) acc[i][1 + d] += wm * vv[d];
+#pragma unroll
+                                    for (int a = 0; a < D; ++a) {
+                                        T t = S[symidx<D>(a, 0)] * gw[0];
+#pragma unroll
+                                        for (int c = 1; c < D; ++c) t += S[symidx<D>(a, c)] * gw[c];
+                                        acc[i][1 + D + a] += t;
+                                    }
                                 }
                             }
-                        }
-                        const T wm = w * mp;
-                        acc[0] += wm;
-#pragma unroll
-                        for (int d = 0; d < D; ++d) acc[1 + d] += wm * v[d];
-#pragma unroll
-                        for (int i = 0; i < D; ++i) {
-                            T a = T(0);
-#pragma unroll
-                            for (int j = 0; j < D; ++j) a += S[symidx<D>(i, j)] * gw[j];
-                            acc[1 + D + i] += a;
                         }
                     }
-                }
-                if constexpr (NSUB > 1) {
+                    // Column gx (slot 0) is final: later groups start further right.
+                    if (live && gx < TS) {
+                        const int tj = gy + sj, tk = (D == 3) ? gz + sk : 0;
+                        const int t = (D == 3) ? gx + TS * (tj + TS * tk) : gx + TS * tj;
 #pragma unroll
-                    for (int u = 1; u < NSUB; ++u)
+                        for (int c = 0; c < NC; ++c)
+                            if (acc[0][c] != T(0)) atomicAdd(&tile[c * TN + t], double(acc[0][c]));
+                    }
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) {
-                            const T o = __shfl_sync(0xffffffffu, acc[c], min(lane + u * NSLOT, 31));
-                            if (sub == 0) acc[c] += o;
-                        }
-                }
-                if (sub == 0) {
-                    const int ti = gl[0] + si, tj = gl[1] + sj, tk = (D == 3) ? gl[D - 1] + sk : 0;
-                    const int t = (D == 3) ? ti + TS * (tj + TS * tk) : ti + TS * tj;
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) tile_add(hi, lo, c * TN + t, acc[c]);
+                    for (int c = 0; c < NC; ++c) {
+                        acc[0][c] = acc[1][c];
+                        acc[1][c] = acc[2][c];
+                        acc[2][c] = T(0);
+                    }
                 }
             }
             __syncthreads();
         }
-        // ---- 3. flush the tile
-        for (int t = tid; t < TN; t += NB) {
+        // ---- flush the tile
+        for (int t = tid; t < TN; t += NT) {
             int node[3], rem = t;
             bool inside = true;
             long long lin = 0;
@@ -303,49 +384,49 @@ __global__ void __launch_bounds__(NB, 2) p2g_group_kernel(DMesh<D, T> M, PView<T
             if (!inside) continue;
 #pragma unroll
             for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + node[d];
-            T val[NC];
+            double val[NC];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                val[c] = hi[c * TN + t];
-                if constexpr (COMP) val[c] += lo[c * TN + t];
-            }
+            for (int c = 0; c < NC; ++c) val[c] = tile[c * TN + t];
 #pragma unroll
-            for (int d = 0; d < D; ++d) val[1 + D + d] += s.g[d] * val[0];
-            if (val[0] != T(0)) atomicAdd(G.m + lin, val[0]);
+            for (int d = 0; d < D; ++d) val[1 + D + d] += double(s.g[d]) * val[0];
+            if (val[0] != 0.0) atomicAdd(G.m + lin, T(val[0]));
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                if (val[1 + d] != T(0)) atomicAdd(G.mv[d] + lin, val[1 + d]);
-                if (val[1 + D + d] != T(0)) atomicAdd(G.f[d] + lin, val[1 + D + d]);
+                if (val[1 + d] != 0.0) atomicAdd(G.mv[d] + lin, T(val[1 + d]));
+                if (val[1 + D + d] != 0.0) atomicAdd(G.f[d] + lin, T(val[1 + D + d]));
             }
         }
         __syncthreads();
     }
 }
 
-template <int D, class T, int BW, bool GEN, int NB>
+template <int D, class T, int BW, bool GEN, int NR>
 size_t p2g_smem_bytes() {
     constexpr int TS = BW + 3;
     constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
     constexpr int NC = 1 + 2 * D;
     constexpr int NG = (D == 3) ? (BW + 1) * (BW + 1) * (BW + 1) : (BW + 1) * (BW + 1);
-    const size_t tiles = sizeof(T) * size_t(NC * TN) * (sizeof(T) == 4 ? 2 : 1);
-    const size_t recs = sizeof(T) * size_t(NB) * Rec<D, GEN>::SIZE;
-    const size_t ints = sizeof(int) * size_t(NG + NG + 1 + NB);
+    const size_t tiles = tile_bytes<NC * TN>();
+    const size_t recs = sizeof(T) * size_t(NR) * Rec<D, GEN>::SIZE;
+    const size_t ints = sizeof(int) * size_t(NG + NG + 1 + NR);
     return tiles + recs + ints;
 }
 
 template <int D, class T, int BW, bool GEN>
 cudaError_t launch_group(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
                          const BinBuffers& b, const LaunchCfg& cfg) {
-    constexpr int NB = 256;
-    auto kern = p2g_group_kernel<D, T, BW, GEN, NB>;
-    const size_t smem = p2g_smem_bytes<D, T, BW, GEN, NB>();
+    // Records per batch: a whole cube3d block (512) in FP32, half of it in FP64
+    // or with the general (WLS/APIC) record.
+    constexpr int NR = (sizeof(T) == 4 && !GEN) ? 512 : 256;
+    auto kern = p2g_group_kernel<D, T, BW, GEN, NR>;
+    const size_t smem = p2g_smem_bytes<D, T, BW, GEN, NR>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NB, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
     const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
-    kern<<<grid, NB, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    KernelScope ks(cfg, "p2g");
+    kern<<<grid, 256, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -355,8 +436,6 @@ cudaError_t launch_group(const DMesh<D, T>& M, const PView<T>& P, const GView<T>
 template <int D, class T, int BW>
 cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
                        const BinBuffers& b, const LaunchCfg& cfg) {
-    cudaError_t e = launch_grid_zero<D, T>(M, G, cfg);
-    if (e != cudaSuccess) return e;
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
     return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_group<D, T, BW, false>(M, P, G, s, b, cfg);

@@ -69,11 +69,88 @@ __global__ void __launch_bounds__(256) grid_update_kernel(DMesh<D, T> M, GView<T
     }
 }
 
+// ---- sparse grid maintenance -------------------------------------------
+// Node block B owns nodes [BW B, BW B + BW - 1] per axis. A particle block b
+// reaches nodes [BW b - 1, BW b + BW + 1], i.e. node blocks b-1 .. b+1 per axis.
+template <int D>
+__global__ void __launch_bounds__(128) mark_touched_kernel(const int* __restrict__ totals,
+                                                           const int* __restrict__ blocklist, int3 nb,
+                                                           unsigned char* __restrict__ cur) {
+    const int nactive = totals[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nactive; i += gridDim.x * blockDim.x) {
+        const int b = blocklist[i] - 1;
+        const int bx = b % nb.x, by = (b / nb.x) % nb.y, bz = (D == 3) ? b / (nb.x * nb.y) : 0;
+        for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = bx + dx, y = by + dy, z = bz + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= nb.x || y >= nb.y || (D == 3 && z >= nb.z)) continue;
+                    cur[x + nb.x * (y + nb.y * z)] = 1;
+                }
+    }
+}
+
+// One warp per node block. mode 0: zero m, mv, f where cur|prev; mode 1: grid
+// update where cur, zero v, vn where prev only.
+template <int D, class T, int BW, int MODE>
+__global__ void __launch_bounds__(256) node_block_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s,
+                                                         const unsigned char* __restrict__ cur,
+                                                         const unsigned char* __restrict__ prev) {
+    constexpr int NPB = (D == 3) ? BW * BW * BW : BW * BW;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; B < M.nblocks; B += warps) {
+        const bool c = cur[B] != 0, pv = prev[B] != 0;
+        if (!c && !pv) continue;
+        const int bx = B % M.nb[0], by = (B / M.nb[0]) % M.nb[1], bz = (D == 3) ? B / (M.nb[0] * M.nb[1]) : 0;
+        for (int q = lane; q < NPB; q += 32) {
+            int idx[3];
+            idx[0] = bx * BW + q % BW;
+            idx[1] = by * BW + (q / BW) % BW;
+            idx[2] = (D == 3) ? bz * BW + q / (BW * BW) : 0;
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < D; ++d) inside = inside && idx[d] < M.n[d];
+            if (!inside) continue;
+            long long I = 0;
+#pragma unroll
+            for (int d = D - 1; d >= 0; --d) I = I * M.n[d] + idx[d];
+            if constexpr (MODE == 0) {
+                G.m[I] = T(0);
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    G.mv[d][I] = T(0);
+                    G.f[d][I] = T(0);
+                }
+            } else {
+                const T m = c ? G.m[I] : T(0);
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    T vn = T(0), v = T(0);
+                    if (m != T(0)) {
+                        vn = G.mv[d][I] / m;
+                        v = vn + (s.dt * G.f[d][I]) / m;
+                    }
+                    if (s.wall_mask) {
+                        const bool lo = (s.wall_mask >> (2 * d)) & 1, hi = (s.wall_mask >> (2 * d + 1)) & 1;
+                        if ((lo && idx[d] < s.wall_layers) || (hi && idx[d] >= M.n[d] - s.wall_layers)) {
+                            vn = T(0);
+                            v = T(0);
+                        }
+                    }
+                    G.vn[d][I] = vn;
+                    G.v[d][I] = v;
+                }
+            }
+        }
+    }
+}
+
 // Final per-particle writes of @G2P and the FP64 constitutive update.
 template <int D, class T>
 __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& s, long long p, const T* x,
                                            const T* vp, const T* vpic, const T* dvf, const T (&gv)[3][3],
-                                           const T* dxs, const T (&Bn)[3][3]) {
+                                           const T* dxs, const T (&Bn)[3][3], const double (&F)[3][3]) {
     if (s.transfer == TB_TRANSFER_APIC) {
 #pragma unroll
         for (int d = 0; d < D; ++d) P.v[d][p] = vpic[d];
@@ -94,7 +171,7 @@ __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& 
         for (int c = 0; c < D; ++c) P.gv[r + c * D][p] = gv[r][c];
 #pragma unroll
     for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
-    particle_update<D, T>(P, s, p, gv);
+    particle_update<D, T>(P, s, p, gv, F);
 }
 
 template <int D, class T, int BW, bool GEN>
@@ -104,8 +181,9 @@ __global__ void __launch_bounds__(128) g2p_tile_kernel(DMesh<D, T> M, GView<T> G
                                                        const int* __restrict__ offsets,
                                                        const int* __restrict__ perm, int* err) {
     constexpr int TS = Tile<D, BW>::TS, TN = Tile<D, BW>::TN;
-    __shared__ T tv[D * TN];
-    __shared__ T tdv[D * TN];
+    // Component-major tile: v_r at [r TN + t], dv_r = (v - vn)_r at [(D + r) TN + t];
+    // lanes reading different nodes hit different banks.
+    __shared__ T tile[2 * D * TN];
     const int nactive = totals[0];
     const int tid = threadIdx.x, nth = blockDim.x;
     const bool apic = s.transfer == TB_TRANSFER_APIC;
@@ -134,8 +212,8 @@ __global__ void __launch_bounds__(128) g2p_tile_kernel(DMesh<D, T> M, GView<T> G
             for (int d = 0; d < D; ++d) {
                 const T vi = inside ? G.v[d][lin] : T(0);
                 const T vni = inside ? G.vn[d][lin] : T(0);
-                tv[d * TN + t] = vi;
-                tdv[d * TN + t] = vi - vni;
+                tile[d * TN + t] = vi;
+                tile[(D + d) * TN + t] = vi - vni;
             }
         }
         __syncthreads();
@@ -146,59 +224,107 @@ __global__ void __launch_bounds__(128) g2p_tile_kernel(DMesh<D, T> M, GView<T> G
             load_x<D, T>(P, p, x);
 #pragma unroll
             for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
+            double F[3][3];
+            load_F<D, T>(P, p, F);
             const T l = P.l ? P.l[p] : s.gimp_l;
             T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
             T gv[3][3] = {}, Bn[3][3] = {};
             Basis<D, T> B;
             if (prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) {
-                const bool need_rel = GEN && (B.wls || apic);
+                int q0[3] = {0, 0, 0};
+                bool ok = true;
 #pragma unroll
-                for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+                for (int d = 0; d < D; ++d) {
+                    q0[d] = B.ax[d].lo - org[d];
+                    ok = ok && q0[d] >= 0 && q0[d] + 2 < TS;
+                }
+                if (!ok) {
+                    atomicOr(err, ERR_TILE_RANGE);
+                } else if constexpr (!GEN) {
+                    // Separable contraction: sum over the x-slot first, then weight
+                    // the partial sums with the y (and z) factors.
+                    T dxh[3];
 #pragma unroll
-                    for (int jj = 0; jj < 3; ++jj)
+                    for (int i = 0; i < 3; ++i) dxh[i] = B.ax[0].der[i] * M.h_inv;
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const int idx[3] = {i, jj, k};
-                            int t = 0;
-                            bool ok = true;
+                    for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
 #pragma unroll
-                            for (int d = D - 1; d >= 0; --d) {
-                                const int q = B.ax[d].lo + idx[d] - org[d];
-                                ok = ok && (q >= 0 && q < TS);
-                                t = t * TS + q;
+                        for (int jj = 0; jj < 3; ++jj) {
+                            T Av[3] = {T(0), T(0), T(0)}, Adv[3] = {T(0), T(0), T(0)}, Ag[3] = {T(0), T(0), T(0)};
+                            const int t0 = (D == 3) ? q0[0] + TS * ((q0[1] + jj) + TS * (q0[D - 1] + k))
+                                                    : q0[0] + TS * (q0[1] + jj);
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) {
+                                const T* nd = tile + (t0 + i);
+                                const T wx = B.ax[0].val[i], gx = dxh[i];
+#pragma unroll
+                                for (int r = 0; r < D; ++r) {
+                                    const T vi = nd[r * TN], dvi = nd[(D + r) * TN];
+                                    Av[r] += wx * vi;
+                                    Adv[r] += wx * dvi;
+                                    Ag[r] += gx * vi;
+                                }
                             }
-                            if (!ok) {
-                                atomicOr(err, ERR_TILE_RANGE);
-                                continue;
+                            T wyz, dyz, wdz;
+                            if constexpr (D == 3) {
+                                wyz = B.ax[1].val[jj] * B.ax[D - 1].val[k];
+                                dyz = (B.ax[1].der[jj] * M.h_inv) * B.ax[D - 1].val[k];
+                                wdz = B.ax[1].val[jj] * (B.ax[D - 1].der[k] * M.h_inv);
+                            } else {
+                                wyz = B.ax[1].val[jj];
+                                dyz = B.ax[1].der[jj] * M.h_inv;
+                                wdz = T(0);
                             }
-                            T rel[3] = {T(0), T(0), T(0)};
-                            if (need_rel) {
+#pragma unroll
+                            for (int r = 0; r < D; ++r) {
+                                vpic[r] += wyz * Av[r];
+                                dvf[r] += wyz * Adv[r];
+                                gv[r][0] += wyz * Ag[r];
+                                gv[r][1] += dyz * Av[r];
+                                if constexpr (D == 3) gv[r][2] += wdz * Av[r];
+                            }
+                        }
+#pragma unroll
+                    for (int d = 0; d < D; ++d) dxs[d] = vpic[d] * s.dt;
+                } else {
+                    // WLS / APIC: node weights are not separable; per-node loop.
+#pragma unroll
+                    for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+#pragma unroll
+                        for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) {
+                                const int idx[3] = {i, jj, k};
+                                const int t = (D == 3) ? (q0[0] + i) + TS * ((q0[1] + jj) + TS * (q0[D - 1] + k))
+                                                       : (q0[0] + i) + TS * (q0[1] + jj);
+                                T rel[3] = {T(0), T(0), T(0)};
 #pragma unroll
                                 for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
-                            }
-                            T w, dw[3];
-                            eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
-                            T vi[3];
+                                T w, dw[3];
+                                eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
+                                const T* nd = tile + t;
+                                T vi[3];
 #pragma unroll
-                            for (int d = 0; d < D; ++d) {
-                                vi[d] = tv[d * TN + t];
-                                vpic[d] += w * vi[d];
-                                dvf[d] += w * tdv[d * TN + t];
-                                dxs[d] += (w * vi[d]) * s.dt;
-                            }
-#pragma unroll
-                            for (int r = 0; r < D; ++r)
-#pragma unroll
-                                for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * dw[c];
-                            if (GEN && apic) {
+                                for (int d = 0; d < D; ++d) {
+                                    vi[d] = nd[d * TN];
+                                    vpic[d] += w * vi[d];
+                                    dvf[d] += w * nd[(D + d) * TN];
+                                    dxs[d] += (w * vi[d]) * s.dt;
+                                }
 #pragma unroll
                                 for (int r = 0; r < D; ++r)
 #pragma unroll
-                                    for (int c = 0; c < D; ++c) Bn[r][c] += (w * vi[r]) * rel[c];
+                                    for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * dw[c];
+                                if (apic) {
+#pragma unroll
+                                    for (int r = 0; r < D; ++r)
+#pragma unroll
+                                        for (int c = 0; c < D; ++c) Bn[r][c] += (w * vi[r]) * rel[c];
+                                }
                             }
-                        }
+                }
             }
-            g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn);
+            g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
         }
         __syncthreads();
     }
@@ -215,6 +341,8 @@ __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T>
         load_x<D, T>(P, p, x);
 #pragma unroll
         for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
+        double F[3][3];
+        load_F<D, T>(P, p, F);
         const T l = P.l ? P.l[p] : s.gimp_l;
         T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
         T gv[3][3] = {}, Bn[3][3] = {};
@@ -263,7 +391,7 @@ __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T>
                         }
                     }
         }
-        g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn);
+        g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
     }
 }
 
@@ -280,7 +408,9 @@ __global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T>
             x[d] = P.x[d][p];
             vp[d] = P.v[d][p];
         }
-        g2p_finish<D, T>(P, s, p, x, vp, z, z, gv, z, Bn);
+        double F[3][3];
+        load_F<D, T>(P, p, F);
+        g2p_finish<D, T>(P, s, p, x, vp, z, z, gv, z, Bn, F);
     }
 }
 
@@ -334,6 +464,7 @@ template <int D, class T>
 cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const LaunchCfg& cfg) {
     const long long nn = M.nnodes;
     const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
+    KernelScope ks(cfg, "grid_zero");
     grid_zero_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(G, nn);
     ++*cfg.launches;
     return cudaGetLastError();
@@ -343,6 +474,7 @@ template <int D, class T>
 cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s, const LaunchCfg& cfg) {
     const long long nn = M.nnodes;
     const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
+    KernelScope ks(cfg, "grid_update");
     grid_update_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(M, G, s);
     ++*cfg.launches;
     return cudaGetLastError();
@@ -355,7 +487,11 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
     auto kern = gen ? g2p_tile_kernel<D, T, BW, true> : g2p_tile_kernel<D, T, BW, false>;
     const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), M.nblocks);
-    kern<<<grid, 128, 0, cfg.stream>>>(M, G, P, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    {
+        KernelScope ks(cfg, "g2p");
+        kern<<<grid, 128, 0, cfg.stream>>>(M, G, P, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    }
+    KernelScope ks(cfg, "g2p_outside");
     const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
     g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids);
     *cfg.launches += 2;
@@ -367,7 +503,39 @@ cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PVi
                               const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const int grid = int(std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 32));
+    KernelScope ks(cfg, "g2p_direct");
     g2p_direct_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, G, P, s, cfg.err);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mark_touched(int dim, const int* nbv, const BinBuffers& b, unsigned char* cur, int nblocks,
+                                const LaunchCfg& cfg) {
+    const int grid = std::max(1, std::min((nblocks + 127) / 128, cfg.num_sms * 8));
+    const int3 nb = make_int3(nbv[0], nbv[1], nbv[2]);
+    KernelScope ks(cfg, "grid_mark");
+    if (dim == 3) mark_touched_kernel<3><<<grid, 128, 0, cfg.stream>>>(b.totals, b.blocklist, nb, cur);
+    else mark_touched_kernel<2><<<grid, 128, 0, cfg.stream>>>(b.totals, b.blocklist, nb, cur);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T, int BW>
+cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const unsigned char* cur,
+                               const unsigned char* prev, const LaunchCfg& cfg) {
+    const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
+    KernelScope ks(cfg, "grid_zero");
+    node_block_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, cur, prev);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T, int BW>
+cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
+                                      const unsigned char* cur, const unsigned char* prev, const LaunchCfg& cfg) {
+    const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
+    KernelScope ks(cfg, "grid_update");
+    node_block_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, prev);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -377,6 +545,7 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
                                   long long* win, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const int grid = int(std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 16));
+    KernelScope ks(cfg, "update_weights");
     update_weights_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, P, s, w, gw, win, cfg.err);
     ++*cfg.launches;
     return cudaGetLastError();
@@ -391,6 +560,11 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
     template cudaError_t launch_g2p_direct<D, T>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,       \
                                                  const Scalars<T>&, const LaunchCfg&);
 #define TB_INST_TB(D, T, BW)                                                                                 \
+    template cudaError_t launch_sparse_zero<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const unsigned char*, \
+                                                      const unsigned char*, const LaunchCfg&);                 \
+    template cudaError_t launch_sparse_grid_update<D, T, BW>(const DMesh<D, T>&, const GView<T>&,              \
+                                                             const Scalars<T>&, const unsigned char*,          \
+                                                             const unsigned char*, const LaunchCfg&);          \
     template cudaError_t launch_g2p<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,         \
                                               const Scalars<T>&, const BinBuffers&, const LaunchCfg&);
 

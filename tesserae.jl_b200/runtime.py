@@ -69,6 +69,18 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.tb_launch_count(self.ptr))
 
+    def profile(self, on: bool = True):
+        """Enable/disable per-kernel CUDA-event timing of this library's launches."""
+        self.check(self.lib.tb_profile_enable(self.ptr, int(bool(on))), "tb_profile_enable")
+
+    def profile_read(self) -> dict:
+        """{kernel family: (launches, ms)} accumulated since the last read (synchronises)."""
+        cap = 64
+        buf = (_abi.tb_kernel_time * cap)()
+        cnt = C.c_int32()
+        self.check(self.lib.tb_profile_read(self.ptr, buf, cap, C.byref(cnt)), "tb_profile_read")
+        return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].ms)) for i in range(min(cnt.value, cap))}
+
     def fn(self, name: str, dtype):
         return getattr(self.lib, f"{name}_{_suffix(dtype)}")
 
@@ -135,8 +147,8 @@ def rollout_host(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     """Host-buffer rollout: `particles` holds numpy arrays; state is copied in,
     advanced `nsteps` steps on the device and copied back (synchronous)."""
     ctx = ctx or _default()
-    if particles.backend != "numpy":
-        raise TypeError("rollout_host takes host (numpy) particles")
+    if particles.backend not in ("numpy", "pinned"):
+        raise TypeError("rollout_host takes host (numpy or pinned) particles")
     rc = ctx.fn("tb_rollout_host", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(params), int(nsteps))
     ctx.check(rc, "rollout_host")

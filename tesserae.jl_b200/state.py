@@ -125,11 +125,18 @@ class CartesianMesh:
 # ---------------------------------------------------------------------------
 
 def _alloc(backend, shape, dtype, device=None, fill=0.0):
+    """numpy (host), pinned (page-locked host, returned as a numpy view) or torch (device)."""
     if backend == "numpy":
         a = np.empty(shape, dtype=dtype)
         a.fill(fill)
         return a
     import torch
+    if backend == "pinned":
+        tdt = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32,
+               np.int64: torch.int64}[np.dtype(dtype).type]
+        a = torch.empty(shape, dtype=tdt, pin_memory=True).numpy()
+        a.fill(fill)
+        return a
     tdt = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32,
            np.int64: torch.int64}[np.dtype(dtype).type]
     return torch.full(shape, fill, dtype=tdt, device=device)
@@ -204,7 +211,7 @@ class Particles:
             dst = getattr(out, k)
             srcn = src if isinstance(src, np.ndarray) else src.detach().cpu().numpy()
             tdt = np.float64 if k == "F" else dtype
-            if backend == "numpy":
+            if backend in ("numpy", "pinned"):
                 dst[...] = srcn.astype(tdt)
             else:
                 import torch
