@@ -227,6 +227,28 @@ int32_t tb_rollout_host_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host
 int32_t tb_rollout_host_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
                             const tb_step_params* params, int32_t nsteps);
 
+/* ---- binning without allocation ---------------------------------------
+ * No counterpart in the reference: Tesserae.jl always allocates its partition
+ * scratch through KernelAbstractions. This entry point is for callers that
+ * cannot call cudaMalloc (code inside another framework's memory pool or a
+ * runtime that forbids device allocation after start-up, loops that must not
+ * stall on the allocator) and have no tb_ctx. It bins like tb_bin_particles_f32
+ * (precision = 1) or _f64 (precision = 0), with the same bit-exact output, but
+ * its scratch is one fixed array compiled into the library, held by every GPU
+ * that loads the library until exit. It allocates nothing: inputs above
+ * TB_NOALLOC_MAX_PARTICLES particles or TB_NOALLOC_MAX_BLOCKS grid blocks are
+ * rejected with TB_ERR_CAPACITY. It runs on the current device and `stream`,
+ * synchronises `stream` once to read the totals, and writes a message into
+ * `errbuf` (may be NULL) on error. The first call on a device looks the scratch
+ * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the scratch: calls that overlap on the GPU race, so serialise
+ * them. */
+#define TB_NOALLOC_MAX_PARTICLES (1 << 20)
+#define TB_NOALLOC_MAX_BLOCKS (1 << 20)
+int32_t tb_bin_particles_noalloc(const tb_mesh* mesh, const tb_particles* particles, int32_t precision,
+                                 tb_partition* partition, void* stream, int64_t* nactive, int64_t* nassigned,
+                                 char* errbuf, int32_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

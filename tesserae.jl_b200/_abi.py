@@ -116,6 +116,8 @@ SIGNATURES = [
     ("tb_launch_count", I64, [VP]),
     ("tb_profile_enable", I32, [VP, I32]),
     ("tb_profile_read", I32, [VP, P(tb_kernel_time), I32, P(I32)]),
+    ("tb_bin_particles_noalloc", I32, [P(tb_mesh), P(tb_particles), I32, P(tb_partition), VP, P(I64), P(I64),
+                                       C.c_char_p, I32]),
 ]
 for _p in ("f64", "f32"):
     SIGNATURES += [
