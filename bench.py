@@ -183,6 +183,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=int, default=1, help="shrink the cube scene (cells per axis / scale)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true",
+                    help="only the timed FP32 leg (for profiler captures); prints a reduced line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -237,7 +239,8 @@ def main():
         return e0.elapsed_time(e1), ctx.launches - l0
 
     results = {}
-    for name, dtype in (("f32", np.float32), ("f64", np.float64)):
+    forms = (("f32", np.float32),) if args.quick else (("f32", np.float32), ("f64", np.float64))
+    for name, dtype in forms:
         P = host64.to("torch", device="cuda", dtype=dtype)
         part = tb.Partition(mesh, n, backend="torch", device="cuda")
         G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
@@ -254,6 +257,18 @@ def main():
         results[name] = {"ms": ms, "launches": launches, "kernels": kt, "clocks": clk.summary()}
         del P, part, G
         torch.cuda.empty_cache()
+
+    if args.quick:
+        if rank == 0:
+            f32 = results["f32"]
+            print(json.dumps({"metric": METRIC, "value": world * n * args.steps / (f32["ms"] * 1e-3),
+                              "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": f32["ms"] / args.steps, "quick": True,
+                              "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(f32["kernels"].items())}}),
+                  flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # FP32 vs FP64 after 100 steps of the same scene (both on the device).
     acc = {}
