@@ -50,53 +50,111 @@ def load_oracle(tb):
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    10 ms from a background thread while the timed region runs; nvidia-smi is
+    the fallback when NVML cannot be loaded."""
 
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
-        self.proc = None
+        self.sm, self.smax, self.reasons, self.source = [], None, set(), None
+        self._stop = None
+        self._thread = None
+        self._proc = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        # the CUDA ordinal and the NVML index differ under CUDA_VISIBLE_DEVICES: match by UUID
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            for cand in (uuid, "GPU-" + uuid):
+                try:
+                    return pynvml, pynvml.nvmlDeviceGetHandleByUUID(cand)
+                except Exception:
+                    pass
+        except Exception:
+            pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _sample(self, nv, h):
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        bits = int(get(h))
+        for name, bit in self.REASON_BITS.items():
+            if bits & bit:
+                self.reasons.add(name)
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self._sample(nv, h)
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self._nv, self._h = nv, h
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+            self.source = "nvml"
+        except Exception:
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits", "-lms", "100"],
+                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi"
+            except OSError:
+                self._proc = None
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
+        if self._thread is not None:
+            if not self.sm:  # a region shorter than one period: take one sample now
+                try:
+                    self._sample(self._nv, self._h)
+                except Exception:
+                    pass
+            self._stop.set()
+            self._thread.join(timeout=5)
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                out, _ = self._proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+                self._proc.kill()
+                out, _ = self._proc.communicate()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for l in out.splitlines():
+                f = [x.strip() for x in l.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.sm.append(float(f[1]))
+                    self.smax = float(f[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, f[5:9]):
+                    if val.lower().startswith("active"):
+                        self.reasons.add(name)
 
     def summary(self) -> dict:
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, f[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.source}
 
 
 def measured_peaks() -> tuple[float, str]:

@@ -227,6 +227,55 @@ int32_t tb_rollout_host_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host
 int32_t tb_rollout_host_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
                             const tb_step_params* params, int32_t nsteps);
 
+/* ---- reverse mode: sensitivities of a rollout ---------------------------
+ * No counterpart in the reference: Tesserae.jl differentiates only constitutive
+ * laws and basis jets (through Tensorial's dual numbers) and has no adjoint of
+ * its transfers. These entry points give the sensitivities of a scalar loss to
+ * the particle state that tb_step_* advances -- positions x, velocities v and
+ * the deformation gradient F (sigma and V are functions of F) -- and to the
+ * per-particle Lame parameters. The adjoint arithmetic is FP64 in both forms
+ * (the _f32 entry points differentiate the mixed FP32 step).
+ * Supported: quadratic B-spline and uGIMP bases, FLIP/PIC transfer (any
+ * flip_alpha), Neo-Hookean and fluid materials, slip walls. WLS bases and APIC
+ * return TB_ERR_UNSUPPORTED. */
+typedef struct tb_adjoint {
+    double* x[3];     /* d loss / d x_p per component */
+    double* v[3];     /* d loss / d v_p */
+    double* F[9];     /* d loss / d F_p, column-major like particles.F */
+    double* mu;       /* d loss / d mu_p, accumulated (+=); NULL = not wanted */
+    double* lambda;   /* d loss / d lambda_p (the bulk modulus K for fluids), accumulated; NULL = not wanted */
+} tb_adjoint;
+
+/* One step backwards. `particles` holds the state at the START of the step as
+ * tb_step_* reads it (x, v, F, sigma, V). On entry `adj` holds the sensitivities
+ * to the state at the END of the step; on return, to the state at its start
+ * (adj.mu and adj.lambda accumulate). The step's partition and forward grid
+ * are recomputed into `partition` and `grid`. Asynchronous. */
+int32_t tb_adjoint_step_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+int32_t tb_adjoint_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+
+/* Checkpointed rollout. tb_tape_forward_* advances `particles` by `nsteps`
+ * steps exactly like tb_step_* and keeps the state at steps 0, K, 2K, ...
+ * (K = checkpoint_every) in context-owned device memory. tb_tape_backward_*
+ * takes in `adj` the sensitivities to the final state and returns the
+ * sensitivities to the state at step 0 (mu and lambda accumulate over all
+ * steps); for each segment of K steps it restores the checkpoint, re-runs the
+ * segment storing every step's state, and steps backwards through it, so the
+ * device memory held is (nsteps/K + K) particle states. `particles` is the
+ * working state and holds the step-0 state again on return. The backward pass
+ * must follow the forward pass on the same context with the same particle
+ * count, mesh and params. Asynchronous. */
+int32_t tb_tape_forward_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, int32_t nsteps, int32_t checkpoint_every);
+int32_t tb_tape_forward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, int32_t nsteps, int32_t checkpoint_every);
+int32_t tb_tape_backward_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                             tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+int32_t tb_tape_backward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                             tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+
 /* ---- binning without allocation ---------------------------------------
  * No counterpart in the reference: Tesserae.jl always allocates its partition
  * scratch through KernelAbstractions. This entry point is for callers that

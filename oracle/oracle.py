@@ -46,6 +46,8 @@ def lib(abi):
         "tbo_step_parallel": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid),
                               P(abi.tb_step_params), C.c_int, C.c_int, P(dbl)],
         "tbo_supportnodes": [C.c_int, P(abi.tb_mesh), C.c_int, P(dbl), dbl, P(i64)],
+        "tbo_adjoint_step": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid),
+                             P(abi.tb_step_params), P(abi.tb_adjoint)],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -113,6 +115,13 @@ class Oracle:
                                         C.byref(particles.struct()), C.byref(grid.struct()), C.byref(params),
                                         nsteps, nthreads, phases), "step_parallel")
         return list(phases)
+
+    def adjoint_step(self, mesh, particles, grid, params, adjoint):
+        """One step backwards: `particles` is the start-of-step state, `adjoint`
+        (an Adjoint on the numpy backend) is updated in place."""
+        _check(self.L.tbo_adjoint_step(_prec(particles.dtype), C.byref(mesh.struct()),
+                                       C.byref(particles.struct()), C.byref(grid.struct()), C.byref(params),
+                                       C.byref(adjoint.struct())), "adjoint_step")
 
     def supportnodes(self, mesh, basis, x, l=0.0):
         xs = (C.c_double * 3)(*list(x) + [0.0] * (3 - len(x)))

@@ -180,6 +180,13 @@ int do_step_parallel(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_ste
     return TB_OK;
 }
 
+// One step backwards (reverse mode of do_step's step; no reference counterpart).
+template <int D, class T>
+int do_adjoint_step(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm, tb_adjoint* a) {
+    auto M = make_mesh<D, T>(*m);
+    return adjoint_step<D, T>(M, *p, *g, *prm, *a);
+}
+
 #define TBO_DISPATCH(FN, ...)                                                   \
     do {                                                                        \
         if (m == nullptr) return TB_ERR_ARG;                                    \
@@ -222,6 +229,11 @@ int tbo_step(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_s
 int tbo_step_parallel(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm,
                       int nsteps, int nthreads, double* phase_s) {
     TBO_DISPATCH(do_step_parallel, m, p, g, prm, nsteps, nthreads, phase_s);
+}
+
+int tbo_adjoint_step(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm,
+                     tb_adjoint* a) {
+    TBO_DISPATCH(do_adjoint_step, m, p, g, prm, a);
 }
 
 int tbo_max_threads(void) { return omp_get_max_threads(); }

@@ -664,6 +664,317 @@ inline void g2p(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p, const tb
 }
 
 // ---------------------------------------------------------------------------
+// reverse mode of one step (the reference has no adjoint; this differentiates
+// the forward step above by hand, all adjoint arithmetic in double)
+// ---------------------------------------------------------------------------
+
+// Second derivatives of the 1-D kernels with respect to xi (the jets above
+// differentiated once more, piece by piece).
+inline double d2_bspline_quadratic(double xi) {
+    const double a = std::fabs(xi);
+    if (a < 0.5) return -2.0;
+    if (a < 1.5) return 1.0;
+    return 0.0;
+}
+inline double d2_ugimp(double xi, double l) {
+    const double a = std::fabs(xi);
+    if (a < l / 2) return -2.0 / l;
+    if (a < 1.0 - l / 2) return 0.0;
+    if (a < 1.0 + l / 2) return 1.0 / l;
+    return 0.0;
+}
+
+// Value, gradient and Hessian (with respect to x_p) of the kernel at every
+// window slot, from per-axis nodewise jets in double.
+template <int D>
+struct AdjWeights {
+    double w[27], g[27][3], H[27][3][3];
+};
+
+template <int D, class T>
+inline void adjoint_weights(const Mesh<D, T>& M, int basis, const T* x, T l_abs, const Weights<D, T>& W,
+                            AdjWeights<D>& A) {
+    const bool gimp = basis == TB_UGIMP;
+    const double lnorm = gimp ? double(T(l_abs / M.h)) : 0.0;
+    const double hi = double(M.h_inv);
+    double val[3][3] = {}, der[3][3] = {}, d2[3][3] = {};
+    for (int d = 0; d < D; ++d)
+        for (int k = 0; k < W.cnt[d]; ++k) {
+            const double xi = (double(x[d]) - double(node_coord(M, d, W.lo[d] + k))) * hi;
+            if (gimp) {
+                jet_ugimp(xi, lnorm, val[d][k], der[d][k]);
+                d2[d][k] = d2_ugimp(xi, lnorm);
+            } else {
+                jet_bspline_quadratic(xi, val[d][k], der[d][k]);
+                d2[d][k] = d2_bspline_quadratic(xi);
+            }
+        }
+    for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+        for (int j = 0; j < W.cnt[1]; ++j)
+            for (int i = 0; i < W.cnt[0]; ++i) {
+                const int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                const int loc[3] = {i, j, k};
+                double w = 1.0;
+                for (int d = 0; d < D; ++d) w *= val[d][loc[d]];
+                A.w[s] = w;
+                for (int a = 0; a < D; ++a) {
+                    double g = der[a][loc[a]];
+                    for (int c = 0; c < D; ++c)
+                        if (c != a) g *= val[c][loc[c]];
+                    A.g[s][a] = g * hi;
+                    for (int b = 0; b < D; ++b) {
+                        double h = (a == b) ? d2[a][loc[a]] : der[a][loc[a]] * der[b][loc[b]];
+                        for (int c = 0; c < D; ++c)
+                            if (c != a && c != b) h *= val[c][loc[c]];
+                        A.H[s][a][b] = h * hi * hi;
+                    }
+                }
+            }
+}
+
+inline bool adjoint_supported(const tb_step_params& prm) {
+    return (prm.basis == TB_BSPLINE_QUADRATIC || prm.basis == TB_UGIMP) && prm.transfer == TB_TRANSFER_FLIP;
+}
+
+template <int D>
+inline double det_and_cof(const double (&F)[3][3], double (&C)[3][3]) {
+    if (D == 3) {
+        C[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+        C[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+        C[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+        C[1][0] = F[0][2] * F[2][1] - F[0][1] * F[2][2];
+        C[1][1] = F[0][0] * F[2][2] - F[0][2] * F[2][0];
+        C[1][2] = F[0][1] * F[2][0] - F[0][0] * F[2][1];
+        C[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
+        C[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+        C[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+        return F[0][0] * C[0][0] + F[0][1] * C[0][1] + F[0][2] * C[0][2];
+    }
+    C[0][0] = F[1][1];
+    C[0][1] = -F[1][0];
+    C[1][0] = -F[0][1];
+    C[1][1] = F[0][0];
+    return F[0][0] * F[1][1] - F[0][1] * F[1][0];
+}
+
+// Sensitivity of the loss to F, mu and lambda through sigma(F) and V = V0 det F
+// (Neo-Hookean sigma = (mu (F F^T - I) + lambda log J I) / J, or the fluid
+// sigma = lambda (J - 1) I), given sigma_bar (full D x D) and V_bar.
+template <int D>
+inline void constitutive_adjoint(const double (&F)[3][3], double mu, double lam, double V0, int material,
+                                 const double (&sb)[3][3], double Vb, double (&Fb)[3][3], double& mub,
+                                 double& lamb) {
+    double C[3][3] = {};
+    const double J = det_and_cof<D>(F, C);
+    double Jb = V0 * Vb;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) Fb[r][c] = 0.0;
+    mub = 0.0;
+    lamb = 0.0;
+    if (material == 1) {
+        double tr = 0.0;
+        for (int d = 0; d < D; ++d) tr += sb[d][d];
+        lamb += (J - 1.0) * tr;
+        Jb += lam * tr;
+    } else {
+        const double lj = std::log(J);
+        double Bm[3][3] = {}, tau[3][3] = {};
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double b = 0.0;
+                for (int k = 0; k < D; ++k) b += F[r][k] * F[c][k];
+                Bm[r][c] = b - (r == c ? 1.0 : 0.0);
+                tau[r][c] = mu * Bm[r][c] + (r == c ? lam * lj : 0.0);
+            }
+        double st = 0.0, trt = 0.0;
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                st += sb[r][c] * tau[r][c];
+                mub += (sb[r][c] / J) * Bm[r][c];
+            }
+        for (int d = 0; d < D; ++d) trt += sb[d][d] / J;
+        Jb += -st / (J * J) + lam * trt / J;
+        lamb += lj * trt;
+        // F_bar += (B_bar + B_bar^T) F with B_bar = mu sigma_bar / J
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double a = 0.0;
+                for (int k = 0; k < D; ++k) a += (mu / J) * (sb[r][k] + sb[k][r]) * F[k][c];
+                Fb[r][c] += a;
+            }
+    }
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) Fb[r][c] += Jb * C[r][c];
+}
+
+// One step backwards on the CPU. `p` is the state at the start of the step,
+// `g` receives the step's forward grid, `a` holds the sensitivities to the
+// end-of-step state on entry and to the start-of-step state on return.
+template <int D, class T>
+inline int adjoint_step(const Mesh<D, T>& M, tb_particles& p, tb_grid& g, const tb_step_params& prm,
+                        tb_adjoint& a) {
+    if (!adjoint_supported(prm)) return TB_ERR_UNSUPPORTED;
+    p2g<D, T>(M, p, g, prm);
+    grid_update<D, T>(M, g, prm);
+    const int64_t nn = M.nnodes;
+    const size_t ndn = static_cast<size_t>(D) * static_cast<size_t>(nn);
+    std::vector<double> vb(ndn, 0.0), vnb(ndn, 0.0), pb(ndn, 0.0), fb(ndn, 0.0);
+    std::vector<double> mb(static_cast<size_t>(nn), 0.0);
+    const double dt = prm.dt, alpha = prm.flip_alpha;
+    // ---- G2P backwards: particle sensitivities in place, grid v / vn sensitivities scattered
+    for (int64_t i = 0; i < p.n; ++i) {
+        T x[3] = {0, 0, 0};
+        for (int d = 0; d < D; ++d) x[d] = CP<T>(p.x[d])[i];
+        const T l = opt<T>(p.l, i, prm.gimp_l);
+        Weights<D, T> W;
+        compute_weights(M, prm.basis, x, l, W);
+        AdjWeights<D> A{};
+        if (!W.empty) adjoint_weights(M, prm.basis, x, l, W, A);
+        double L[3][3] = {};
+        auto for_nodes = [&](auto&& fn) {
+            if (W.empty) return;
+            for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+                for (int j = 0; j < W.cnt[1]; ++j)
+                    for (int ii = 0; ii < W.cnt[0]; ++ii) {
+                        const int s = ii + 3 * j + (D == 3 ? 9 * k : 0);
+                        int64_t node[3] = {W.lo[0] + ii, W.lo[1] + j, W.lo[2] + k};
+                        fn(s, node_linear<D>(M.n, node));
+                    }
+        };
+        for_nodes([&](int s, int64_t I) {
+            for (int r = 0; r < D; ++r)
+                for (int c = 0; c < D; ++c) L[r][c] += double(CP<T>(g.v[r])[I]) * A.g[s][c];
+        });
+        double F[3][3] = {}, Fb[3][3] = {};
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                F[r][c] = CP<double>(p.F[r + c * D])[i];
+                Fb[r][c] = a.F[r + c * D][i];
+            }
+        double Lb[3][3] = {}, Fbn[3][3] = {};
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double s1 = 0.0, s2 = 0.0;
+                for (int k = 0; k < D; ++k) {
+                    s1 += ((r == k ? 1.0 : 0.0) + dt * L[k][r]) * Fb[k][c];  // (I + dt L)^T F_bar
+                    s2 += Fb[r][k] * F[c][k];                                // F_bar F^T
+                }
+                Fbn[r][c] = s1;
+                Lb[r][c] = dt * s2;
+            }
+        double xb[3] = {}, vbp[3] = {}, dvb[3] = {}, vpb[3] = {};
+        for (int d = 0; d < D; ++d) {
+            xb[d] = a.x[d][i];
+            vbp[d] = a.v[d][i];
+            dvb[d] = alpha * vbp[d];
+            vpb[d] = (1.0 - alpha) * vbp[d] + dt * xb[d];
+        }
+        for_nodes([&](int s, int64_t I) {
+            double vi[3], vni[3], gb[3] = {0, 0, 0}, wb = 0.0;
+            for (int d = 0; d < D; ++d) {
+                vi[d] = double(CP<T>(g.v[d])[I]);
+                vni[d] = double(CP<T>(g.vn[d])[I]);
+            }
+            for (int r = 0; r < D; ++r) {
+                double lg = 0.0;
+                for (int c = 0; c < D; ++c) lg += Lb[r][c] * A.g[s][c];
+                vb[size_t(r) * nn + I] += A.w[s] * (vpb[r] + dvb[r]) + lg;
+                vnb[size_t(r) * nn + I] += -A.w[s] * dvb[r];
+                wb += vpb[r] * vi[r] + dvb[r] * (vi[r] - vni[r]);
+                for (int c = 0; c < D; ++c) gb[c] += Lb[r][c] * vi[r];
+            }
+            for (int b = 0; b < D; ++b) {
+                double h = 0.0;
+                for (int c = 0; c < D; ++c) h += A.H[s][b][c] * gb[c];
+                xb[b] += wb * A.g[s][b] + h;
+            }
+        });
+        for (int d = 0; d < D; ++d) {
+            a.x[d][i] = xb[d];
+            a.v[d][i] = alpha * vbp[d];
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) a.F[r + c * D][i] = Fbn[r][c];
+    }
+    // ---- grid update backwards (walled components were overwritten with 0)
+    for (int64_t I = 0; I < nn; ++I) {
+        const double m = double(CP<T>(g.m)[I]);
+        int64_t idx[3] = {0, 0, 0}, r = I;
+        for (int d = 0; d < D; ++d) { idx[d] = r % M.n[d]; r /= M.n[d]; }
+        double acc = 0.0;
+        for (int d = 0; d < D; ++d) {
+            double v_b = vb[size_t(d) * nn + I], vn_b = vnb[size_t(d) * nn + I];
+            const bool lo = (prm.wall_mask >> (2 * d)) & 1, hi = (prm.wall_mask >> (2 * d + 1)) & 1;
+            if ((lo && idx[d] < prm.wall_layers) || (hi && idx[d] >= M.n[d] - prm.wall_layers)) v_b = vn_b = 0.0;
+            if (m == 0.0) continue;
+            const double vt = vn_b + v_b;
+            fb[size_t(d) * nn + I] = dt * v_b / m;
+            pb[size_t(d) * nn + I] = vt / m;
+            acc += vt * double(CP<T>(g.mv[d])[I]) + dt * v_b * double(CP<T>(g.f[d])[I]);
+        }
+        mb[I] = (m == 0.0) ? 0.0 : -acc / (m * m);
+    }
+    // ---- P2G backwards: gather into x, v and (through sigma, V) into F, mu, lambda
+    for (int64_t i = 0; i < p.n; ++i) {
+        ParticleIn<D, T> q;
+        load_particle<D, T>(p, prm, i, q);
+        Weights<D, T> W;
+        compute_weights(M, prm.basis, q.x, q.l, W);
+        double xb[3] = {}, vbs[3] = {}, sb[3][3] = {}, Vb = 0.0;
+        if (!W.empty) {
+            AdjWeights<D> A{};
+            adjoint_weights(M, prm.basis, q.x, q.l, W, A);
+            const double mp = double(q.m), Vp = double(q.V);
+            for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+                for (int j = 0; j < W.cnt[1]; ++j)
+                    for (int ii = 0; ii < W.cnt[0]; ++ii) {
+                        const int s = ii + 3 * j + (D == 3 ? 9 * k : 0);
+                        int64_t node[3] = {W.lo[0] + ii, W.lo[1] + j, W.lo[2] + k};
+                        const int64_t I = node_linear<D>(M.n, node);
+                        double wb = mp * mb[I];
+                        double gb[3] = {0, 0, 0};
+                        for (int d = 0; d < D; ++d) {
+                            const double p_b = pb[size_t(d) * nn + I], f_b = fb[size_t(d) * nn + I];
+                            wb += mp * (double(q.v[d]) * p_b + double(T(prm.gravity[d])) * f_b);
+                            vbs[d] += mp * A.w[s] * p_b;
+                        }
+                        for (int r = 0; r < D; ++r) {
+                            const double f_b = fb[size_t(r) * nn + I];
+                            double sg = 0.0;
+                            for (int c = 0; c < D; ++c) {
+                                sg += double(q.sig[r][c]) * A.g[s][c];
+                                gb[c] += -Vp * double(q.sig[r][c]) * f_b;
+                                sb[r][c] += -Vp * f_b * A.g[s][c];
+                            }
+                            Vb += -f_b * sg;
+                        }
+                        for (int b = 0; b < D; ++b) {
+                            double h = 0.0;
+                            for (int c = 0; c < D; ++c) h += A.H[s][b][c] * gb[c];
+                            xb[b] += wb * A.g[s][b] + h;
+                        }
+                    }
+        }
+        double F[3][3] = {}, Fb[3][3] = {}, mub = 0.0, lamb = 0.0;
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) F[r][c] = CP<double>(p.F[r + c * D])[i];
+        const double mu = p.mu ? double(CP<T>(p.mu)[i]) : prm.mu;
+        const double lam = p.lambda ? double(CP<T>(p.lambda)[i]) : prm.lambda;
+        const double V0 = p.V0 ? double(CP<T>(p.V0)[i]) : prm.V0;
+        constitutive_adjoint<D>(F, mu, lam, V0, prm.material, sb, Vb, Fb, mub, lamb);
+        for (int d = 0; d < D; ++d) {
+            a.x[d][i] += xb[d];
+            a.v[d][i] += vbs[d];
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) a.F[r + c * D][i] += Fb[r][c];
+        if (a.mu) a.mu[i] += mub;
+        if (a.lambda) a.lambda[i] += lamb;
+    }
+    return TB_OK;
+}
+
+// ---------------------------------------------------------------------------
 // colour-phased multithreaded step (src/Parallel/region.jl:212-256 with the
 // CPUBlockStrategy partition): blocks of one colour share no support node
 // because the block width (4 cells) exceeds the window reach, so the blocks of

@@ -6,18 +6,19 @@ weights, the block partition and the recognised @P2G / @G2P equation sets) that
 calls the CUDA kernels through the C ABI declared in include/tesserae_b200.h.
 """
 from . import _abi
-from .state import (BasisWeights, CartesianMesh, Grid, Particles, Partition, generate_basis_weights,
+from .state import (Adjoint, BasisWeights, CartesianMesh, Grid, Particles, Partition, generate_basis_weights,
                     generate_grid, lame, step_params)
 from . import scenes
 
-__all__ = ["_abi", "BasisWeights", "CartesianMesh", "Grid", "Particles", "Partition", "generate_basis_weights",
+__all__ = ["_abi", "Adjoint", "BasisWeights", "CartesianMesh", "Grid", "Particles", "Partition", "generate_basis_weights",
            "generate_grid", "lame", "step_params", "scenes"]
 
 
 def __getattr__(name):
     # The device API needs torch and the built library; import it lazily so the
     # host-only parts (scenes, containers) load without either.
-    if name in ("runtime", "Context", "update", "P2G", "G2P", "step", "rollout_host"):
+    if name in ("runtime", "Context", "update", "P2G", "G2P", "step", "rollout_host", "adjoint_step",
+                "tape_forward", "tape_backward", "rollout_grad", "RolloutFunction"):
         import importlib
         runtime = importlib.import_module(__name__ + ".runtime")
         return runtime if name == "runtime" else getattr(runtime, name)

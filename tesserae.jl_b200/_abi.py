@@ -98,6 +98,10 @@ class tb_step_params(C.Structure):
     ]
 
 
+class tb_adjoint(C.Structure):
+    _fields_ = [("x", VP * 3), ("v", VP * 3), ("F", VP * 9), ("mu", VP), ("lambda_", VP)]
+
+
 class tb_kernel_time(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("ms", C.c_double)]
 
@@ -128,6 +132,12 @@ for _p in ("f64", "f32"):
         (f"tb_g2p_{_p}", I32, [VP, P(tb_mesh), P(tb_grid), P(tb_particles), P(tb_step_params)]),
         (f"tb_step_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params), I32]),
         (f"tb_rollout_host_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
+        (f"tb_adjoint_step_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                        P(tb_step_params), P(tb_adjoint)]),
+        (f"tb_tape_forward_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                        P(tb_step_params), I32, I32]),
+        (f"tb_tape_backward_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                         P(tb_step_params), P(tb_adjoint)]),
     ]
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent

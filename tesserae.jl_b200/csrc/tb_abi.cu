@@ -99,6 +99,18 @@ struct tb_ctx {
     // context-owned state for tb_rollout_host_*
     void* roll_buf = nullptr;
     size_t roll_cap = 0;
+    // reverse mode: FP64 grid sensitivities (13 components x nnodes)
+    double* adj_grid = nullptr;
+    long long adj_grid_cap = 0;
+    // checkpoint tape: states at steps 0, K, 2K, ... and one segment of K states
+    char* tape_cp = nullptr;
+    long long tape_cp_cap = 0;
+    char* tape_seg = nullptr;
+    long long tape_seg_cap = 0;
+    bool tape_valid = false;
+    long long tape_n = 0;
+    int tape_dim = 0, tape_elem = 0;
+    int tape_nsteps = 0, tape_every = 1;
 };
 
 namespace {
@@ -564,6 +576,218 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     return check_device_status(c);
 }
 
+// ---------------------------------------------------------------------------
+// reverse mode
+// ---------------------------------------------------------------------------
+
+int check_adjoint_params(tb_ctx* c, const tb_step_params* p) {
+    int rc = check_params(c, p);
+    if (rc != TB_OK) return rc;
+    if (p->basis != TB_BSPLINE_QUADRATIC && p->basis != TB_UGIMP)
+        return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the quadratic B-spline and uGIMP bases (basis %d)",
+                    p->basis);
+    if (p->transfer != TB_TRANSFER_FLIP)
+        return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the FLIP/PIC transfer only");
+    return TB_OK;
+}
+
+int make_adjview(tb_ctx* c, const tb_adjoint* a, int dim, long long n, AdjView& A) {
+    if (!a) return fail(c, TB_ERR_ARG, "adjoint is NULL");
+    std::memset(&A, 0, sizeof A);
+    for (int d = 0; d < dim; ++d) {
+        A.x[d] = a->x[d];
+        A.v[d] = a->v[d];
+        if (n && (!A.x[d] || !A.v[d])) return fail(c, TB_ERR_ARG, "adjoint.x/v component %d is NULL", d);
+    }
+    for (int k = 0; k < dim * dim; ++k) {
+        A.F[k] = a->F[k];
+        if (n && !A.F[k]) return fail(c, TB_ERR_ARG, "adjoint.F component %d is NULL", k);
+    }
+    A.mu = a->mu;
+    A.lam = a->lambda;
+    return TB_OK;
+}
+
+int grad_grid(tb_ctx* c, int dim, long long nn, GradGrid& GB) {
+    const long long need = nn * (1 + 4 * dim);
+    cudaError_t e = grow(c->adj_grid, c->adj_grid_cap, need);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc grid sensitivities");
+    std::memset(&GB, 0, sizeof GB);
+    double* q = c->adj_grid;
+    for (int d = 0; d < dim; ++d) GB.vb[d] = q + nn * d;
+    q += nn * dim;
+    for (int d = 0; d < dim; ++d) GB.vnb[d] = q + nn * d;
+    q += nn * dim;
+    GB.mb = q;
+    q += nn;
+    for (int d = 0; d < dim; ++d) GB.pb[d] = q + nn * d;
+    q += nn * dim;
+    for (int d = 0; d < dim; ++d) GB.fb[d] = q + nn * d;
+    return TB_OK;
+}
+
+// Recompute the step's partition and forward grid from `p`, then run the three
+// backward kernels.
+template <int D, class T, int BW>
+int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                 const tb_step_params* prm, const tb_adjoint* adj) {
+    int rc = run_step<D, T, BW>(c, m, p, part, g, prm, 1, true, true, true, false);
+    if (rc != TB_OK) return rc;
+    const auto M = make_dmesh<D, T>(*m);
+    const auto S = make_scalars<T>(*prm);
+    PView<T> P;
+    GView<T> G;
+    AdjView A;
+    GradGrid GB;
+    if ((rc = make_pview<T>(c, p, D, true, false, P)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    if ((rc = make_adjview(c, adj, D, P.n, A)) != TB_OK) return rc;
+    if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
+    const cudaError_t e = launch_adjoint<D, T>(M, G, P, S, A, GB, cfg_of(c));
+    return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "adjoint launch");
+}
+
+template <class T>
+int adjoint_dispatch(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                     const tb_step_params* prm, const tb_adjoint* adj) {
+    if (m->dim == 3) return adjoint_impl<3, T, 4>(c, m, p, part, g, prm, adj);
+    if (m->block_log2 == 3) return adjoint_impl<2, T, 8>(c, m, p, part, g, prm, adj);
+    return adjoint_impl<2, T, 4>(c, m, p, part, g, prm, adj);
+}
+
+template <class T>
+int do_adjoint_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                    const tb_step_params* prm, const tb_adjoint* adj) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
+        return rc;
+    return adjoint_dispatch<T>(c, m, p, part, g, prm, adj);
+}
+
+// The state tb_step_* reads and writes, as (particle array, element size)
+// fields: x, v (T), F (double), sigma (T), V (T). grad_v is output only.
+struct StateFields {
+    int count = 0;
+    void** slot[32];
+    size_t elem[32];
+};
+
+template <class T>
+StateFields state_fields(tb_particles* p, int D) {
+    StateFields f;
+    auto add = [&](void** s, size_t e) {
+        f.slot[f.count] = s;
+        f.elem[f.count] = e;
+        ++f.count;
+    };
+    for (int d = 0; d < D; ++d) add(&p->x[d], sizeof(T));
+    for (int d = 0; d < D; ++d) add(&p->v[d], sizeof(T));
+    for (int k = 0; k < D * D; ++k) add(&p->F[k], sizeof(double));
+    for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&p->sigma[k], sizeof(T));
+    add(&p->V, sizeof(T));
+    return f;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+template <class T>
+size_t state_bytes(int D, long long n) {
+    const int nf = 2 * D + (D == 3 ? 6 : 3) + 1;
+    return size_t(nf) * align256(sizeof(T) * size_t(n)) + size_t(D * D) * align256(sizeof(double) * size_t(n));
+}
+
+// Particles whose state fields point into the snapshot at `base`.
+template <class T>
+tb_particles snapshot_view(const tb_particles* p, int D, char* base) {
+    tb_particles q = *p;
+    StateFields f = state_fields<T>(&q, D);
+    size_t off = 0;
+    for (int i = 0; i < f.count; ++i) {
+        *f.slot[i] = base + off;
+        off += align256(f.elem[i] * size_t(p->n));
+    }
+    return q;
+}
+
+template <class T>
+int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int D) {
+    StateFields fd = state_fields<T>(const_cast<tb_particles*>(dst), D);
+    StateFields fs = state_fields<T>(const_cast<tb_particles*>(src), D);
+    for (int i = 0; i < fd.count; ++i) {
+        if (!*fs.slot[i] || !*fd.slot[i]) return fail(c, TB_ERR_ARG, "particle state field %d is NULL", i);
+        const cudaError_t e = cudaMemcpyAsync(*fd.slot[i], *fs.slot[i], fd.elem[i] * size_t(src->n),
+                                              cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "state copy");
+    }
+    return TB_OK;
+}
+
+template <class T>
+int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                    const tb_step_params* prm, int nsteps, int every) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
+        return rc;
+    if (nsteps < 0 || every < 1) return fail(c, TB_ERR_ARG, "nsteps must be >= 0 and checkpoint_every >= 1");
+    if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
+    const int D = m->dim;
+    PView<T> P;
+    if ((rc = make_pview<T>(c, p, D, true, false, P)) != TB_OK) return rc;
+    c->tape_valid = false;
+    const long long ncp = nsteps > 0 ? (nsteps + every - 1) / every : 1;
+    const size_t sb = state_bytes<T>(D, p->n);
+    cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(ncp * sb));
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc checkpoints");
+    for (long long k = 0; k < ncp; ++k) {
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb);
+        if ((rc = copy_state<T>(c, &cp, p, D)) != TB_OK) return rc;
+        const int steps = std::min<long long>(every, nsteps - k * every);
+        if (steps > 0 && (rc = dispatch_step<T>(c, m, p, part, g, prm, steps, true, true, true, true)) != TB_OK)
+            return rc;
+    }
+    c->tape_valid = true;
+    c->tape_n = p->n;
+    c->tape_dim = D;
+    c->tape_elem = int(sizeof(T));
+    c->tape_nsteps = nsteps;
+    c->tape_every = every;
+    return TB_OK;
+}
+
+template <class T>
+int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                     const tb_step_params* prm, const tb_adjoint* adj) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
+        return rc;
+    if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
+    const int D = m->dim;
+    if (!c->tape_valid || c->tape_n != p->n || c->tape_dim != D || c->tape_elem != int(sizeof(T)))
+        return fail(c, TB_ERR_ARG, "no forward tape for these particles on this context (run tb_tape_forward first)");
+    const int K = c->tape_every, nsteps = c->tape_nsteps;
+    const size_t sb = state_bytes<T>(D, p->n);
+    cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * sb));
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape segment");
+    const long long ncp = nsteps > 0 ? (nsteps + K - 1) / K : 1;
+    for (long long k = ncp - 1; k >= 0 && nsteps > 0; --k) {
+        const int len = int(std::min<long long>(K, nsteps - k * K));
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb);
+        if ((rc = copy_state<T>(c, p, &cp, D)) != TB_OK) return rc;
+        for (int j = 0; j < len; ++j) {
+            tb_particles sj = snapshot_view<T>(p, D, c->tape_seg + j * sb);
+            if ((rc = copy_state<T>(c, &sj, p, D)) != TB_OK) return rc;
+            if (j + 1 < len && (rc = dispatch_step<T>(c, m, p, part, g, prm, 1, true, true, true, true)) != TB_OK)
+                return rc;
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            tb_particles sj = snapshot_view<T>(p, D, c->tape_seg + j * sb);
+            if ((rc = adjoint_dispatch<T>(c, m, &sj, part, g, prm, adj)) != TB_OK) return rc;
+        }
+    }
+    tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp);
+    return copy_state<T>(c, p, &cp0, D);
+}
+
 }  // namespace
 
 extern "C" {
@@ -602,6 +826,9 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->roll_buf);
     cudaFree(c->touched_cur);
     cudaFree(c->touched_prev);
+    cudaFree(c->adj_grid);
+    cudaFree(c->tape_cp);
+    cudaFree(c->tape_seg);
     delete c->prof;
     delete c;
 }
@@ -716,6 +943,32 @@ int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, con
 int32_t tb_rollout_host_f32(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
                             int32_t nsteps) {
     return do_rollout<float>(c, m, host, prm, nsteps);
+}
+
+int32_t tb_adjoint_step_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, tb_adjoint* adj) {
+    return do_adjoint_step<double>(c, m, p, part, g, prm, adj);
+}
+int32_t tb_adjoint_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, tb_adjoint* adj) {
+    return do_adjoint_step<float>(c, m, p, part, g, prm, adj);
+}
+
+int32_t tb_tape_forward_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, int32_t nsteps, int32_t every) {
+    return do_tape_forward<double>(c, m, p, part, g, prm, nsteps, every);
+}
+int32_t tb_tape_forward_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, int32_t nsteps, int32_t every) {
+    return do_tape_forward<float>(c, m, p, part, g, prm, nsteps, every);
+}
+int32_t tb_tape_backward_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                             const tb_step_params* prm, tb_adjoint* adj) {
+    return do_tape_backward<double>(c, m, p, part, g, prm, adj);
+}
+int32_t tb_tape_backward_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                             const tb_step_params* prm, tb_adjoint* adj) {
+    return do_tape_backward<float>(c, m, p, part, g, prm, adj);
 }
 
 }  // extern "C"

@@ -92,6 +92,29 @@ template <int D, class T>
 cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
                               const LaunchCfg& cfg);
 
+// Reverse mode: the caller's FP64 sensitivity arrays (tb_adjoint) and the
+// context's FP64 grid sensitivities (component-major, nnodes each).
+struct AdjView {
+    double* x[3];
+    double* v[3];
+    double* F[9];
+    double* mu;
+    double* lam;
+};
+struct GradGrid {
+    double* vb[3];   // d loss / d v_i (scattered by G2P backwards)
+    double* vnb[3];  // d loss / d vn_i
+    double* mb;      // d loss / d m_i
+    double* pb[3];   // d loss / d mv_i
+    double* fb[3];   // d loss / d f_i
+};
+
+// G2P, grid update and P2G backwards for one step whose forward grid is in G
+// (tb_adjoint.cu). Zeroes GB's v / vn sensitivities first.
+template <int D, class T>
+cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                           const AdjView& A, const GradGrid& GB, const LaunchCfg& cfg);
+
 template <int D, class T>
 cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* grad_w,
                                   long long* window, const LaunchCfg& cfg);

@@ -30,9 +30,12 @@
 // equal exponent, costs the same 8 bytes per value as a (hi, lo) FP32 Kahan pair,
 // and a shared-memory f64 atomic add runs at 1.8x the rate of an FP32 atomic add
 // followed by an exact two-sum of its rounding error (1.50 vs 0.84 T op/s
-// measured on B200). After the last batch the tile is flushed with one global
+// measured on B200). A plain FP32 tile without compensation would save 0.45 ms
+// of a 4.9 ms cube3d step. After the last batch the tile is flushed with one global
 // atomic per non-zero node value (gravity, sum w m g = g sum w m, is added there
-// from the tile mass).
+// from the tile mass). (Writing the tiles to a staging array and summing the at
+// most 2^D tiles of each node in a fused grid pass was measured slower on
+// cube3d: 3.26 vs 3.04 ms for P2G plus the grid work.)
 #include "tb_launch.cuh"
 
 namespace tb {
@@ -92,13 +95,16 @@ __host__ __device__ constexpr size_t tile_bytes() {
     return ((sizeof(double) * NCTN + 15) / 16) * 16;
 }
 
+// 9 warps: the 25 pencils of a 3D block fill 27 (warp, pencil) slots, one task per warp.
+constexpr int P2G_THREADS = 288;
+
 template <int D, class T, int BW, bool GEN, int NR>
-__global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
+__global__ void __launch_bounds__(P2G_THREADS, (sizeof(T) == 4 && !GEN) ? 2 : 1) p2g_group_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
                                                           const int* __restrict__ totals,
                                                           const int* __restrict__ blocklist,
                                                           const int* __restrict__ offsets,
                                                           const int* __restrict__ perm, int* err) {
-    constexpr int NT = 256;
+    constexpr int NT = P2G_THREADS;
     constexpr int TS = BW + 3;
     constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
     constexpr int NC = 1 + 2 * D;
@@ -108,6 +114,8 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
     constexpr int NW = NT / 32;
     constexpr int NJK = (D == 3) ? 9 : 3;  // window rows
     constexpr int NSUB = 32 / NJK;         // pencils per warp: 3 (3D), 10 (2D)
+    constexpr int NPENCIL = NG / G1;
+    constexpr int NTASK = (NPENCIL + NSUB - 1) / NSUB;  // 9 in 3D: one per warp
     using R = Rec<D, GEN>;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -115,7 +123,7 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
     T* rec = reinterpret_cast<T*>(smem_raw + tile_bytes<NC * TN>());
     int* gcount = reinterpret_cast<int*>(rec + NR * RS);
     int* gstart = gcount + NG;
-    int* order = gstart + NG + 1;
+    int* pslot = gstart + NG + 1;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nactive = totals[0];
@@ -141,10 +149,11 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
             const int nbat = min(NR, s1 - b0);
             for (int g = tid; g < NG; g += NT) gcount[g] = 0;
             __syncthreads();
-            // ---- 1. records + group histogram
-            int grp[NR / NT], rank[NR / NT];
+            // ---- 1a. group (window start) and rank of every particle of the batch
+            constexpr int ITEMS = (NR + NT - 1) / NT;
+            int grp[ITEMS], rank[ITEMS];
 #pragma unroll
-            for (int u = 0; u < NR / NT; ++u) {
+            for (int u = 0; u < ITEMS; ++u) {
                 const int ti = tid + u * NT;
                 grp[u] = -1;
                 rank[u] = 0;
@@ -155,7 +164,11 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
                 for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
                 const T l = P.l ? P.l[p] : s.gimp_l;
                 Basis<D, T> B;
-                if (!prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) continue;
+                if (!prepare_basis<D, T, false>(M, s.basis == TB_WLS_UGIMP ? TB_UGIMP
+                                                   : (s.basis == TB_WLS_BSPLINE_QUADRATIC ? TB_BSPLINE_QUADRATIC
+                                                                                           : s.basis),
+                                                x, l, B, err))
+                    continue;
                 int gi = 0;
                 bool ok = true;
 #pragma unroll
@@ -168,7 +181,55 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
                     atomicOr(err, ERR_TILE_RANGE);
                     continue;
                 }
-                T* r = rec + ti * RS;
+                grp[u] = gi;
+                rank[u] = atomicAdd(&gcount[gi], 1);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                int carry = 0;
+                for (int g0 = 0; g0 < NG; g0 += 32) {
+                    const int g = g0 + lane;
+                    const int c = g < NG ? gcount[g] : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    if (g < NG) gstart[g] = carry + incl - c;
+                    carry += __shfl_sync(0xffffffffu, incl, 31);
+                }
+                if (lane == 0) gstart[NG] = carry;
+            } else if (warp == 1) {
+                // Pencil slots by size, largest first, so the NSUB pencils a warp
+                // sweeps in lockstep have similar lengths.
+                int myp = lane < NPENCIL ? lane : -1;
+                int mysize = 0;
+                if (myp >= 0) {
+                    const int gb = G1 * myp;
+                    for (int gx = 0; gx < G1; ++gx) mysize += gcount[gb + gx];
+                }
+                int rk = 0;
+                for (int o = 0; o < NPENCIL; ++o) {
+                    const int os = __shfl_sync(0xffffffffu, mysize, o);
+                    rk += (os > mysize) || (os == mysize && o < lane);
+                }
+                if (myp >= 0) pslot[rk] = myp;
+            }
+            __syncthreads();
+            // ---- 1b. records, written at their group-sorted position
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                if (grp[u] < 0) continue;
+                const int ti = tid + u * NT;
+                const long long p = perm[b0 + ti] - 1;
+                T x[3];
+#pragma unroll
+                for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+                const T l = P.l ? P.l[p] : s.gimp_l;
+                Basis<D, T> B;
+                prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err);
+                T* r = rec + (gstart[grp[u]] + rank[u]) * RS;
                 const T mp = P.m ? P.m[p] : s.mass;
                 const T Vp = P.V[p];
                 T v[3] = {T(0), T(0), T(0)};
@@ -210,39 +271,15 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
 #pragma unroll
                     for (int k = 0; k < D * D; ++k) r[R::BP + k] = apic ? P.B[k][p] : T(0);
                 }
-                grp[u] = gi;
-                rank[u] = atomicAdd(&gcount[gi], 1);
             }
-            __syncthreads();
-            if (warp == 0) {
-                int carry = 0;
-                for (int g0 = 0; g0 < NG; g0 += 32) {
-                    const int g = g0 + lane;
-                    const int c = g < NG ? gcount[g] : 0;
-                    int incl = c;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += t;
-                    }
-                    if (g < NG) gstart[g] = carry + incl - c;
-                    carry += __shfl_sync(0xffffffffu, incl, 31);
-                }
-                if (lane == 0) gstart[NG] = carry;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < NR / NT; ++u)
-                if (grp[u] >= 0) order[gstart[grp[u]] + rank[u]] = tid + u * NT;
             __syncthreads();
             // ---- 2./3. pencils of groups along x: the NSUB lane sets of a warp
             //      walk NSUB different pencils, so every lane owns its (pencil, row)
             //      and adds its sums to the tile without any cross-lane reduction.
-            constexpr int NPENCIL = NG / G1;
-            constexpr int NTASK = (NPENCIL + NSUB - 1) / NSUB;
             for (int task = warp; task < NTASK; task += NW) {
-                const int pc = task * NSUB + sub;
-                const bool live = sub < NSUB && pc < NPENCIL;
+                const int slot = task * NSUB + sub;
+                const bool live = sub < NSUB && slot < NPENCIL;
+                const int pc = live ? pslot[slot] : 0;
                 const int gy = live ? pc % G1 : 0, gz = (D == 3 && live) ? pc / G1 : 0;
                 const int gbase = G1 * (gy + G1 * gz);
                 T acc[3][NC];
@@ -260,7 +297,7 @@ __global__ void __launch_bounds__(256, 2) p2g_group_kernel(DMesh<D, T> M, PView<
                     if (gx < G1 && live) {
                         const int q1 = gstart[gbase + gx + 1];
                         for (int q = gstart[gbase + gx]; q < q1; ++q) {
-                            const T* r = rec + order[q] * RS;
+                            const T* r = rec + q * RS;
                             const V4<T> m4 = ld4(r + 0), s4 = ld4(r + 4), x4 = ld4(r + 12);
                             const V2<T> s2 = ld2(r + 8), x2 = ld2(r + 16), y2 = ld2(r + R::AX + 6 + 2 * sj);
                             const T mp = m4.a;
@@ -408,7 +445,7 @@ size_t p2g_smem_bytes() {
     constexpr int NG = (D == 3) ? (BW + 1) * (BW + 1) * (BW + 1) : (BW + 1) * (BW + 1);
     const size_t tiles = tile_bytes<NC * TN>();
     const size_t recs = sizeof(T) * size_t(NR) * Rec<D, GEN>::SIZE;
-    const size_t ints = sizeof(int) * size_t(NG + NG + 1 + NR);
+    const size_t ints = sizeof(int) * size_t(NG + NG + 1 + 32);
     return tiles + recs + ints;
 }
 
@@ -423,10 +460,10 @@ cudaError_t launch_group(const DMesh<D, T>& M, const PView<T>& P, const GView<T>
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2G_THREADS, smem);
     const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
     KernelScope ks(cfg, "p2g");
-    kern<<<grid, 256, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
     ++*cfg.launches;
     return cudaGetLastError();
 }

@@ -6,6 +6,8 @@ C ABI of libtesserae_b200.so.
   P2G(grid, particles, partition, mesh, params) @P2G (m, mv, f sums + grid half)        p2g.jl:66, gpu.jl:196
   G2P(grid, particles, mesh, params)            @G2P (FLIP/APIC + Neo-Hookean)          g2p.jl:71, gpu.jl:226
   step(...)                                     the whole README.md:66-87 loop body, n times
+  adjoint_step / tape_forward / tape_backward   reverse mode (no reference counterpart)
+  rollout_grad                                  gradients of a rollout loss w.r.t. v0 and log E
 
 The precision form follows the particle dtype: float64 -> the plain `_f64`
 entry points, float32 (F float64) -> the mixed `_f32` ones. Every call raises
@@ -19,7 +21,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from .state import BasisWeights, CartesianMesh, Grid, Particles, Partition
+from .state import Adjoint, BasisWeights, CartesianMesh, Grid, Particles, Partition
 
 
 def _suffix(dtype) -> str:
@@ -152,6 +154,101 @@ def rollout_host(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     rc = ctx.fn("tb_rollout_host", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(params), int(nsteps))
     ctx.check(rc, "rollout_host")
+
+
+def adjoint_step(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+                 adj: Adjoint, ctx: Context | None = None):
+    """One step backwards: `particles` is the state at the start of the step;
+    `adj` (float64 device arrays) maps end-of-step sensitivities to start-of-step
+    ones in place (mu / lam accumulate)."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_adjoint_step", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                    _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                                    _ref(adj.struct()))
+    ctx.check(rc, "adjoint_step")
+
+
+def tape_forward(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+                 nsteps: int, checkpoint_every: int = 20, ctx: Context | None = None):
+    """Advance `nsteps` steps (as `step`) keeping checkpoints every `checkpoint_every` steps."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_tape_forward", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                    _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                                    int(nsteps), int(checkpoint_every))
+    ctx.check(rc, "tape_forward")
+
+
+def tape_backward(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+                  adj: Adjoint, ctx: Context | None = None):
+    """Sensitivities to the final state (in `adj`) -> sensitivities to the step-0
+    state; `particles` is restored to the step-0 state."""
+    ctx = ctx or _default()
+    rc = ctx.fn("tb_tape_backward", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                                     _ref(adj.struct()))
+    ctx.check(rc, "tape_backward")
+
+
+def rollout_grad(particles: Particles, mesh: CartesianMesh, params, nsteps: int, loss_grad,
+                 checkpoint_every: int = 20, nu: float | None = None, ctx: Context | None = None):
+    """Gradients of a rollout loss with respect to the initial velocities and the
+    per-particle log Young's modulus.
+
+    `loss_grad(particles_final) -> (loss, dL/dx, dL/dv)` gives the loss and its
+    sensitivities to the final positions and velocities (float64 tensors of
+    shape (dim, n)). With per-particle Lame arrays (particles.mu / particles.lam)
+    and E entering both as mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)),
+    dL/dlogE = mu dL/dmu + lambda dL/dlambda. `particles` is left in its initial
+    state. Returns (loss, dL/dv0, dL/dlogE or None)."""
+    import torch
+    ctx = ctx or _default()
+    D, n = particles.dim, particles.n
+    part = Partition(mesh, n, backend="torch", device=particles.device or "cuda")
+    grid = Grid(mesh, particles.dtype, backend="torch", device=particles.device or "cuda")
+    tape_forward(grid, particles, part, mesh, params, nsteps, checkpoint_every, ctx=ctx)
+    loss, gx, gv = loss_grad(particles)
+    lame = particles.mu is not None and particles.lam is not None
+    adj = Adjoint(n, D, backend="torch", device=particles.device or "cuda", lame=lame)
+    adj.x.copy_(gx)
+    adj.v.copy_(gv)
+    tape_backward(grid, particles, part, mesh, params, adj, ctx=ctx)
+    glogE = None
+    if lame:
+        glogE = adj.mu * particles.mu.double() + adj.lam * particles.lam.double()
+    torch.cuda.current_stream().synchronize()
+    return loss, adj.v, glogE
+
+
+class RolloutFunction:
+    """torch.autograd.Function over the checkpointed rollout: forward maps the
+    initial velocities (dim, n) to the final positions (dim, n); backward runs the
+    adjoint tape. The counterpart of a ChainRulesCore rrule on the Julia side."""
+
+    @staticmethod
+    def apply(v0, particles: Particles, mesh: CartesianMesh, params, nsteps: int, checkpoint_every: int = 20,
+              ctx: Context | None = None):
+        import torch
+
+        class _F(torch.autograd.Function):
+            @staticmethod
+            def forward(fctx, v):
+                c = ctx or _default()
+                particles.v.copy_(v.to(particles.v.dtype))
+                fctx.part = Partition(mesh, particles.n, backend="torch", device=v.device)
+                fctx.grid = Grid(mesh, particles.dtype, backend="torch", device=v.device)
+                tape_forward(fctx.grid, particles, fctx.part, mesh, params, nsteps, checkpoint_every, ctx=c)
+                xT = particles.x.detach().double().clone()
+                return xT
+
+            @staticmethod
+            def backward(fctx, gx):
+                c = ctx or _default()
+                adj = Adjoint(particles.n, particles.dim, backend="torch", device=gx.device, lame=False)
+                adj.x.copy_(gx.double())
+                tape_backward(fctx.grid, particles, fctx.part, mesh, params, adj, ctx=c)
+                return adj.v.to(v0.dtype)
+
+        return _F.apply(v0)
 
 
 _ctx = None

@@ -154,7 +154,9 @@ def clusters3d(scale: int = 1, n_total: int = 32 * 1024 * 1024, seed: int | None
 def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
     """64^3 cells (h = 1/64), sphere r = 0.3 at (0.5, 0.5, 0.5), 4 particles per cell
     per axis on a lattice jittered by U[-l/4, l/4], per-particle log E = log(1e5) +
-    N(0, 0.1), nu = 0.3, rho0 = 1e3, dt = 5e-4, 200 steps."""
+    N(0, 0.1), nu = 0.3, rho0 = 1e3, dt = 5e-4, 200 steps. The initial velocity is
+    not part of the configuration; it is set to (0, 0, 0.5) + U[-0.1, 0.1]^3 per
+    particle, so the sphere moves toward the loss target (0.5, 0.5, 0.8) and deforms."""
     cells = 64 // scale
     h = 1.0 / 64
     L = cells * h
@@ -173,6 +175,8 @@ def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
     V0 = lp ** 3
     P.V[...] = V0
     logE = np.log(1e5) + rng.normal(0.0, 0.1, size=n)
+    P.v[...] = rng.uniform(-0.1, 0.1, size=(3, n))
+    P.v[2] += 0.5
     mu, lam = lame(np.exp(logE), 0.3)
     P.mu[...] = mu
     P.lam[...] = lam

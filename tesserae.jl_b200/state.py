@@ -228,6 +228,54 @@ class Particles:
         return out
 
 
+class Adjoint:
+    """Sensitivities of a scalar loss to the particle state (x, v, F) and to the
+    per-particle Lame parameters, all float64 in both precision forms (the
+    tb_adjoint descriptor). `mu` / `lam` accumulate across steps."""
+
+    def __init__(self, n, dim, backend="numpy", device=None, lame=True):
+        self.n, self.dim, self.backend = int(n), int(dim), backend
+        D = self.dim
+        a = lambda shape: _alloc(backend, shape, np.float64, device, 0.0)  # noqa: E731
+        self.x = a((D, self.n))
+        self.v = a((D, self.n))
+        self.F = a((D * D, self.n))
+        self.mu = a((self.n,)) if lame else None
+        self.lam = a((self.n,)) if lame else None
+
+    def zero_(self):
+        for k in ("x", "v", "F", "mu", "lam"):
+            arr = getattr(self, k)
+            if arr is None:
+                continue
+            if isinstance(arr, np.ndarray):
+                arr.fill(0.0)
+            else:
+                arr.zero_()
+        return self
+
+    def struct(self) -> _abi.tb_adjoint:
+        s = _abi.tb_adjoint()
+        D = self.dim
+        for d, p in enumerate(_row_ptrs(self.x, D)):
+            s.x[d] = p
+        for d, p in enumerate(_row_ptrs(self.v, D)):
+            s.v[d] = p
+        for k, p in enumerate(_row_ptrs(self.F, D * D)):
+            s.F[k] = p
+        s.mu = _ptr(self.mu)
+        s.lambda_ = _ptr(self.lam)
+        return s
+
+    def numpy(self) -> dict:
+        out = {}
+        for k in ("x", "v", "F", "mu", "lam"):
+            a = getattr(self, k)
+            if a is not None:
+                out[k] = a if isinstance(a, np.ndarray) else a.detach().cpu().numpy()
+        return out
+
+
 class Grid:
     """SoA grid fields m, mv, f, v, vn over prod(n_nodes) column-major nodes."""
 
