@@ -200,6 +200,101 @@ def active_nodes(mesh, particles_np) -> int:
     return int(mask.sum())
 
 
+def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions: int = 2) -> dict:
+    """Differentiable rollout on the sphere scene (64^3 cells, ~1.9M particles,
+    200 steps, checkpoint every 20), mixed FP32 form: device time of the plain
+    forward rollout, the taped forward and the backward pass for the
+    centre-of-mass loss, plus directional derivatives of a linear loss on the
+    final positions against central differences of the FP64 device rollout."""
+    import torch
+    sc = tb.scenes.sphere3d(scale=scale)
+    mesh, prm, host = sc.mesh, sc.params, sc.particles
+    n, nsteps = host.n, sc.nsteps
+    part = tb.Partition(mesh, n, backend="torch", device="cuda")
+    G32 = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    P = host.to("torch", device="cuda", dtype=np.float32)
+    runtime.step(G32, P, part, mesh, prm, 3, ctx=ctx)  # warm-up
+    P = host.to("torch", device="cuda", dtype=np.float32)
+    fwd_ms = timed(lambda: runtime.step(G32, P, part, mesh, prm, nsteps, ctx=ctx))
+    P = host.to("torch", device="cuda", dtype=np.float32)
+    tape_ms = timed(lambda: runtime.tape_forward(G32, P, part, mesh, prm, nsteps, every, ctx=ctx))
+    c = torch.tensor(sc.meta["target"], dtype=torch.float64, device="cuda")[:, None]
+    r = P.x.double().mean(dim=1, keepdim=True) - c
+    loss = float((r ** 2).sum())
+    adj = tb.Adjoint(n, 3, backend="torch", device="cuda")
+    adj.x.copy_((2 * r / n).expand(-1, n))
+    bwd_ms = timed(lambda: runtime.tape_backward(G32, P, part, mesh, prm, adj, ctx=ctx))
+    glogE = adj.mu * P.mu.double() + adj.lam * P.lam.double()
+    gnorm_v, gnorm_logE = float(adj.v.norm()), float(glogE.norm())
+    # per-kernel split of one backward segment
+    ctx.profile(True)
+    runtime.tape_forward(G32, P, part, mesh, prm, every, every, ctx=ctx)
+    ctx.profile_read()
+    runtime.tape_backward(G32, P, part, mesh, prm, adj, ctx=ctx)
+    kt = ctx.profile_read()
+    ctx.profile(False)
+
+    # finite-difference check: L = sum c . x_T with random c
+    rng = np.random.default_rng(17)
+    cw = rng.normal(size=(3, n))
+    P = host.to("torch", device="cuda", dtype=np.float32)
+    runtime.tape_forward(G32, P, part, mesh, prm, nsteps, every, ctx=ctx)
+    adj_c = tb.Adjoint(n, 3, backend="torch", device="cuda")
+    adj_c.x.copy_(torch.from_numpy(cw))
+    runtime.tape_backward(G32, P, part, mesh, prm, adj_c, ctx=ctx)
+    g = adj_c.numpy()
+    G64 = tb.generate_grid(mesh, np.float64, backend="torch", device="cuda")
+
+    def loss64(Q):
+        Qd = Q.to("torch", device="cuda")
+        runtime.step(G64, Qd, part, mesh, prm, nsteps, ctx=ctx)
+        ctx.synchronize()
+        return float(np.sum(cw * Qd.x.cpu().numpy()))
+
+    checks = []
+    for k in range(fd_directions):
+        for field, eps in (("v", 1e-5), ("logE", 1e-4)):
+            d = rng.normal(size=(3, n) if field == "v" else (n,))
+            Qp, Qm = host.to("numpy"), host.to("numpy")
+            if field == "v":
+                Qp.v += eps * d
+                Qm.v -= eps * d
+                ad = float(np.sum(g["v"] * d))
+            else:
+                Qp.mu *= np.exp(eps * d)
+                Qp.lam *= np.exp(eps * d)
+                Qm.mu *= np.exp(-eps * d)
+                Qm.lam *= np.exp(-eps * d)
+                ad = float(np.sum((g["mu"] * host.mu + g["lam"] * host.lam) * d))
+            fd = (loss64(Qp) - loss64(Qm)) / (2 * eps)
+            checks.append({"field": field, "adjoint": ad, "fd": fd, "rel_err": abs(ad - fd) / max(abs(fd), 1e-30)})
+    del G64, P
+    torch.cuda.empty_cache()
+    return {
+        "value": (tape_ms + bwd_ms) / fwd_ms,
+        "backward_over_forward": bwd_ms / fwd_ms,
+        "workload": f"sphere3d: 64^3 cells, sphere r=0.3, {n} particles, {nsteps} steps, checkpoint every "
+                    f"{every}, mixed FP32 form; loss = |x_com - (0.5, 0.5, 0.8)|^2",
+        "n_particles": n, "steps": nsteps, "checkpoint_every": every, "loss": loss,
+        "forward_ms_per_step": fwd_ms / nsteps, "tape_forward_ms_per_step": tape_ms / nsteps,
+        "backward_ms_per_step": bwd_ms / nsteps,
+        "grad_v0_norm": gnorm_v, "grad_logE_norm": gnorm_logE,
+        "backward_kernels_ms_per_step": {k: v[1] / every for k, v in sorted(kt.items())},
+        "fd_check": {"against": "central differences of the FP64 device rollout, L = sum c . x_T, random c",
+                     "max_rel_err": max(ch["rel_err"] for ch in checks), "directions": checks},
+    }
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -241,6 +336,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scale", type=int, default=1, help="shrink the cube scene (cells per axis / scale)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rollout leg")
+    ap.add_argument("--adj-scale", type=int, default=1, help="shrink the sphere scene of the adjoint leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed FP32 leg (for profiler captures); prints a reduced line")
     args = ap.parse_args()
@@ -369,6 +466,8 @@ def main():
            "note": "one bench step = one tb_rollout_host_f32 call on pinned host buffers (H2D, S steps, D2H)"}
     del hostp
 
+    adjoint = None if args.no_adjoint else adjoint_leg(tb, runtime, ctx, scale=args.adj_scale)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -427,7 +526,7 @@ def main():
                    "l2": "inputs larger than L2 (2.7 GB particle state per replica)"},
         "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
         "accuracy": acc,
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": adjoint,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_active_node": per_n,

@@ -262,11 +262,13 @@ int32_t tb_adjoint_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* part
  * takes in `adj` the sensitivities to the final state and returns the
  * sensitivities to the state at step 0 (mu and lambda accumulate over all
  * steps); for each segment of K steps it restores the checkpoint, re-runs the
- * segment storing every step's state, and steps backwards through it, so the
- * device memory held is (nsteps/K + K) particle states. `particles` is the
- * working state and holds the step-0 state again on return. The backward pass
- * must follow the forward pass on the same context with the same particle
- * count, mesh and params. Asynchronous. */
+ * segment keeping every step's input state, grid and partition, and steps
+ * backwards through it, so the device memory held is nsteps/K particle states
+ * plus K (state + grid + partition) slots. `particles` is the working state
+ * and holds the step-0 state again on return; the backward pass uses its own
+ * grids and partitions (`partition` and `grid` are not touched). It must
+ * follow the forward pass on the same context with the same particle count,
+ * mesh and params. Asynchronous. */
 int32_t tb_tape_forward_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                             tb_grid* grid, const tb_step_params* params, int32_t nsteps, int32_t checkpoint_every);
 int32_t tb_tape_forward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,

@@ -626,13 +626,17 @@ int grad_grid(tb_ctx* c, int dim, long long nn, GradGrid& GB) {
     return TB_OK;
 }
 
-// Recompute the step's partition and forward grid from `p`, then run the three
-// backward kernels.
+// The three backward kernels for one step. With `recompute` the step's
+// partition and forward grid are first rebuilt from `p` into `part` and `g`;
+// otherwise `part`, `g` and `totals` (device nactive, nassigned) already hold them.
 template <int D, class T, int BW>
 int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                 const tb_step_params* prm, const tb_adjoint* adj) {
-    int rc = run_step<D, T, BW>(c, m, p, part, g, prm, 1, true, true, true, false);
-    if (rc != TB_OK) return rc;
+                 const tb_step_params* prm, const tb_adjoint* adj, bool recompute, const int* totals) {
+    int rc;
+    if (recompute) {
+        if ((rc = run_step<D, T, BW>(c, m, p, part, g, prm, 1, true, true, true, false)) != TB_OK) return rc;
+        totals = c->d_totals;
+    }
     const auto M = make_dmesh<D, T>(*m);
     const auto S = make_scalars<T>(*prm);
     PView<T> P;
@@ -643,16 +647,20 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
     if ((rc = make_adjview(c, adj, D, P.n, A)) != TB_OK) return rc;
     if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
-    const cudaError_t e = launch_adjoint<D, T>(M, G, P, S, A, GB, cfg_of(c));
+    if (!part || !part->blocklist || !part->offsets || (P.n && (!part->particleindices || !part->blockids)))
+        return fail(c, TB_ERR_ARG, "partition array is NULL");
+    const AdjPartition AP{totals, part->blocklist, part->offsets, part->particleindices, part->blockids};
+    const cudaError_t e = launch_adjoint<D, T, BW>(M, G, P, S, A, GB, AP, cfg_of(c));
     return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "adjoint launch");
 }
 
 template <class T>
 int adjoint_dispatch(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                     const tb_step_params* prm, const tb_adjoint* adj) {
-    if (m->dim == 3) return adjoint_impl<3, T, 4>(c, m, p, part, g, prm, adj);
-    if (m->block_log2 == 3) return adjoint_impl<2, T, 8>(c, m, p, part, g, prm, adj);
-    return adjoint_impl<2, T, 4>(c, m, p, part, g, prm, adj);
+                     const tb_step_params* prm, const tb_adjoint* adj, bool recompute = true,
+                     const int* totals = nullptr) {
+    if (m->dim == 3) return adjoint_impl<3, T, 4>(c, m, p, part, g, prm, adj, recompute, totals);
+    if (m->block_log2 == 3) return adjoint_impl<2, T, 8>(c, m, p, part, g, prm, adj, recompute, totals);
+    return adjoint_impl<2, T, 4>(c, m, p, part, g, prm, adj, recompute, totals);
 }
 
 template <class T>
@@ -694,6 +702,42 @@ template <class T>
 size_t state_bytes(int D, long long n) {
     const int nf = 2 * D + (D == 3 ? 6 : 3) + 1;
     return size_t(nf) * align256(sizeof(T) * size_t(n)) + size_t(D * D) * align256(sizeof(double) * size_t(n));
+}
+
+// One step of a tape segment: the state before the step, the step's forward
+// grid and partition, and its device totals.
+template <class T>
+size_t slot_bytes(int D, long long n, long long nn, long long nb) {
+    return state_bytes<T>(D, n) + size_t(1 + 4 * D) * align256(sizeof(T) * size_t(nn)) +
+           2 * align256(sizeof(int) * size_t(n)) + 2 * align256(sizeof(int) * size_t(nb)) +
+           align256(sizeof(int) * size_t(nb + 1)) + 256;
+}
+
+template <class T>
+void slot_views(char* base, int D, long long n, long long nn, long long nb, tb_grid& g, tb_partition& part,
+                int*& totals) {
+    char* q = base + state_bytes<T>(D, n);
+    auto take = [&](size_t bytes) {
+        char* r = q;
+        q += align256(bytes);
+        return r;
+    };
+    g = tb_grid{};
+    g.m = take(sizeof(T) * size_t(nn));
+    for (int d = 0; d < D; ++d) {
+        g.mv[d] = take(sizeof(T) * size_t(nn));
+        g.f[d] = take(sizeof(T) * size_t(nn));
+        g.v[d] = take(sizeof(T) * size_t(nn));
+        g.vn[d] = take(sizeof(T) * size_t(nn));
+    }
+    part = tb_partition{};
+    part.blockids = reinterpret_cast<int32_t*>(take(sizeof(int) * size_t(n)));
+    part.particleindices = reinterpret_cast<int32_t*>(take(sizeof(int) * size_t(n)));
+    part.counts = reinterpret_cast<int32_t*>(take(sizeof(int) * size_t(nb)));
+    part.blocklist = reinterpret_cast<int32_t*>(take(sizeof(int) * size_t(nb)));
+    part.offsets = reinterpret_cast<int32_t*>(take(sizeof(int) * size_t(nb + 1)));
+    part.nblocks = nb;
+    totals = reinterpret_cast<int*>(take(2 * sizeof(int)));
 }
 
 // Particles whose state fields point into the snapshot at `base`.
@@ -764,24 +808,41 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
     const int D = m->dim;
     if (!c->tape_valid || c->tape_n != p->n || c->tape_dim != D || c->tape_elem != int(sizeof(T)))
         return fail(c, TB_ERR_ARG, "no forward tape for these particles on this context (run tb_tape_forward first)");
+    (void)part;
+    (void)g;
     const int K = c->tape_every, nsteps = c->tape_nsteps;
-    const size_t sb = state_bytes<T>(D, p->n);
-    cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * sb));
+    long long nn = 1;
+    for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
+    const long long nb = mesh_nblocks(m);
+    const size_t sb = state_bytes<T>(D, p->n), slot = slot_bytes<T>(D, p->n, nn, nb);
+    cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * slot));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape segment");
     const long long ncp = nsteps > 0 ? (nsteps + K - 1) / K : 1;
     for (long long k = ncp - 1; k >= 0 && nsteps > 0; --k) {
         const int len = int(std::min<long long>(K, nsteps - k * K));
         tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb);
         if ((rc = copy_state<T>(c, p, &cp, D)) != TB_OK) return rc;
+        // re-run the segment, keeping each step's input state, grid and partition
         for (int j = 0; j < len; ++j) {
-            tb_particles sj = snapshot_view<T>(p, D, c->tape_seg + j * sb);
+            char* base = c->tape_seg + j * slot;
+            tb_particles sj = snapshot_view<T>(p, D, base);
+            tb_grid gj;
+            tb_partition pj;
+            int* tj;
+            slot_views<T>(base, D, p->n, nn, nb, gj, pj, tj);
             if ((rc = copy_state<T>(c, &sj, p, D)) != TB_OK) return rc;
-            if (j + 1 < len && (rc = dispatch_step<T>(c, m, p, part, g, prm, 1, true, true, true, true)) != TB_OK)
-                return rc;
+            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, j + 1 < len)) != TB_OK) return rc;
+            e = cudaMemcpyAsync(tj, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
+            if (e != cudaSuccess) return cuda_fail(c, e, "tape totals copy");
         }
         for (int j = len - 1; j >= 0; --j) {
-            tb_particles sj = snapshot_view<T>(p, D, c->tape_seg + j * sb);
-            if ((rc = adjoint_dispatch<T>(c, m, &sj, part, g, prm, adj)) != TB_OK) return rc;
+            char* base = c->tape_seg + j * slot;
+            tb_particles sj = snapshot_view<T>(p, D, base);
+            tb_grid gj;
+            tb_partition pj;
+            int* tj;
+            slot_views<T>(base, D, p->n, nn, nb, gj, pj, tj);
+            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj)) != TB_OK) return rc;
         }
     }
     tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp);

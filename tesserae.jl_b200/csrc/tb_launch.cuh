@@ -109,11 +109,21 @@ struct GradGrid {
     double* fb[3];   // d loss / d f_i
 };
 
+// The partition of the step being reversed (device arrays).
+struct AdjPartition {
+    const int* totals;     // [2] nactive, nassigned
+    const int* blocklist;
+    const int* offsets;
+    const int* perm;
+    const int* blockids;
+};
+
 // G2P, grid update and P2G backwards for one step whose forward grid is in G
-// (tb_adjoint.cu). Zeroes GB's v / vn sensitivities first.
-template <int D, class T>
+// and whose partition is `part` (tb_adjoint.cu). Zeroes GB's v / vn
+// sensitivities first.
+template <int D, class T, int BW>
 cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
-                           const AdjView& A, const GradGrid& GB, const LaunchCfg& cfg);
+                           const AdjView& A, const GradGrid& GB, const AdjPartition& part, const LaunchCfg& cfg);
 
 template <int D, class T>
 cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* grad_w,
