@@ -205,10 +205,12 @@ __device__ __forceinline__ void bspline_quadratic_axis(T xi, T* v0, T* v1) {
 // Window and 1-D jets of one particle for B-spline / uGIMP kernels (the
 // kernel part of WLS too). Returns false when the particle is outside the mesh
 // (empty window, cartesian.jl:190-199). `full` reports a 3^D window.
+// Support window of one particle: xi = (x - xmin) h_inv per axis, the clamped
+// window start and node count per axis (supportnodes, bspline.jl:28-40 and
+// cartesian.jl:190-199). Returns false when the particle is outside the mesh.
 template <int D, class T>
-__device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, const T* x, T lnorm, Axis<T>* ax,
-                                             bool& full) {
-    T xi[3];
+__device__ __forceinline__ bool axis_window(const DMesh<D, T>& M, int basis, const T* x, T lnorm, T* xi, int* lo,
+                                            int* cnt) {
     bool inside = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -218,7 +220,6 @@ __device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, co
     }
     if (!inside) return false;
     const bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
-    full = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         int s, e;
@@ -230,9 +231,24 @@ __device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, co
             s = int(floor(xi[d] - T(0.5)));
             e = s + 2;
         }
-        int lo = max(s, 0), hi = min(e, M.n[d] - 1);
-        ax[d].lo = lo;
-        ax[d].cnt = hi - lo + 1;
+        lo[d] = max(s, 0);
+        cnt[d] = min(e, M.n[d] - 1) - lo[d] + 1;
+    }
+    return true;
+}
+
+template <int D, class T>
+__device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, const T* x, T lnorm, Axis<T>* ax,
+                                             bool& full) {
+    T xi[3];
+    int lo[3], cnt[3];
+    if (!axis_window<D, T>(M, basis, x, lnorm, xi, lo, cnt)) return false;
+    const bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    full = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        ax[d].lo = lo[d];
+        ax[d].cnt = cnt[d];
         full = full && (ax[d].cnt == 3);
     }
     if (basis == TB_BSPLINE_QUADRATIC && full) {

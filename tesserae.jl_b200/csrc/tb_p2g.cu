@@ -437,6 +437,383 @@ __global__ void __launch_bounds__(P2G_THREADS, (sizeof(T) == 4 && !GEN) ? 2 : 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Plain kernel (B-spline or uGIMP, FLIP/PIC blend): the same pencil sweep
+// without shared-memory atomics.
+//   1a. window start only (no basis values) -> group and rank in the group;
+//   1b. basis jets once per particle, record written at its group-sorted slot;
+//   2.  a lane walks its pencil's groups in x order, two records in flight at a
+//       time; after each group the x-node the window leaves for good is final
+//       for this (pencil, row) and is stored, with plain stores, to the lane's
+//       own slot of a staging array (the group loop is unrolled, so the shift of
+//       the 3-node row is a register rename);
+//   3.  one thread per tile node sums the at most 3^(D-1) staged partials that
+//       reach it (pencils gy = ty - sj, gz = tz - sk) in FP64 and adds the node
+//       to the grid with one global atomic per non-zero value.
+// On B200 an FP64 shared-memory atomic add is a compare-and-swap loop; in the
+// tiled form of this sweep those atomics retried 2.5 times each and, with the
+// record loads, kept the shared-memory pipe at 69% of its wavefront rate. The
+// staged form issues no shared atomic. Partials are the FP32 sums of one
+// pencil row (at most 3 groups); the sum over pencils is FP64.
+//
+// Record (T words): [0] m_p [1..3] m_p v_p [4..9] S = -V_p sigma_p (Tensorial
+// symmetric order; 3 used in 2D) [10..15] x jets (value, h_inv-scaled
+// derivative per slot) [16..21] y jets [22..27] z jets. 28 words = 7 x 16 bytes,
+// so 8 consecutive records stored as 16-byte vectors hit 8 distinct bank groups.
+constexpr int PRS = 28;
+
+__device__ __forceinline__ void st2(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+template <class T>
+struct PlainRec {
+    V4<T> m4, s4, xb;
+    V2<T> s2, xa, y2, z2;
+};
+
+template <int D, class T>
+__device__ __forceinline__ void load_plain(const T* r, int sj, int sk, PlainRec<T>& o) {
+    o.m4 = ld4(r + 0);
+    o.s4 = ld4(r + 4);
+    if constexpr (D == 3) o.s2 = ld2(r + 8);
+    o.xa = ld2(r + 10);
+    o.xb = ld4(r + 12);
+    o.y2 = ld2(r + 16 + 2 * sj);
+    if constexpr (D == 3) o.z2 = ld2(r + 22 + 2 * sk);
+}
+
+template <int D, class T>
+__device__ __forceinline__ void accumulate_plain(const PlainRec<T>& o, T (&acc)[3][1 + 2 * D]) {
+    const T mp = o.m4.a;
+    const T mv[3] = {o.m4.b, o.m4.c, o.m4.d};
+    T S[6] = {o.s4.a, o.s4.b, o.s4.c, o.s4.d, T(0), T(0)};
+    if constexpr (D == 3) {
+        S[4] = o.s2.a;
+        S[5] = o.s2.b;
+    }
+    const T wx[3] = {o.xa.a, o.xb.a, o.xb.c}, dx[3] = {o.xa.b, o.xb.b, o.xb.d};
+    T wyz, dyz, wdz = T(0);
+    if constexpr (D == 3) {
+        wyz = o.y2.a * o.z2.a;
+        dyz = o.y2.b * o.z2.a;
+        wdz = o.y2.a * o.z2.b;
+    } else {
+        wyz = o.y2.a;
+        dyz = o.y2.b;
+    }
+    // f_a = S[a,0] dx wyz + S[a,1] wx dyz + S[a,2] wx wdz
+    T fa[3], fb[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        fa[a] = S[symidx<D>(a, 0)] * wyz;
+        fb[a] = S[symidx<D>(a, 1)] * dyz;
+        if constexpr (D == 3) fb[a] += S[symidx<D>(a, 2)] * wdz;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T w = wx[i] * wyz;
+        acc[i][0] += w * mp;
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[i][1 + d] += w * mv[d];
+#pragma unroll
+        for (int a = 0; a < D; ++a) acc[i][1 + D + a] += dx[i] * fa[a] + wx[i] * fb[a];
+    }
+}
+
+template <int NC, class T>
+__device__ __forceinline__ void stage_node(T* part, int base, int stride, const T (&a)[NC]) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) part[base + c * stride] = a[c];
+}
+
+// Staging layout: partial (component c, pencil pc, row jk, tile x) at
+// ((c * NPENCIL + pc) * NJK + jk) * TS + x.
+template <int D, int BW>
+struct PencilShape {
+    static constexpr int TS = BW + 3;
+    static constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
+    static constexpr int NC = 1 + 2 * D;
+    static constexpr int G1 = BW + 1;
+    static constexpr int NG = (D == 3) ? G1 * G1 * G1 : G1 * G1;
+    static constexpr int NJK = (D == 3) ? 9 : 3;
+    static constexpr int NSUB = 32 / NJK;
+    static constexpr int NPENCIL = NG / G1;
+    static constexpr int NPART = NC * NPENCIL * NJK * TS;
+};
+
+template <int D, class T, int BW, int NR>
+__global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_pencil_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
+                                                                    const int* __restrict__ totals,
+                                                                    const int* __restrict__ blocklist,
+                                                                    const int* __restrict__ offsets,
+                                                                    const int* __restrict__ perm, int* err) {
+    using SH = PencilShape<D, BW>;
+    constexpr int NT = P2G_THREADS;
+    constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
+    constexpr int NW = NT / 32;
+    constexpr int NJK = SH::NJK, NSUB = SH::NSUB, NPENCIL = SH::NPENCIL;
+    constexpr int NTASK = (NPENCIL + NSUB - 1) / NSUB;
+    constexpr int ITEMS = (NR + NT - 1) / NT;
+    constexpr int CSTR = NPENCIL * NJK * TS;  // stride between components in the staging array
+    static_assert(NPENCIL <= 32, "pencil ranking runs in one warp");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* rec = reinterpret_cast<T*>(smem_raw);
+    T* part = rec + NR * PRS;
+    int* gcount = reinterpret_cast<int*>(part + SH::NPART);
+    int* gstart = gcount + NG;
+    int* pslot = gstart + NG + 1;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nactive = totals[0];
+    const int jk = lane % NJK, sub = lane / NJK;
+    const int sj = jk % 3, sk = (D == 3) ? jk / 3 : 0;
+    const bool gimp = s.basis == TB_UGIMP;
+
+    for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+    __syncthreads();
+
+    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        const int b = blocklist[bi] - 1;
+        int org[3] = {0, 0, 0};
+        {
+            int r = b;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                org[d] = (r % M.nb[d]) * BW - 1;
+                r /= M.nb[d];
+            }
+        }
+        const int s0 = offsets[b], s1 = offsets[b + 1];
+        for (int b0 = s0; b0 < s1; b0 += NR) {
+            const int nbat = min(NR, s1 - b0);
+            // ---- 1a. window start -> group, rank within the group
+            int grp[ITEMS], rank[ITEMS];
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                const int ti = tid + u * NT;
+                grp[u] = -1;
+                rank[u] = 0;
+                if (ti >= nbat) continue;
+                const long long p = perm[b0 + ti] - 1;
+                T x[3], xi[3];
+                int lo[3], cnt[3];
+#pragma unroll
+                for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+                T lnorm = T(0);
+                if (gimp) {
+                    lnorm = (P.l ? P.l[p] : s.gimp_l) / M.h;
+                    if (!(lnorm >= T(0) && lnorm <= T(1))) {
+                        atomicOr(err, ERR_GIMP_LENGTH);
+                        continue;
+                    }
+                }
+                if (!axis_window<D, T>(M, s.basis, x, lnorm, xi, lo, cnt)) continue;
+                int gi = 0;
+                bool ok = true;
+#pragma unroll
+                for (int d = D - 1; d >= 0; --d) {
+                    const int q = lo[d] - org[d];
+                    ok = ok && q >= 0 && q < G1;
+                    gi = gi * G1 + q;
+                }
+                if (!ok) {
+                    atomicOr(err, ERR_TILE_RANGE);
+                    continue;
+                }
+                grp[u] = gi;
+                rank[u] = atomicAdd(&gcount[gi], 1);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                int carry = 0;
+                for (int g0 = 0; g0 < NG; g0 += 32) {
+                    const int g = g0 + lane;
+                    const int c = g < NG ? gcount[g] : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    if (g < NG) gstart[g] = carry + incl - c;
+                    carry += __shfl_sync(0xffffffffu, incl, 31);
+                }
+                if (lane == 0) gstart[NG] = carry;
+            } else if (warp == 1) {
+                // pencil slots by size, largest first: the NSUB pencils a warp
+                // sweeps in lockstep then have similar lengths
+                const int myp = lane < NPENCIL ? lane : -1;
+                int mysize = 0;
+                if (myp >= 0) {
+                    const int gb = G1 * myp;
+                    for (int gx = 0; gx < G1; ++gx) mysize += gcount[gb + gx];
+                }
+                int rk = 0;
+                for (int o = 0; o < NPENCIL; ++o) {
+                    const int os = __shfl_sync(0xffffffffu, mysize, o);
+                    rk += (os > mysize) || (os == mysize && o < lane);
+                }
+                if (myp >= 0) pslot[rk] = myp;
+            }
+            __syncthreads();
+            // ---- 1b. basis jets and record at the group-sorted slot
+            for (int g = tid; g < NG; g += NT) gcount[g] = 0;  // ready for the next batch
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                if (grp[u] < 0) continue;
+                const int ti = tid + u * NT;
+                const long long p = perm[b0 + ti] - 1;
+                T x[3];
+#pragma unroll
+                for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+                const T l = P.l ? P.l[p] : s.gimp_l;
+                Basis<D, T> B;
+                prepare_basis<D, T, false>(M, s.basis, x, l, B, err);
+                T* r = rec + (gstart[grp[u]] + rank[u]) * PRS;
+                const T mp = P.m ? P.m[p] : s.mass;
+                const T nV = -P.V[p];
+                T v[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                for (int d = 0; d < D; ++d) v[d] = P.v[d][p];
+                T Sv[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) Sv[k] = (k < nsym<D>()) ? nV * P.sig[k < nsym<D>() ? k : 0][p] : T(0);
+                T jv[3][3], jd[3][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        jv[d][k] = d < D ? B.ax[d < D ? d : 0].val[k] : T(0);
+                        jd[d][k] = d < D ? B.ax[d < D ? d : 0].der[k] * M.h_inv : T(0);
+                    }
+                st4(r + 0, mp, mp * v[0], mp * v[1], mp * v[2]);
+                st4(r + 4, Sv[0], Sv[1], Sv[2], Sv[3]);
+                st2(r + 8, Sv[4], Sv[5]);
+                st2(r + 10, jv[0][0], jd[0][0]);
+                st4(r + 12, jv[0][1], jd[0][1], jv[0][2], jd[0][2]);
+                st4(r + 16, jv[1][0], jd[1][0], jv[1][1], jd[1][1]);
+                st2(r + 20, jv[1][2], jd[1][2]);
+                st2(r + 22, jv[2][0], jd[2][0]);
+                st4(r + 24, jv[2][1], jd[2][1], jv[2][2], jd[2][2]);
+            }
+            __syncthreads();
+            // ---- 2. pencil sweeps; every live (pencil, row) stages all TS x-nodes
+            for (int task = warp; task < NTASK; task += NW) {
+                const int slot = task * NSUB + sub;
+                if (sub >= NSUB || slot >= NPENCIL) continue;
+                const int pc = pslot[slot];
+                const int gbase = G1 * pc;
+                const int pbase = (pc * NJK + jk) * TS;
+                T acc[3][NC];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) acc[i][c] = T(0);
+                // The groups of the pencil in x order; two records of a group are
+                // loaded before either is accumulated. After group gx the x-node
+                // gx is final (later groups start further right).
+                int qs = gstart[gbase];
+#pragma unroll
+                for (int gx = 0; gx < G1 + 2; ++gx) {
+                    if (gx < G1) {
+                        const int qe = gstart[gbase + gx + 1];
+                        int q = qs;
+                        for (; q + 1 < qe; q += 2) {
+                            PlainRec<T> r0, r1;
+                            load_plain<D, T>(rec + q * PRS, sj, sk, r0);
+                            load_plain<D, T>(rec + (q + 1) * PRS, sj, sk, r1);
+                            accumulate_plain<D, T>(r0, acc);
+                            accumulate_plain<D, T>(r1, acc);
+                        }
+                        if (q < qe) {
+                            PlainRec<T> r0;
+                            load_plain<D, T>(rec + q * PRS, sj, sk, r0);
+                            accumulate_plain<D, T>(r0, acc);
+                        }
+                        qs = qe;
+                    }
+                    stage_node<NC, T>(part, pbase + gx, CSTR, acc[0]);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        acc[0][c] = acc[1][c];
+                        acc[1][c] = acc[2][c];
+                        acc[2][c] = T(0);
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- 3. per tile node: sum the staged partials (FP64), add to the grid
+            for (int t = tid; t < TN; t += NT) {
+                int node[3], tn[3] = {0, 0, 0}, rem = t;
+                bool inside = true;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    tn[d] = rem % TS;
+                    rem /= TS;
+                    node[d] = org[d] + tn[d];
+                    inside = inside && node[d] >= 0 && node[d] < M.n[d];
+                }
+                if (!inside) continue;
+                double val[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) val[c] = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < (D == 3 ? 3 : 1); ++kk)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const int gy = tn[1] - jj, gz = (D == 3) ? tn[2] - kk : 0;
+                        if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
+                        const int pc = gy + G1 * gz;
+                        const int idx = (pc * NJK + jj + 3 * kk) * TS + tn[0];
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) val[c] += double(part[idx + c * CSTR]);
+                    }
+                long long lin = 0;
+#pragma unroll
+                for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + node[d];
+#pragma unroll
+                for (int d = 0; d < D; ++d) val[1 + D + d] += double(s.g[d]) * val[0];
+                if (val[0] != 0.0) atomicAdd(G.m + lin, T(val[0]));
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    if (val[1 + d] != 0.0) atomicAdd(G.mv[d] + lin, T(val[1 + d]));
+                    if (val[1 + D + d] != 0.0) atomicAdd(G.f[d] + lin, T(val[1 + D + d]));
+                }
+            }
+        }
+    }
+}
+
+template <int D, class T, int BW, int NR>
+size_t pencil_smem_bytes() {
+    using SH = PencilShape<D, BW>;
+    return sizeof(T) * (size_t(NR) * PRS + SH::NPART) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
+}
+
+template <int D, class T, int BW>
+cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                          const BinBuffers& b, const LaunchCfg& cfg) {
+    // Records per batch: a whole cube3d block (512). FP32: 2 CTAs per SM
+    // (78 KB of shared memory, 110 registers); FP64: 1 CTA per SM.
+    constexpr int NR = 512;
+    auto kern = p2g_pencil_kernel<D, T, BW, NR>;
+    const size_t smem = pencil_smem_bytes<D, T, BW, NR>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2G_THREADS, smem);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    KernelScope ks(cfg, "p2g");
+    kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
 template <int D, class T, int BW, bool GEN, int NR>
 size_t p2g_smem_bytes() {
     constexpr int TS = BW + 3;
@@ -475,7 +852,7 @@ cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& 
                        const BinBuffers& b, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
-    return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_group<D, T, BW, false>(M, P, G, s, b, cfg);
+    return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_pencil<D, T, BW>(M, P, G, s, b, cfg);
 }
 
 #define TB_INST_P2G(D, T, BW)                                                                        \
