@@ -589,28 +589,49 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
         const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int b0 = s0; b0 < s1; b0 += NR) {
             const int nbat = min(NR, s1 - b0);
-            // ---- 1a. window start -> group, rank within the group
+            // ---- 1a. every global load of the batch first (the ids, then all of
+            //      the particles' fields at once: two dependent round trips per
+            //      batch), then window start -> group, rank within the group. The
+            //      fields stay in registers for 1b.
             int grp[ITEMS], rank[ITEMS];
+            long long pid[ITEMS];
+            T px[ITEMS][3], pv[ITEMS][3], pV[ITEMS], pm[ITEMS], pl[ITEMS], psg[ITEMS][6];
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
                 const int ti = tid + u * NT;
+                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                const long long p = pid[u] >= 0 ? pid[u] : 0;
+                const bool on = pid[u] >= 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    px[u][d] = (on && d < D) ? P.x[d < D ? d : 0][p] : T(0);
+                    pv[u][d] = (on && d < D) ? P.v[d < D ? d : 0][p] : T(0);
+                }
+                pV[u] = on ? P.V[p] : T(0);
+                pm[u] = (on && P.m) ? P.m[p] : s.mass;
+                pl[u] = (on && P.l) ? P.l[p] : s.gimp_l;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) psg[u][k] = (on && k < nsym<D>()) ? P.sig[k < nsym<D>() ? k : 0][p] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
                 grp[u] = -1;
                 rank[u] = 0;
-                if (ti >= nbat) continue;
-                const long long p = perm[b0 + ti] - 1;
-                T x[3], xi[3];
+                if (pid[u] < 0) continue;
+                T xi[3];
                 int lo[3], cnt[3];
-#pragma unroll
-                for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
                 T lnorm = T(0);
                 if (gimp) {
-                    lnorm = (P.l ? P.l[p] : s.gimp_l) / M.h;
+                    lnorm = pl[u] / M.h;
                     if (!(lnorm >= T(0) && lnorm <= T(1))) {
                         atomicOr(err, ERR_GIMP_LENGTH);
                         continue;
                     }
                 }
-                if (!axis_window<D, T>(M, s.basis, x, lnorm, xi, lo, cnt)) continue;
+                if (!axis_window<D, T>(M, s.basis, px[u], lnorm, xi, lo, cnt)) continue;
                 int gi = 0;
                 bool ok = true;
 #pragma unroll
@@ -664,23 +685,15 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
                 if (grp[u] < 0) continue;
-                const int ti = tid + u * NT;
-                const long long p = perm[b0 + ti] - 1;
-                T x[3];
-#pragma unroll
-                for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
-                const T l = P.l ? P.l[p] : s.gimp_l;
                 Basis<D, T> B;
-                prepare_basis<D, T, false>(M, s.basis, x, l, B, err);
+                prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err);
                 T* r = rec + (gstart[grp[u]] + rank[u]) * PRS;
-                const T mp = P.m ? P.m[p] : s.mass;
-                const T nV = -P.V[p];
-                T v[3] = {T(0), T(0), T(0)};
-#pragma unroll
-                for (int d = 0; d < D; ++d) v[d] = P.v[d][p];
+                const T mp = pm[u];
+                const T nV = -pV[u];
+                const T* v = pv[u];
                 T Sv[6];
 #pragma unroll
-                for (int k = 0; k < 6; ++k) Sv[k] = (k < nsym<D>()) ? nV * P.sig[k < nsym<D>() ? k : 0][p] : T(0);
+                for (int k = 0; k < 6; ++k) Sv[k] = nV * psg[u][k];
                 T jv[3][3], jd[3][3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)

@@ -175,7 +175,7 @@ __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& 
 }
 
 template <int D, class T, int BW, bool GEN>
-__global__ void __launch_bounds__(128) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
+__global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 8 : 4)) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
                                                        const int* __restrict__ totals,
                                                        const int* __restrict__ blocklist,
                                                        const int* __restrict__ offsets,
@@ -398,7 +398,9 @@ __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T>
 // Particles outside the mesh (block id 0): empty window, so only the particle
 // equations run (v and x keep their values under FLIP).
 template <int D, class T>
-__global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T> s, const int* __restrict__ blockids) {
+__global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T> s, const int* __restrict__ blockids,
+                                                          const int* __restrict__ totals) {
+    if ((long long)totals[1] >= P.n) return;  // every particle is inside a block
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
         if (blockids[p] != 0) continue;
         T x[3], vp[3], z[3] = {T(0), T(0), T(0)};
@@ -493,7 +495,7 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
     }
     KernelScope ks(cfg, "g2p_outside");
     const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
-    g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids);
+    g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
     *cfg.launches += 2;
     return cudaGetLastError();
 }
