@@ -9,10 +9,12 @@
 //            the compacted block list and the totals [nactive, nassigned]
 //   scatter  one thread per particle: a warp reserves one run per distinct
 //            block with a single atomic and writes its particles in lane order
-//   fixup    one CTA per non-empty block: the block's segment is a set of runs,
-//            one per warp (32 consecutive particle ids), each ascending; the
-//            runs are sorted by warp id (bitonic, shared memory, or a global
-//            scratch region for segments above 2048 runs) and copied in order.
+//   fixup    one warp per non-empty block: the block's segment is a set of runs,
+//            one per scatter warp (32 consecutive particle ids), each ascending;
+//            the runs are ranked by warp id and copied in order. Blocks of more
+//            than 64 runs are sorted by a second kernel (one CTA per block,
+//            bitonic in shared memory, or in a global scratch region for
+//            segments above 2048 runs).
 // The result is deterministic regardless of atomic order.
 #include "tb_launch.cuh"
 
@@ -258,6 +260,86 @@ __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __res
     }
 }
 
+// One warp per non-empty block: the block's segment of the scattered ids is a
+// concatenation of runs, one per scatter warp that held particles of the block,
+// each ascending and contiguous, and no two runs of a segment share a warp id.
+// The warp finds the run heads with ballots, ranks the runs by warp id (every
+// run against every run, at most FIXW_RUNS of them) and copies the segment
+// element-parallel, each element to its run's place. A block with more runs is appended to an
+// overflow list that bin_fixup_kernel then sorts.
+constexpr int FIXW_RUNS = 64;
+constexpr int FIXW_THREADS = 256;
+
+__global__ void __launch_bounds__(FIXW_THREADS) bin_fixup_warp_kernel(const int* __restrict__ totals,
+                                                                      const int* __restrict__ blocklist,
+                                                                      const int* __restrict__ offsets,
+                                                                      const int* __restrict__ counts,
+                                                                      const int* __restrict__ S,
+                                                                      int* __restrict__ perm,
+                                                                      int* __restrict__ overflow,
+                                                                      unsigned long long* __restrict__ noverflow) {
+    constexpr int NWARP = FIXW_THREADS / 32;
+    __shared__ int hpos[NWARP][FIXW_RUNS + 1];
+    __shared__ int hkey[NWARP][FIXW_RUNS];
+    __shared__ int hout[NWARP][FIXW_RUNS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nactive = totals[0];
+    const unsigned full = 0xffffffffu;
+    const unsigned below = (1u << lane) - 1u;
+    for (int bi = blockIdx.x * NWARP + w; bi < nactive; bi += gridDim.x * NWARP) {
+        const int b = blocklist[bi] - 1;
+        const int s = offsets[b], n = counts[b];
+        const int* seg = S + s;
+        int* out = perm + s;
+        int nruns = 0;
+        for (int j0 = 0; j0 < n; j0 += 32) {
+            const int j = j0 + lane;
+            const int v = j < n ? seg[j] : 0;
+            int prev = __shfl_up_sync(full, v, 1);
+            if (lane == 0) prev = j0 > 0 ? seg[j0 - 1] : -1;
+            const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
+            const unsigned hm = __ballot_sync(full, head);
+            const int idx = nruns + __popc(hm & below);
+            if (head && idx < FIXW_RUNS) {
+                hpos[w][idx] = j;
+                hkey[w][idx] = v >> 5;
+            }
+            nruns += __popc(hm);
+        }
+        if (nruns > FIXW_RUNS) {
+            if (lane == 0) overflow[atomicAdd(noverflow, 1ull)] = b + 1;
+            __syncwarp();
+            continue;
+        }
+        if (lane == 0) hpos[w][nruns] = n;
+        __syncwarp();
+        // output start of each run: total length of the runs with a smaller warp id
+        for (int r = lane; r < nruns; r += 32) {
+            const int key = hkey[w][r];
+            int start = 0;
+            for (int q = 0; q < nruns; ++q)
+                if (hkey[w][q] < key) start += hpos[w][q + 1] - hpos[w][q];
+            hout[w][r] = start;
+        }
+        __syncwarp();
+        // copy element-parallel: the run of element j is the number of heads at
+        // or before j, minus one
+        int rbase = 0;
+        for (int j0 = 0; j0 < n; j0 += 32) {
+            const int j = j0 + lane;
+            const int v = j < n ? seg[j] : 0;
+            int prev = __shfl_up_sync(full, v, 1);
+            if (lane == 0) prev = j0 > 0 ? seg[j0 - 1] : -1;
+            const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
+            const unsigned hm = __ballot_sync(full, head);
+            const int r = rbase + __popc(hm & (below | (1u << lane))) - 1;
+            if (j < n) out[hout[w][r] + (j - hpos[w][r])] = v + 1;
+            rbase += __popc(hm);
+        }
+        __syncwarp();
+    }
+}
+
 inline unsigned grid_for(long long n, int threads) { return unsigned((n + threads - 1) / threads); }
 
 }  // namespace
@@ -291,11 +373,19 @@ cudaError_t launch_bin_rest(int nb, long long n, const BinBuffers& b, const Laun
             KernelScope ks(cfg, "bin_scatter");
             bin_scatter_kernel<<<grid_for(n, 256), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors, b.perm_tmp);
         }
-        const int grid = std::min(nb, cfg.num_sms * 16);
+        // Blocks of more than FIXW_RUNS runs go to an overflow list kept in the
+        // cursor array (free once the scatter is done), its length in partials[0].
+        cudaError_t e = cudaMemsetAsync(b.partials, 0, sizeof(unsigned long long), cfg.stream);
+        if (e != cudaSuccess) return e;
         KernelScope ks(cfg, "bin_fixup");
-        bin_fixup_kernel<<<grid, FIX_THREADS, 0, cfg.stream>>>(b.totals, b.blocklist, b.offsets, b.counts,
-                                                               b.perm_tmp, b.perm, b.sort_scratch);
-        *cfg.launches += 2;
+        const int wgrid = std::max(1, std::min((nb + FIXW_THREADS / 32 - 1) / (FIXW_THREADS / 32), cfg.num_sms * 8));
+        bin_fixup_warp_kernel<<<wgrid, FIXW_THREADS, 0, cfg.stream>>>(b.totals, b.blocklist, b.offsets, b.counts,
+                                                                      b.perm_tmp, b.perm, b.cursors, b.partials);
+        const int grid = std::min(nb, cfg.num_sms * 16);
+        bin_fixup_kernel<<<grid, FIX_THREADS, 0, cfg.stream>>>(reinterpret_cast<const int*>(b.partials), b.cursors,
+                                                               b.offsets, b.counts, b.perm_tmp, b.perm,
+                                                               b.sort_scratch);
+        *cfg.launches += 3;
     }
     return cudaGetLastError();
 }
