@@ -3,8 +3,11 @@
 Workload: the 3D cube scene (unit cube 256^3 cells, centre cube of side 0.5 at
 2^3 particles per cell = 16 777 216 particles, Neo-Hookean E = 1e6, nu = 0.3,
 gravity), seeded synthetic data. One bench "step" = one MPM step over all
-particles. The headline form is the mixed FP32 step (FP32 state, FP64 F/J/log J,
-FP64-accumulated P2G tiles); the plain FP64 step is measured beside it.
+particles. The headline form is the mixed FP32 step with FP64 positions (FP32
+velocity, stress, volume, weights and transfers; FP64 x, F, det F, log J; P2G
+partials summed in FP64), the form that holds the 100-step error against the
+FP64 run below 1e-5. The same step with FP32 positions and the plain FP64 step
+are measured beside it, with their accuracy.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -164,18 +167,18 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-# Algorithmic bytes per particle and per active node of each kernel family,
-# mixed FP32 form (F FP64) and plain FP64 form: the scatter/gather reads and
-# writes of the reference's equations (weights evaluated in the kernels).
-def algorithmic_bytes(kind: str, dtype) -> tuple[int, int]:
-    s = np.dtype(dtype).itemsize
+# Algorithmic bytes per particle and per active node of each kernel family:
+# the scatter/gather reads and writes of the reference's equations (weights
+# evaluated in the kernels), for a state scalar of `s` bytes and positions of
+# `sx` bytes (FP64 positions in the headline form); F is FP64 in every form.
+def algorithmic_bytes(kind: str, s: int, sx: int) -> tuple[int, int]:
     per_p = {
         # x, v, V, sigma(6) read
-        "p2g": (3 + 3 + 1 + 6) * s,
+        "p2g": 3 * sx + (3 + 1 + 6) * s,
         # x, v, F(9 x 8) read; x, v, grad_v(9), F, sigma(6), V written
-        "g2p": (3 + 3) * s + 72 + (3 + 3 + 9 + 6 + 1) * s + 72,
+        "g2p": 3 * sx + 3 * s + 72 + 3 * sx + (3 + 9 + 6 + 1) * s + 72,
         # x read, block id written
-        "bin_count": 3 * s + 4,
+        "bin_count": 3 * sx + 4,
     }[kind]
     per_n = {
         "p2g": 7 * s,       # m, mv, f written once per active node
@@ -183,6 +186,37 @@ def algorithmic_bytes(kind: str, dtype) -> tuple[int, int]:
         "bin_count": 0,
     }[kind]
     return per_p, per_n
+
+
+def step_bytes(s: int, sx: int) -> tuple[int, int]:
+    """Algorithmic bytes of one whole MPM step per particle and per active node:
+    binning (x read; block id and particle index written), P2G, G2P; per active
+    node the P2G result write, the grid update's read and write and the G2P read."""
+    per_p = (3 * sx + 8) + algorithmic_bytes("p2g", s, sx)[0] + algorithmic_bytes("g2p", s, sx)[0]
+    per_n = 7 * s + 7 * s + 6 * s + 6 * s
+    return per_p, per_n
+
+
+FORMS = {
+    # name: (state dtype, FP64 positions, description)
+    "x64": (np.float32, True, "mixed FP32 with FP64 positions (FP64 x, F, det F, log J; FP64-summed P2G partials)"),
+    "f32": (np.float32, False, "mixed FP32 with FP32 positions (FP64 F, det F, log J; FP64-summed P2G partials)"),
+    "f64": (np.float64, False, "plain FP64"),
+}
+
+
+def read_traffic(kernel: str, n: int):
+    """DRAM bytes (read + write) per launch of `kernel` on the full workload,
+    scaled from the committed ncu capture's per-particle figure
+    (profiles/traffic_cube3d.txt: lines `<kernel> <bytes per particle>`)."""
+    f = ROOT / "profiles" / "traffic_cube3d.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and parts[0] == kernel:
+            return float(parts[1]) * n
+    return None
 
 
 def active_nodes(mesh, particles_np) -> int:
@@ -202,10 +236,11 @@ def active_nodes(mesh, particles_np) -> int:
 
 def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions: int = 2) -> dict:
     """Differentiable rollout on the sphere scene (64^3 cells, ~1.9M particles,
-    200 steps, checkpoint every 20), mixed FP32 form: device time of the plain
-    forward rollout, the taped forward and the backward pass for the
-    centre-of-mass loss, plus directional derivatives of a linear loss on the
-    final positions against central differences of the FP64 device rollout."""
+    200 steps, checkpoint every 20), mixed FP32 form with FP32 positions (the
+    form the tape runs): device time of the plain forward rollout, the taped
+    forward and the backward pass for the centre-of-mass loss, plus directional
+    derivatives of a linear loss on the final positions, from the FP64 tape and
+    from the FP32 tape, against central differences of the FP64 device rollout."""
     import torch
     sc = tb.scenes.sphere3d(scale=scale)
     mesh, prm, host = sc.mesh, sc.params, sc.particles
@@ -244,16 +279,21 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
     kt = ctx.profile_read()
     ctx.profile(False)
 
-    # finite-difference check: L = sum c . x_T with random c
+    # finite-difference check: L = sum c . x_T with random c, gradients from the
+    # FP64 tape (the check of the adjoint itself) and from the FP32 tape timed above
     rng = np.random.default_rng(17)
     cw = rng.normal(size=(3, n))
-    P = host.to("torch", device="cuda", dtype=np.float32)
-    runtime.tape_forward(G32, P, part, mesh, prm, nsteps, every, ctx=ctx)
-    adj_c = tb.Adjoint(n, 3, backend="torch", device="cuda")
-    adj_c.x.copy_(torch.from_numpy(cw))
-    runtime.tape_backward(G32, P, part, mesh, prm, adj_c, ctx=ctx)
-    g = adj_c.numpy()
     G64 = tb.generate_grid(mesh, np.float64, backend="torch", device="cuda")
+
+    def grads(dtype, G):
+        Q = host.to("torch", device="cuda", dtype=dtype)
+        runtime.tape_forward(G, Q, part, mesh, prm, nsteps, every, ctx=ctx)
+        adj_c = tb.Adjoint(n, 3, backend="torch", device="cuda")
+        adj_c.x.copy_(torch.from_numpy(cw))
+        runtime.tape_backward(G, Q, part, mesh, prm, adj_c, ctx=ctx)
+        return adj_c.numpy()
+
+    gs = {"f64": grads(np.float64, G64), "f32": grads(np.float32, G32)}
 
     def loss64(Q):
         Qd = Q.to("torch", device="cuda")
@@ -269,15 +309,17 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
             if field == "v":
                 Qp.v += eps * d
                 Qm.v -= eps * d
-                ad = float(np.sum(g["v"] * d))
+                ad = {f: float(np.sum(g["v"] * d)) for f, g in gs.items()}
             else:
                 Qp.mu *= np.exp(eps * d)
                 Qp.lam *= np.exp(eps * d)
                 Qm.mu *= np.exp(-eps * d)
                 Qm.lam *= np.exp(-eps * d)
-                ad = float(np.sum((g["mu"] * host.mu + g["lam"] * host.lam) * d))
+                ad = {f: float(np.sum((g["mu"] * host.mu + g["lam"] * host.lam) * d)) for f, g in gs.items()}
             fd = (loss64(Qp) - loss64(Qm)) / (2 * eps)
-            checks.append({"field": field, "adjoint": ad, "fd": fd, "rel_err": abs(ad - fd) / max(abs(fd), 1e-30)})
+            checks.append({"field": field, "fd": fd, "adjoint_f64": ad["f64"], "adjoint_f32": ad["f32"],
+                           "rel_err_f64": abs(ad["f64"] - fd) / max(abs(fd), 1e-30),
+                           "rel_err_f32": abs(ad["f32"] - fd) / max(abs(fd), 1e-30)})
     del G64, P
     torch.cuda.empty_cache()
     return {
@@ -291,7 +333,8 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
         "grad_v0_norm": gnorm_v, "grad_logE_norm": gnorm_logE,
         "backward_kernels_ms_per_step": {k: v[1] / every for k, v in sorted(kt.items())},
         "fd_check": {"against": "central differences of the FP64 device rollout, L = sum c . x_T, random c",
-                     "max_rel_err": max(ch["rel_err"] for ch in checks), "directions": checks},
+                     "max_rel_err": max(ch["rel_err_f64"] for ch in checks),
+                     "max_rel_err_fp32_tape": max(ch["rel_err_f32"] for ch in checks), "directions": checks},
     }
 
 
@@ -394,9 +437,10 @@ def main():
         return e0.elapsed_time(e1), ctx.launches - l0
 
     results = {}
-    forms = (("f32", np.float32),) if args.quick else (("f32", np.float32), ("f64", np.float64))
-    for name, dtype in forms:
-        P = host64.to("torch", device="cuda", dtype=dtype)
+    forms = ("x64",) if args.quick else ("x64", "f32", "f64")
+    for name in forms:
+        dtype, x64, _ = FORMS[name]
+        P = host64.to("torch", device="cuda", dtype=dtype, x64=x64)
         part = tb.Partition(mesh, n, backend="torch", device="cuda")
         G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
         runtime.step(G, P, part, mesh, prm, args.warmup, ctx=ctx)
@@ -415,21 +459,23 @@ def main():
 
     if args.quick:
         if rank == 0:
-            f32 = results["f32"]
-            print(json.dumps({"metric": METRIC, "value": world * n * args.steps / (f32["ms"] * 1e-3),
+            hd = results["x64"]
+            print(json.dumps({"metric": METRIC, "value": world * n * args.steps / (hd["ms"] * 1e-3),
                               "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-                              "warmup": args.warmup, "ms_per_step": f32["ms"] / args.steps, "quick": True,
-                              "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(f32["kernels"].items())}}),
+                              "warmup": args.warmup, "ms_per_step": hd["ms"] / args.steps, "quick": True,
+                              "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(hd["kernels"].items())}}),
                   flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
 
-    # FP32 vs FP64 after 100 steps of the same scene (both on the device).
-    acc = {}
+    # Both FP32 forms against the plain FP64 form after 100 steps of the same
+    # scene (all on the device; the FP64 form is parity-tested against the
+    # FP64 oracle).
     Ps = {}
-    for name, dtype in (("f32", np.float32), ("f64", np.float64)):
-        P = host64.to("torch", device="cuda", dtype=dtype)
+    for name in ("x64", "f32", "f64"):
+        dtype, x64, _ = FORMS[name]
+        P = host64.to("torch", device="cuda", dtype=dtype, x64=x64)
         part = tb.Partition(mesh, n, backend="torch", device="cuda")
         G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
         runtime.step(G, P, part, mesh, prm, sc.nsteps, ctx=ctx)
@@ -441,17 +487,21 @@ def main():
     def rel(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
-    acc = {"steps": sc.nsteps, "rel_err_x": rel(Ps["f32"]["x"], Ps["f64"]["x"]),
-           "rel_err_v": rel(Ps["f32"]["v"], Ps["f64"]["v"]),
-           "rel_err_displacement": rel(Ps["f32"]["x"] - x0, Ps["f64"]["x"] - x0),
-           "against": "plain FP64 form on the device (parity-tested against the FP64 oracle)"}
+    def accuracy(name):
+        a, b = Ps[name], Ps["f64"]
+        return {"steps": sc.nsteps, "rel_err_x": rel(a["x"], b["x"]), "rel_err_v": rel(a["v"], b["v"]),
+                "rel_err_displacement": rel(a["x"] - x0, b["x"] - x0),
+                "against": "plain FP64 form on the device (parity-tested against the FP64 oracle)"}
+
+    acc = accuracy("x64")
+    acc_f32 = accuracy("f32")
     del Ps
 
     # End to end through the host-buffer C-ABI call: pinned host state in,
     # S MPM steps, state out, every call.
     S = 10
     calls = max(2, args.steps // S)
-    hostp = host64.to("pinned", dtype=np.float32)
+    hostp = host64.to("pinned", dtype=np.float32, x64=True)
     runtime.rollout_host(hostp, mesh, prm, S, ctx=ctx)  # allocates the context's device state
     barrier()
     t0 = time.perf_counter()
@@ -463,7 +513,7 @@ def main():
         hostp.F.nbytes
     e2e = {"value": world * n * S * calls / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": fbytes,
            "d2h_bytes_per_step": fbytes, "mpm_steps_per_call": S,
-           "note": "one bench step = one tb_rollout_host_f32 call on pinned host buffers (H2D, S steps, D2H)"}
+           "note": "one bench step = one tb_rollout_host_f32x64 call on pinned host buffers (H2D, S steps, D2H)"}
     del hostp
 
     adjoint = None if args.no_adjoint else adjoint_leg(tb, runtime, ctx, scale=args.adj_scale)
@@ -473,21 +523,20 @@ def main():
             dist.destroy_process_group()
         return
 
-    # Roofline of the dominant kernel (mixed FP32 form).
-    kt = results["f32"]["kernels"]
+    # Roofline of the dominant kernel of the headline form.
+    kt = results["x64"]["kernels"]
     dom = max(("p2g", "g2p"), key=lambda k: kt.get(k, (0, 0.0))[1])
     launches_dom, ms_dom = kt[dom]
-    per_p, per_n = algorithmic_bytes(dom, np.float32)
+    per_p, per_n = algorithmic_bytes(dom, 4, 8)
     nact = active_nodes(mesh, host64.x)
     alg_bytes = n * per_p + nact * per_n
     achieved = alg_bytes / (ms_dom / launches_dom * 1e-3) / 1e9
     peak, peak_src = measured_peaks()
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic_cube3d.json"
-    if tfile.exists():
-        tj = json.loads(tfile.read_text())
-        if dom in tj:
-            traffic = tj[dom]["dram_bytes_per_particle"] * n
+    traffic = read_traffic(dom, n)
+    sp, sn = step_bytes(4, 8)
+    step_alg = n * sp + nact * sn
+    hd = results["x64"]
+    step_gbs = step_alg / (hd["ms"] / args.steps * 1e-3) / 1e9
 
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -508,12 +557,12 @@ def main():
     f32, f64 = results["f32"], results["f64"]
     out = {
         "metric": METRIC,
-        "value": world * n * args.steps / (f32["ms"] * 1e-3),
+        "value": world * n * args.steps / (hd["ms"] * 1e-3),
         "unit": "particle-steps/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": f32["ms"] / args.steps,
+        "ms_per_step": hd["ms"] / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -521,22 +570,27 @@ def main():
         "data": "synthetic (seeded cube3d scene, numpy PCG64)",
         "config": {"workload": "cube3d: unit cube 256^3 cells, centre cube side 0.5 at 2^3 particles/cell, "
                                "Neo-Hookean E=1e6 nu=0.3, gravity, dt=5e-5; one MPM step per bench step",
-                   "n_particles": n, "scale": args.scale, "form": "mixed FP32 (FP64 F, det F, log J; FP64 tiles)",
+                   "n_particles": n, "scale": args.scale, "form": FORMS["x64"][2],
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (2.7 GB particle state per replica)"},
-        "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
+                   "l2": "inputs larger than L2 (3.1 GB particle state per replica)"},
         "accuracy": acc,
+        "fp32_positions": {"value": world * n * args.steps / (f32["ms"] * 1e-3), "ms_per_step": f32["ms"] / args.steps,
+                           "form": FORMS["f32"][2], "accuracy": acc_f32},
+        "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
         "adjoint_over_forward": adjoint,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_active_node": per_n,
                      "active_nodes": nact},
+        "step_roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak,
+                          "algorithmic_bytes": step_alg, "bytes_per_particle": sp, "bytes_per_active_node": sn},
         "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(kt.items())},
+        "kernels_ms_per_step_fp32_positions": {k: v[1] / 3 for k, v in sorted(f32["kernels"].items())},
         "kernels_ms_per_step_f64": {k: v[1] / 3 for k, v in sorted(f64["kernels"].items())},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": f32["launches"],
-        "clocks": f32["clocks"],
+        "gpu_launches": hd["launches"],
+        "clocks": hd["clocks"],
     }
     print(json.dumps(out), flush=True)
     if dist is not None:

@@ -216,6 +216,17 @@ int32_t tb_step_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, t
                     tb_grid* grid, const tb_step_params* params, int32_t nsteps);
 int32_t tb_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                     tb_grid* grid, const tb_step_params* params, int32_t nsteps);
+/* FP64-position form of tb_step_f32: particles->x[d] are double arrays, every
+ * other field as in tb_step_f32 (F double). Windows and in-cell offsets are
+ * computed from the FP64 positions, binning uses the Float64 findblock rule,
+ * and G2P adds the FP32 displacement to the FP64 position. A Float32 position
+ * near 0.5 carries an ulp of 6e-8, larger than a step's displacement rounding
+ * allows for 1e-5 accuracy over 100 steps; this form removes that error.
+ * B-spline / uGIMP bases with the FLIP/PIC transfer only (TB_ERR_UNSUPPORTED
+ * otherwise). The reference's counterpart is the same step under
+ * gpu_preserve (src/adapt.jl:15-17), which leaves chosen arrays in Float64. */
+int32_t tb_step_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                       tb_grid* grid, const tb_step_params* params, int32_t nsteps);
 
 /* ---- host-buffer rollout (end-to-end form of tb_step_*) ----------------
  * `host` holds HOST pointers (pinned memory recommended) for the particle state;
@@ -226,6 +237,9 @@ int32_t tb_rollout_host_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host
                             const tb_step_params* params, int32_t nsteps);
 int32_t tb_rollout_host_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
                             const tb_step_params* params, int32_t nsteps);
+/* host-buffer form of tb_step_f32x64 (x double on the host as well). */
+int32_t tb_rollout_host_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* host,
+                               const tb_step_params* params, int32_t nsteps);
 
 /* ---- reverse mode: sensitivities of a rollout ---------------------------
  * No counterpart in the reference: Tesserae.jl differentiates only constitutive

@@ -140,6 +140,11 @@ for _p in ("f64", "f32"):
                                          P(tb_step_params), P(tb_adjoint)]),
     ]
 
+SIGNATURES += [
+    ("tb_step_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params), I32]),
+    ("tb_rollout_host_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
+]
+
 PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "csrc" / "libtesserae_b200.so"
 

@@ -185,17 +185,20 @@ int check_params(tb_ctx* c, const tb_step_params* p) {
     return TB_OK;
 }
 
+// x64: the FP64-position form (particles.x are double arrays, the rest T).
 template <class T>
-int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool apic, PView<T>& P) {
+int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool apic, PView<T>& P,
+               bool x64 = false) {
     if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
     if (p->n < 0 || p->n > 0x7fffffffll)
         return fail(c, TB_ERR_CAPACITY, "particle count %lld exceeds the partition's Int32 capacity", (long long)p->n);
     std::memset(&P, 0, sizeof P);
     P.n = p->n;
     for (int d = 0; d < dim; ++d) {
-        P.x[d] = static_cast<T*>(p->x[d]);
+        if (x64) P.x64[d] = static_cast<double*>(p->x[d]);
+        else P.x[d] = static_cast<T*>(p->x[d]);
         P.v[d] = static_cast<T*>(p->v[d]);
-        if (p->n && !P.x[d]) return fail(c, TB_ERR_ARG, "particles.x[%d] is NULL", d);
+        if (p->n && !p->x[d]) return fail(c, TB_ERR_ARG, "particles.x[%d] is NULL", d);
         if (need_state && p->n && !P.v[d]) return fail(c, TB_ERR_ARG, "particles.v[%d] is NULL", d);
     }
     P.V = static_cast<T*>(p->V);
@@ -334,23 +337,27 @@ cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const G
 
 template <int D, class T, int BW>
 int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-             const tb_step_params* prm, int nsteps, bool do_bin, bool do_p2g, bool do_grid, bool do_g2p) {
+             const tb_step_params* prm, int nsteps, bool do_bin, bool do_p2g, bool do_grid, bool do_g2p,
+             bool x64 = false) {
     auto M = make_dmesh<D, T>(*m);
     auto S = make_scalars<T>(*prm);
     PView<T> P;
     GView<T> G;
     int rc;
-    if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P)) != TB_OK) return rc;
+    if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P, x64)) != TB_OK) return rc;
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
     BinBuffers B;
     if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
     const LaunchCfg cfg = cfg_of(c);
     const T* xs[3] = {P.x[0], P.x[1], D == 3 ? P.x[2] : P.x[1]};
+    // FP64 positions are binned by the FP64 findblock (the reference's Float64 rule)
+    const auto M64 = make_dmesh<D, double>(*m);
+    const double* xs64[3] = {P.x64[0], P.x64[1], D == 3 ? P.x64[2] : P.x64[1]};
     cudaError_t e = cudaSuccess;
     if ((do_p2g || do_grid) && (rc = touched_buffers(c, M.nblocks)) != TB_OK) return rc;
     c->grid_sparse_ok = false;  // the first step of every call runs densely
     for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
-        if (do_bin) e = launch_bin<D, T>(M, xs, P.n, B, cfg);
+        if (do_bin) e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xs, P.n, B, cfg);
         if (e == cudaSuccess && do_p2g) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
         if (e == cudaSuccess && do_grid) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
         if (e == cudaSuccess && do_g2p) e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg);
@@ -361,15 +368,18 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
 
 template <class T>
 int dispatch_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                  const tb_step_params* prm, int nsteps, bool b, bool p2g, bool gr, bool g2p) {
+                  const tb_step_params* prm, int nsteps, bool b, bool p2g, bool gr, bool g2p, bool x64 = false) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK) return rc;
     if ((rc = check_mesh(c, m)) != TB_OK) return rc;
     if ((rc = check_params(c, prm)) != TB_OK) return rc;
     if (nsteps < 0) return fail(c, TB_ERR_ARG, "nsteps must be >= 0");
-    if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
-    if (m->block_log2 == 3) return run_step<2, T, 8>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
-    return run_step<2, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p);
+    if (x64 && (prm->transfer != TB_TRANSFER_FLIP || prm->basis == TB_WLS_BSPLINE_QUADRATIC ||
+                prm->basis == TB_WLS_UGIMP))
+        return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs the B-spline / uGIMP FLIP step only");
+    if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
+    if (m->block_log2 == 3) return run_step<2, T, 8>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
+    return run_step<2, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
 }
 
 template <class T>
@@ -454,7 +464,8 @@ int do_g2p_direct(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p
 // Host-buffer rollout: stage the particle state into a context-owned device
 // block, run the steps on a context-owned grid and partition, copy back.
 template <class T>
-int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm, int nsteps) {
+int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm, int nsteps,
+               bool x64 = false) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK) return rc;
     if ((rc = check_mesh(c, m)) != TB_OK) return rc;
@@ -477,7 +488,7 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     auto add = [&](void** slot, size_t elem, bool inout) {
         if (*slot) fields.push_back({slot, elem, inout});
     };
-    for (int d = 0; d < D; ++d) add(&host->x[d], sizeof(T), true);
+    for (int d = 0; d < D; ++d) add(&host->x[d], x64 ? sizeof(double) : sizeof(T), true);
     for (int d = 0; d < D; ++d) add(&host->v[d], sizeof(T), true);
     add(&host->V, sizeof(T), true);
     for (int k = 0; k < D * D; ++k) add(&host->grad_v[k], sizeof(T), true);
@@ -566,7 +577,7 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
         e = cudaMemcpyAsync(dptr[i], *fields[i].host_slot, fields[i].elem * size_t(n), cudaMemcpyHostToDevice,
                             c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "rollout H2D");
-    rc = dispatch_step<T>(c, m, &dev, &part, &g, prm, nsteps, true, true, true, true);
+    rc = dispatch_step<T>(c, m, &dev, &part, &g, prm, nsteps, true, true, true, true, x64);
     if (rc != TB_OK) return rc;
     for (size_t i = 0; i < fields.size() && e == cudaSuccess; ++i)
         if (fields[i].inout)
@@ -997,6 +1008,11 @@ int32_t tb_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true);
 }
 
+int32_t tb_step_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                       const tb_step_params* prm, int32_t nsteps) {
+    return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true, true);
+}
+
 int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
                             int32_t nsteps) {
     return do_rollout<double>(c, m, host, prm, nsteps);
@@ -1004,6 +1020,11 @@ int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, con
 int32_t tb_rollout_host_f32(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
                             int32_t nsteps) {
     return do_rollout<float>(c, m, host, prm, nsteps);
+}
+
+int32_t tb_rollout_host_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,
+                               int32_t nsteps) {
+    return do_rollout<float>(c, m, host, prm, nsteps, true);
 }
 
 int32_t tb_adjoint_step_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,

@@ -34,7 +34,7 @@ struct DMesh {
     long long nnodes;
     T xmin[3];
     T h, h_inv;
-    double xmin64[3], h64;
+    double xmin64[3], h64, h_inv64;
 };
 
 template <int D, class T>
@@ -54,14 +54,18 @@ inline DMesh<D, T> make_dmesh(const tb_mesh& m) {
     M.h = T(m.h);          // the Float32 form casts h and h_inv separately (src/adapt.jl:53-57)
     M.h_inv = T(m.h_inv);
     M.h64 = m.h;
+    M.h_inv64 = m.h_inv;
     return M;
 }
 
-// Particle SoA views. T is the state scalar; F is always double.
+// Particle SoA views. T is the state scalar; F is always double. In the
+// FP64-position form (FP32 state with FP64 positions) x is NULL and x64 holds
+// the positions; otherwise x64 is NULL.
 template <class T>
 struct PView {
     long long n;
     T* x[3];
+    double* x64[3];
     T* v[3];
     T* V;
     const T* m;
@@ -190,9 +194,7 @@ __device__ __forceinline__ void jet_ugimp(T xi, T l, T& val, T& der) {
 // Fast full-support axis values (bspline.jl:90-100): t = fract(xi - 1/2),
 // N = (1/2 - t + t^2/2, 1/2 + t - t^2, t^2/2), N' = (t - 1, 1 - 2t, t).
 template <class T>
-__device__ __forceinline__ void bspline_quadratic_axis(T xi, T* v0, T* v1) {
-    T u = xi - T(0.5);
-    T t = u - floor(u);
+__device__ __forceinline__ void bspline_quadratic_poly(T t, T* v0, T* v1) {
     const T half = T(0.5);
     v0[0] = half + t * (T(-1) + t * half);
     v0[1] = half + t * (T(1) + t * T(-1));
@@ -200,6 +202,13 @@ __device__ __forceinline__ void bspline_quadratic_axis(T xi, T* v0, T* v1) {
     v1[0] = T(-1) + t;
     v1[1] = T(1) + t * T(-2);
     v1[2] = t;
+}
+
+template <class T>
+__device__ __forceinline__ void bspline_quadratic_axis(T xi, T* v0, T* v1) {
+    T u = xi - T(0.5);
+    T t = u - floor(u);
+    bspline_quadratic_poly(t, v0, v1);
 }
 
 // Window and 1-D jets of one particle for B-spline / uGIMP kernels (the
@@ -393,6 +402,92 @@ __device__ __forceinline__ bool prepare_basis(const DMesh<D, T>& M, int basis, c
         if (!wls_minv<D, T>(M, B.ax, x, closed, B.Mi)) {
             atomicOr(err, ERR_WLS_SINGULAR);
             return false;
+        }
+    }
+    return true;
+}
+
+// FP64-position form: the window and the 1-D jets of a particle whose position
+// is FP64. xi = (x - xmin) h_inv and the in-cell offsets are computed in FP64;
+// only the offset from the window's first node, a number in [0, 3), is rounded
+// to T before the jets are evaluated, so the weights carry T's relative
+// precision of that offset rather than of the absolute coordinate. Window rules
+// as axis_window (B-spline and uGIMP; WLS is not on this form).
+template <int D, class T>
+__device__ __forceinline__ bool axis_window_x64(const DMesh<D, T>& M, int basis, const double* x, double lnorm,
+                                                double* xi, int* lo, int* cnt) {
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        xi[d] = (x[d] - M.xmin64[d]) * M.h_inv64;
+        const double c = floor(xi[d]);
+        inside = inside && (c >= 0.0 && c <= double(M.n[d] - 2));
+    }
+    if (!inside) return false;
+    const bool gimp = basis == TB_UGIMP;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        int st, e;
+        if (gimp) {
+            const double r = 1.0 + lnorm / 2.0;
+            st = int(floor(xi[d] - r)) + 1;
+            e = int(floor(xi[d] + r));
+        } else {
+            st = int(floor(xi[d] - 0.5));
+            e = st + 2;
+        }
+        lo[d] = max(st, 0);
+        cnt[d] = min(e, M.n[d] - 1) - lo[d] + 1;
+    }
+    return true;
+}
+
+template <int D, class T>
+__device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basis, const double* x, T l_abs,
+                                                  Basis<D, T>& B, int* err) {
+    double lnorm = 0.0;
+    const bool gimp = basis == TB_UGIMP;
+    if (gimp) {
+        lnorm = double(l_abs) / M.h64;
+        if (!(lnorm >= 0.0 && lnorm <= 1.0)) {
+            atomicOr(err, ERR_GIMP_LENGTH);
+            return false;
+        }
+    }
+    double xi[3];
+    int lo[3], cnt[3];
+    if (!axis_window_x64<D, T>(M, basis, x, lnorm, xi, lo, cnt)) return false;
+    B.wls = false;
+    bool full = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        B.ax[d].lo = lo[d];
+        B.ax[d].cnt = cnt[d];
+        full = full && cnt[d] == 3;
+    }
+    if (!gimp && full) {
+        // the fast path's t = fract(xi - 1/2) is xi - 1/2 - lo, in [0, 1); kept
+        // below 1 after rounding so that the jets stay on the FP64 window
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            T t = T(xi[d] - 0.5 - double(lo[d]));
+            if (t >= T(1)) t = T(1) - T(1) / T(1 << 24);
+            bspline_quadratic_poly(t, B.ax[d].val, B.ax[d].der);
+        }
+        return true;
+    }
+    const T ln = T(lnorm);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            B.ax[d].val[k] = T(0);
+            B.ax[d].der[k] = T(0);
+            if (k < cnt[d]) {
+                const T xn = T(xi[d] - double(lo[d] + k));
+                if (gimp) jet_ugimp(xn, ln, B.ax[d].val[k], B.ax[d].der[k]);
+                else jet_bspline_quadratic(xn, B.ax[d].val[k], B.ax[d].der[k]);
+            }
         }
     }
     return true;

@@ -543,7 +543,7 @@ struct PencilShape {
     static constexpr int NPART = NC * NPENCIL * NJK * TS;
 };
 
-template <int D, class T, int BW, int NR>
+template <int D, class T, int BW, int NR, bool X64>
 __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_pencil_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
                                                                     const int* __restrict__ totals,
                                                                     const int* __restrict__ blocklist,
@@ -596,6 +596,7 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
             int grp[ITEMS], rank[ITEMS];
             long long pid[ITEMS];
             T px[ITEMS][3], pv[ITEMS][3], pV[ITEMS], pm[ITEMS], pl[ITEMS], psg[ITEMS][6];
+            double pxd[ITEMS][3];
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
                 const int ti = tid + u * NT;
@@ -607,7 +608,13 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
                 const bool on = pid[u] >= 0;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    px[u][d] = (on && d < D) ? P.x[d < D ? d : 0][p] : T(0);
+                    if constexpr (X64) {
+                        pxd[u][d] = (on && d < D) ? P.x64[d < D ? d : 0][p] : 0.0;
+                        px[u][d] = T(0);
+                    } else {
+                        px[u][d] = (on && d < D) ? P.x[d < D ? d : 0][p] : T(0);
+                        pxd[u][d] = 0.0;
+                    }
                     pv[u][d] = (on && d < D) ? P.v[d < D ? d : 0][p] : T(0);
                 }
                 pV[u] = on ? P.V[p] : T(0);
@@ -621,17 +628,30 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
                 grp[u] = -1;
                 rank[u] = 0;
                 if (pid[u] < 0) continue;
-                T xi[3];
                 int lo[3], cnt[3];
-                T lnorm = T(0);
-                if (gimp) {
-                    lnorm = pl[u] / M.h;
-                    if (!(lnorm >= T(0) && lnorm <= T(1))) {
-                        atomicOr(err, ERR_GIMP_LENGTH);
-                        continue;
+                bool inside;
+                if constexpr (X64) {
+                    double xi[3], lnorm = 0.0;
+                    if (gimp) {
+                        lnorm = double(pl[u]) / M.h64;
+                        if (!(lnorm >= 0.0 && lnorm <= 1.0)) {
+                            atomicOr(err, ERR_GIMP_LENGTH);
+                            continue;
+                        }
                     }
+                    inside = axis_window_x64<D, T>(M, s.basis, pxd[u], lnorm, xi, lo, cnt);
+                } else {
+                    T xi[3], lnorm = T(0);
+                    if (gimp) {
+                        lnorm = pl[u] / M.h;
+                        if (!(lnorm >= T(0) && lnorm <= T(1))) {
+                            atomicOr(err, ERR_GIMP_LENGTH);
+                            continue;
+                        }
+                    }
+                    inside = axis_window<D, T>(M, s.basis, px[u], lnorm, xi, lo, cnt);
                 }
-                if (!axis_window<D, T>(M, s.basis, px[u], lnorm, xi, lo, cnt)) continue;
+                if (!inside) continue;
                 int gi = 0;
                 bool ok = true;
 #pragma unroll
@@ -686,7 +706,8 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
             for (int u = 0; u < ITEMS; ++u) {
                 if (grp[u] < 0) continue;
                 Basis<D, T> B;
-                prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err);
+                if constexpr (X64) prepare_basis_x64<D, T>(M, s.basis, pxd[u], pl[u], B, err);
+                else prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err);
                 T* r = rec + (gstart[grp[u]] + rank[u]) * PRS;
                 const T mp = pm[u];
                 const T nV = -pV[u];
@@ -806,13 +827,13 @@ size_t pencil_smem_bytes() {
     return sizeof(T) * (size_t(NR) * PRS + SH::NPART) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
 }
 
-template <int D, class T, int BW>
+template <int D, class T, int BW, bool X64>
 cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
                           const BinBuffers& b, const LaunchCfg& cfg) {
     // Records per batch: a whole cube3d block (512). FP32: 2 CTAs per SM
-    // (78 KB of shared memory, 110 registers); FP64: 1 CTA per SM.
+    // (103 KB of shared memory); FP64: 1 CTA per SM.
     constexpr int NR = 512;
-    auto kern = p2g_pencil_kernel<D, T, BW, NR>;
+    auto kern = p2g_pencil_kernel<D, T, BW, NR, X64>;
     const size_t smem = pencil_smem_bytes<D, T, BW, NR>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e == cudaSuccess)
@@ -865,7 +886,13 @@ cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& 
                        const BinBuffers& b, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
-    return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_pencil<D, T, BW>(M, P, G, s, b, cfg);
+    if (P.x64[0]) {  // FP64-position form: plain path, FP32 state only (checked by the caller)
+        if constexpr (sizeof(T) == 4) {
+            if (!gen) return launch_pencil<D, T, BW, true>(M, P, G, s, b, cfg);
+        }
+        return cudaErrorInvalidValue;
+    }
+    return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_pencil<D, T, BW, false>(M, P, G, s, b, cfg);
 }
 
 #define TB_INST_P2G(D, T, BW)                                                                        \

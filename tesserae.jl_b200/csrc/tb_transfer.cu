@@ -169,12 +169,14 @@ __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& 
     for (int r = 0; r < D; ++r)
 #pragma unroll
         for (int c = 0; c < D; ++c) P.gv[r + c * D][p] = gv[r][c];
+    if (P.x[0]) {  // the FP64-position form writes x itself
 #pragma unroll
-    for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
+        for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
+    }
     particle_update<D, T>(P, s, p, gv, F);
 }
 
-template <int D, class T, int BW, bool GEN>
+template <int D, class T, int BW, bool GEN, bool X64>
 __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 8 : 4)) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
                                                        const int* __restrict__ totals,
                                                        const int* __restrict__ blocklist,
@@ -220,8 +222,14 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
         const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int j = s0 + tid; j < s1; j += nth) {
             const long long p = perm[j] - 1;
-            T x[3], vp[3];
-            load_x<D, T>(P, p, x);
+            T x[3] = {T(0), T(0), T(0)}, vp[3];
+            double xd[3] = {0.0, 0.0, 0.0};
+            if constexpr (X64) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) xd[d] = P.x64[d][p];
+            } else {
+                load_x<D, T>(P, p, x);
+            }
 #pragma unroll
             for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
             double F[3][3];
@@ -230,7 +238,10 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
             T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
             T gv[3][3] = {}, Bn[3][3] = {};
             Basis<D, T> B;
-            if (prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err)) {
+            bool in;
+            if constexpr (X64) in = prepare_basis_x64<D, T>(M, s.basis, xd, l, B, err);
+            else in = prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err);
+            if (in) {
                 int q0[3] = {0, 0, 0};
                 bool ok = true;
 #pragma unroll
@@ -325,6 +336,10 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
                 }
             }
             g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
+            if constexpr (X64) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) P.x64[d][p] = xd[d] + double(dxs[d]);
+            }
         }
         __syncthreads();
     }
@@ -407,7 +422,7 @@ __global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T>
         T gv[3][3] = {}, Bn[3][3] = {};
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-            x[d] = P.x[d][p];
+            x[d] = P.x[0] ? P.x[d][p] : T(0);  // FP64 positions stay as they are
             vp[d] = P.v[d][p];
         }
         double F[3][3];
@@ -487,7 +502,15 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
                        const BinBuffers& b, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
-    auto kern = gen ? g2p_tile_kernel<D, T, BW, true> : g2p_tile_kernel<D, T, BW, false>;
+    auto kern = gen ? g2p_tile_kernel<D, T, BW, true, false> : g2p_tile_kernel<D, T, BW, false, false>;
+    if (P.x64[0]) {  // FP64-position form: plain path, FP32 state only (checked by the caller)
+        if constexpr (sizeof(T) == 4) {
+            if (gen) return cudaErrorInvalidValue;
+            kern = g2p_tile_kernel<D, T, BW, false, true>;
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
     const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), M.nblocks);
     {
         KernelScope ks(cfg, "g2p");

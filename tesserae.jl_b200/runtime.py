@@ -10,7 +10,9 @@ C ABI of libtesserae_b200.so.
   rollout_grad                                  gradients of a rollout loss w.r.t. v0 and log E
 
 The precision form follows the particle dtype: float64 -> the plain `_f64`
-entry points, float32 (F float64) -> the mixed `_f32` ones. Every call raises
+entry points, float32 (F float64) -> the mixed `_f32` ones, float32 with
+float64 positions (`Particles(..., x64=True)`) -> `tb_step_f32x64` /
+`tb_rollout_host_f32x64` (step and rollout_host only). Every call raises
 RuntimeError with the library's message on a non-zero status; there is no
 fallback path.
 """
@@ -86,6 +88,14 @@ class Context:
     def fn(self, name: str, dtype):
         return getattr(self.lib, f"{name}_{_suffix(dtype)}")
 
+    def pfn(self, name: str, particles: Particles, x64_ok: bool = False):
+        """Entry point for the particles' precision form."""
+        if getattr(particles, "x64", False):
+            if not x64_ok:
+                raise TypeError(f"{name}: the FP64-position form is available for step and rollout_host only")
+            return getattr(self.lib, f"{name}_f32x64")
+        return self.fn(name, particles.dtype)
+
 
 def _ref(s):
     return C.byref(s)
@@ -97,14 +107,16 @@ def update(target, particles: Particles, mesh: CartesianMesh, params=None, ctx: 
     if isinstance(target, BasisWeights):
         if params is None:
             raise ValueError("update(weights, ...) needs step params (basis kind, uGIMP length)")
-        rc = ctx.fn("tb_update_weights", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+        rc = ctx.pfn("tb_update_weights", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                           _ref(params), _ref(target.struct()))
         ctx.check(rc, "update!(weights)")
         return target
     if isinstance(target, Partition):
         na, nass = C.c_int64(), C.c_int64()
-        rc = ctx.fn("tb_bin_particles", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
-                                                         _ref(target.struct()), C.byref(na), C.byref(nass))
+        # binning reads only x: FP64 positions bin by the Float64 rule
+        xdtype = np.float64 if getattr(particles, "x64", False) else particles.dtype
+        rc = ctx.fn("tb_bin_particles", xdtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                _ref(target.struct()), C.byref(na), C.byref(nass))
         ctx.check(rc, "update!(partition)")
         target.nactive, target.nassigned = na.value, nass.value
         return target
@@ -116,7 +128,7 @@ def P2G(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianM
     """The recognised @P2G body: m = sum w m_p, mv = sum w m_p v_p (APIC: + B D^-1 (x_i - x_p)),
     f = sum -V sigma grad w + w m_p g; with `grid_half`, vn = mv/m and v = vn + dt f/m."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_p2g", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_p2g", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                            _ref(partition.struct()), _ref(grid.struct()), _ref(params))
     ctx.check(rc, "@P2G")
     if grid_half:
@@ -129,7 +141,7 @@ def P2G(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianM
 def G2P(grid: Grid, particles: Particles, mesh: CartesianMesh, params, ctx: Context | None = None):
     """The recognised @G2P body (README.md:79-86 / APIC)."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_g2p", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(grid.struct()),
+    rc = ctx.pfn("tb_g2p", particles)(ctx.ptr, _ref(mesh.struct()), _ref(grid.struct()),
                                            _ref(particles.struct()), _ref(params))
     ctx.check(rc, "@G2P")
     return particles
@@ -139,9 +151,9 @@ def step(grid: Grid, particles: Particles, partition: Partition, mesh: Cartesian
          ctx: Context | None = None):
     """`nsteps` fused steps (bin -> P2G -> grid update -> G2P) without host sync."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_step", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
-                                            _ref(partition.struct()), _ref(grid.struct()), _ref(params),
-                                            int(nsteps))
+    rc = ctx.pfn("tb_step", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                    _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                                    int(nsteps))
     ctx.check(rc, "step")
 
 
@@ -151,8 +163,8 @@ def rollout_host(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     ctx = ctx or _default()
     if particles.backend not in ("numpy", "pinned"):
         raise TypeError("rollout_host takes host (numpy or pinned) particles")
-    rc = ctx.fn("tb_rollout_host", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
-                                                    _ref(params), int(nsteps))
+    rc = ctx.pfn("tb_rollout_host", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()),
+                                                            _ref(particles.struct()), _ref(params), int(nsteps))
     ctx.check(rc, "rollout_host")
 
 
@@ -162,7 +174,7 @@ def adjoint_step(grid: Grid, particles: Particles, partition: Partition, mesh: C
     `adj` (float64 device arrays) maps end-of-step sensitivities to start-of-step
     ones in place (mu / lam accumulate)."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_adjoint_step", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_adjoint_step", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                     _ref(adj.struct()))
     ctx.check(rc, "adjoint_step")
@@ -172,7 +184,7 @@ def tape_forward(grid: Grid, particles: Particles, partition: Partition, mesh: C
                  nsteps: int, checkpoint_every: int = 20, ctx: Context | None = None):
     """Advance `nsteps` steps (as `step`) keeping checkpoints every `checkpoint_every` steps."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_tape_forward", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_tape_forward", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                     int(nsteps), int(checkpoint_every))
     ctx.check(rc, "tape_forward")
@@ -183,7 +195,7 @@ def tape_backward(grid: Grid, particles: Particles, partition: Partition, mesh: 
     """Sensitivities to the final state (in `adj`) -> sensitivities to the step-0
     state; `particles` is restored to the step-0 state."""
     ctx = ctx or _default()
-    rc = ctx.fn("tb_tape_backward", particles.dtype)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_tape_backward", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                      _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                      _ref(adj.struct()))
     ctx.check(rc, "tape_backward")

@@ -148,16 +148,18 @@ def nsym(dim: int) -> int:
 
 class Particles:
     """SoA particle state. Scalar type `dtype` (float64 or float32) for every
-    field except F, which is float64 in both forms."""
+    field except F, which is float64 in both forms. With `x64=True` (float32
+    only) the positions are float64 as well: the FP64-position form."""
 
     FIELDS = ("x", "v", "V", "m", "l", "grad_v", "sigma", "F", "B", "V0", "mu", "lam")
 
-    def __init__(self, n, dim, dtype=np.float64, backend="numpy", device=None, optional=()):
+    def __init__(self, n, dim, dtype=np.float64, backend="numpy", device=None, optional=(), x64=False):
         self.n, self.dim, self.dtype = int(n), int(dim), np.dtype(dtype).type
+        self.x64 = bool(x64) and self.dtype == np.float32
         self.backend, self.device = backend, device
         D = self.dim
         a = lambda shape, dt=self.dtype, fill=0.0: _alloc(backend, shape, dt, device, fill)  # noqa: E731
-        self.x = a((D, self.n))
+        self.x = a((D, self.n), np.float64 if self.x64 else self.dtype)
         self.v = a((D, self.n))
         self.V = a((self.n,))
         self.grad_v = a((D * D, self.n))
@@ -199,18 +201,20 @@ class Particles:
         s.lambda_ = _ptr(self.lam)
         return s
 
-    def to(self, backend, device=None, dtype=None) -> "Particles":
-        """Copy into another backend (numpy <-> torch) and/or scalar type."""
+    def to(self, backend, device=None, dtype=None, x64=None) -> "Particles":
+        """Copy into another backend (numpy <-> torch) and/or scalar type
+        (`x64`: float64 positions with a float32 state; default: as self)."""
         dtype = np.dtype(dtype or self.dtype).type
+        x64 = self.x64 if x64 is None else bool(x64)
         opt = tuple(k for k in ("m", "l", "B", "V0", "mu", "lam") if getattr(self, k) is not None)
-        out = Particles(self.n, self.dim, dtype, backend, device, optional=opt)
+        out = Particles(self.n, self.dim, dtype, backend, device, optional=opt, x64=x64)
         for k in self.FIELDS:
             src = getattr(self, k)
             if src is None:
                 continue
             dst = getattr(out, k)
             srcn = src if isinstance(src, np.ndarray) else src.detach().cpu().numpy()
-            tdt = np.float64 if k == "F" else dtype
+            tdt = np.float64 if (k == "F" or (k == "x" and out.x64)) else dtype
             if backend in ("numpy", "pinned"):
                 dst[...] = srcn.astype(tdt)
             else:

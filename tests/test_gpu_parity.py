@@ -296,6 +296,97 @@ def test_step_fp32_vs_fp64_oracle(tb, oracle, ctx):
     assert err_u <= 1e-3, err_u
 
 
+def test_step_x64_vs_fp64_oracle(tb, oracle, ctx):
+    """The FP64-position form (tb_step_f32x64: FP32 state, FP64 positions and F)
+    after 100 steps against the FP64 oracle: relative L2 error <= 1e-6 on
+    positions and velocities and <= 1e-5 on displacements, and at least 10x
+    below the Float32-position form on every one of them."""
+    from tesserae_b200 import runtime
+    sc = tb.scenes.cube3d(scale=8)
+    mesh, prm = sc.mesh, sc.params
+    P64 = sc.particles
+    x0 = P64.x.copy()
+    errs = {}
+    for form, kw in (("f32", {}), ("x64", {"x64": True})):
+        Pd = P64.to("torch", device="cuda", dtype=np.float32, **kw)
+        assert Pd.x.dtype == (torch.float64 if kw else torch.float32)
+        part = tb.Partition(mesh, P64.n, backend="torch", device="cuda")
+        Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+        runtime.step(Gd, Pd, part, mesh, prm, 100, ctx=ctx)
+        ctx.synchronize()
+        errs[form] = Pd.numpy()
+    Po = P64.to("numpy")
+    Go = tb.generate_grid(mesh)
+    oracle.step(mesh, Po, Go, prm, 100)
+    res = {}
+    for form, got in errs.items():
+        res[form] = (rel_l2(got["x"].astype(np.float64), Po.x), rel_l2(got["v"].astype(np.float64), Po.v),
+                     rel_l2(got["x"].astype(np.float64) - x0, Po.x - x0))
+    ex, ev, eu = res["x64"]
+    assert ex <= 1e-6 and ev <= 1e-6 and eu <= 1e-5, res
+    for a, b in zip(res["x64"], res["f32"]):
+        assert a * 10 <= b, res
+
+
+def test_step_x64_binning_matches_fp64(tb, oracle, ctx):
+    """Binning in the FP64-position form follows the Float64 findblock rule: the
+    partition after one step equals the oracle's FP64 binning of the new
+    positions bit for bit."""
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", np.float64)
+    mesh, prm = sc.mesh, sc.params
+    Pd = P.to("torch", device="cuda", dtype=np.float32, x64=True)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+    runtime.step(Gd, Pd, part, mesh, prm, 2, ctx=ctx)
+    ctx.synchronize()
+    xnew = tb.Particles(P.n, 3)
+    xnew.x[...] = Pd.x.cpu().numpy()
+    part2 = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    runtime.step(Gd, Pd, part2, mesh, prm, 1, ctx=ctx)  # bins the same positions first
+    ctx.synchronize()
+    part_o = tb.Partition(mesh, P.n)
+    na, nass = oracle.bin(mesh, xnew, part_o)
+    part2.nactive, part2.nassigned = na, nass  # the fused step does not read the totals back
+    assert_same_partition(part_o, part2, (na, nass))
+
+
+def test_rollout_host_x64_matches_device_step(tb, ctx):
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", np.float32)
+    mesh, prm = sc.mesh, sc.params
+    P = P.to("numpy", x64=True)
+    assert P.x.dtype == np.float64
+    Pd = P.to("torch", device="cuda")
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+    runtime.step(Gd, Pd, part, mesh, prm, 3, ctx=ctx)
+    ctx.synchronize()
+    runtime.rollout_host(P, mesh, prm, 3, ctx=ctx)
+    got = Pd.numpy()
+    for k in ("x", "v", "F", "sigma", "V"):
+        assert rel_l2(getattr(P, k), got[k]) <= 1e-6, k
+
+
+def test_x64_rejects_other_forms(tb, ctx):
+    """The FP64-position form runs the B-spline / uGIMP FLIP step only: APIC is
+    refused with TB_ERR_UNSUPPORTED, and the per-kernel verbs refuse it in Python."""
+    import ctypes
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", np.float32)
+    mesh = sc.mesh
+    Pd = P.to("torch", device="cuda", x64=True)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+    prm = type(sc.params).from_buffer_copy(sc.params)
+    prm.transfer = tb._abi.TB_TRANSFER_APIC
+    rc = ctx.lib.tb_step_f32x64(ctx.ptr, ctypes.byref(mesh.struct()), ctypes.byref(Pd.struct()),
+                                ctypes.byref(part.struct()), ctypes.byref(Gd.struct()), ctypes.byref(prm), 1)
+    assert rc == tb._abi.TB_ERR_UNSUPPORTED
+    with pytest.raises(TypeError):
+        runtime.G2P(Gd, Pd, mesh, sc.params, ctx=ctx)
+
+
 def test_rollout_host_matches_device_step(tb, ctx):
     from tesserae_b200 import runtime
     sc, P = small_scene(tb, "cube", np.float32)
