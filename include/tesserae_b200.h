@@ -228,6 +228,39 @@ int32_t tb_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, t
 int32_t tb_step_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                        tb_grid* grid, const tb_step_params* params, int32_t nsteps);
 
+/* ---- reorder_particles! -------------------------------------------------
+ * reference: reorder_particles!(particles, partition; threshold) and
+ * block_ordered_particle_contiguity (src/Parallel/gpu_block_strategy.jl:172-238,
+ * src/Parallel/cpu_block_strategy.jl:221-269). The partition must come from
+ * binning these particles. The score is the fraction of neighbouring particles
+ * in memory that share a block (1 when fully block-grouped); with `threshold` in
+ * [0, 1] the particles are reordered when the score is below it (always at 1,
+ * never at 0): every field present in `particles` is permuted into block order,
+ * partition->blockids follow and partition->particleindices become 1..n. Fields
+ * are 4 or 8 bytes per the precision form (x double in _f32x64, F always double).
+ * Synchronous; `reordered` (may be NULL) receives 1 if it reordered. Particles
+ * outside the mesh are an error when a reorder is due (TB_ERR_ARG), as on the
+ * reference's GPU path. */
+int32_t tb_reorder_particles_f64(tb_ctx* ctx, int32_t dim, tb_particles* particles, tb_partition* partition,
+                                 double threshold, int32_t* reordered);
+int32_t tb_reorder_particles_f32(tb_ctx* ctx, int32_t dim, tb_particles* particles, tb_partition* partition,
+                                 double threshold, int32_t* reordered);
+int32_t tb_reorder_particles_f32x64(tb_ctx* ctx, int32_t dim, tb_particles* particles, tb_partition* partition,
+                                    double threshold, int32_t* reordered);
+/* block_ordered_particle_contiguity of `n` particles binned into `partition`. Synchronous. */
+int32_t tb_particle_contiguity(tb_ctx* ctx, const tb_partition* partition, int64_t n, double* score);
+/* tb_step_* with reorder_particles!(particles, partition; threshold) after every
+ * binning, decided on the device (no host synchronisation): the loop of
+ * docs/literate/tutorials/taylor_impact.jl:120-127. A reorder that is due while
+ * particles lie outside the mesh is skipped and reported as TB_ERR_DEVICE at the
+ * next synchronising call. */
+int32_t tb_step_reorder_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, int32_t nsteps, double threshold);
+int32_t tb_step_reorder_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                            tb_grid* grid, const tb_step_params* params, int32_t nsteps, double threshold);
+int32_t tb_step_reorder_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                               tb_grid* grid, const tb_step_params* params, int32_t nsteps, double threshold);
+
 /* ---- host-buffer rollout (end-to-end form of tb_step_*) ----------------
  * `host` holds HOST pointers (pinned memory recommended) for the particle state;
  * the context stages it into its own device buffers, runs `nsteps` steps and

@@ -18,7 +18,8 @@ def __getattr__(name):
     # The device API needs torch and the built library; import it lazily so the
     # host-only parts (scenes, containers) load without either.
     if name in ("runtime", "Context", "update", "P2G", "G2P", "step", "rollout_host", "adjoint_step",
-                "tape_forward", "tape_backward", "rollout_grad", "RolloutFunction"):
+                "tape_forward", "tape_backward", "rollout_grad", "RolloutFunction", "reorder_particles",
+                "block_ordered_particle_contiguity"):
         import importlib
         runtime = importlib.import_module(__name__ + ".runtime")
         return runtime if name == "runtime" else getattr(runtime, name)

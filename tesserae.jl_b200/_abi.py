@@ -143,7 +143,14 @@ for _p in ("f64", "f32"):
 SIGNATURES += [
     ("tb_step_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params), I32]),
     ("tb_rollout_host_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
+    ("tb_particle_contiguity", I32, [VP, P(tb_partition), I64, P(C.c_double)]),
 ]
+for _p in ("f64", "f32", "f32x64"):
+    SIGNATURES += [
+        (f"tb_reorder_particles_{_p}", I32, [VP, I32, P(tb_particles), P(tb_partition), C.c_double, P(I32)]),
+        (f"tb_step_reorder_{_p}", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                        P(tb_step_params), I32, C.c_double]),
+    ]
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "csrc" / "libtesserae_b200.so"

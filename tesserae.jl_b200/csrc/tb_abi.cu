@@ -111,6 +111,13 @@ struct tb_ctx {
     long long tape_n = 0;
     int tape_dim = 0, tape_elem = 0;
     int tape_nsteps = 0, tape_every = 1;
+    // reorder_particles!: 8-byte-per-particle scratch, score accumulators,
+    // decision words and the score
+    unsigned long long* ro_scratch = nullptr;
+    long long ro_scratch_cap = 0;
+    unsigned long long* ro_acc = nullptr;  // [2]
+    int* ro_decision = nullptr;            // [2]
+    double* ro_score = nullptr;            // [1]
 };
 
 namespace {
@@ -279,8 +286,59 @@ int check_device_status(tb_ctx* c) {
         if (h & ERR_TILE_RANGE) why += " support window outside its block tile;";
         if (h & ERR_GIMP_LENGTH) why += " uGIMP requires 0 <= l <= spacing(mesh);";
         if (h & ERR_WLS_SINGULAR) why += " singular WLS moment matrix;";
+        if (h & ERR_REORDER_OUTSIDE)
+            why += " reorder_particles!: some particles are outside the mesh and were not assigned to any block;";
         return fail(c, TB_ERR_DEVICE, "kernel reported:%s", why.c_str());
     }
+    return TB_OK;
+}
+
+// Every particle field present in `p` with its element size (x is double in
+// the FP64-position form, F always double, the rest the state scalar).
+int particle_fields(const tb_particles* p, int D, size_t elem, bool x64, std::vector<ReorderField>& out) {
+    out.clear();
+    auto add = [&](void* ptr, size_t e) {
+        if (ptr) out.push_back({ptr, int(e)});
+    };
+    for (int d = 0; d < D; ++d) add(p->x[d], x64 ? sizeof(double) : elem);
+    for (int d = 0; d < D; ++d) add(p->v[d], elem);
+    add(p->V, elem);
+    add(p->m, elem);
+    add(p->l, elem);
+    for (int k = 0; k < D * D; ++k) add(p->grad_v[k], elem);
+    for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(p->sigma[k], elem);
+    for (int k = 0; k < D * D; ++k) add(p->F[k], sizeof(double));
+    for (int k = 0; k < D * D; ++k) add(p->B[k], elem);
+    add(p->V0, elem);
+    add(p->mu, elem);
+    add(p->lambda, elem);
+    return TB_OK;
+}
+
+int reorder_args(tb_ctx* c, const tb_partition* part, long long n, double threshold, ReorderArgs& a) {
+    if (!part || (n && (!part->blockids || !part->particleindices)) || !part->counts || !part->offsets)
+        return fail(c, TB_ERR_ARG, "partition array is NULL");
+    cudaError_t e;
+    if ((e = grow(c->ro_scratch, c->ro_scratch_cap, n)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc reorder");
+    if (!c->ro_acc) {
+        if ((e = cudaMalloc(&c->ro_acc, 2 * sizeof(unsigned long long))) != cudaSuccess ||
+            (e = cudaMalloc(&c->ro_decision, 2 * sizeof(int))) != cudaSuccess ||
+            (e = cudaMalloc(&c->ro_score, sizeof(double))) != cudaSuccess)
+            return cuda_fail(c, e, "cudaMalloc reorder words");
+    }
+    a = ReorderArgs{};
+    a.n = n;
+    a.nblocks = int(part->nblocks);
+    a.blockids = part->blockids;
+    a.perm = part->particleindices;
+    a.counts = part->counts;
+    a.offsets = part->offsets;
+    a.threshold = threshold;
+    a.acc = c->ro_acc;
+    a.decision = c->ro_decision;
+    a.score = c->ro_score;
+    a.scratch = c->ro_scratch;
+    a.report_outside = true;
     return TB_OK;
 }
 
@@ -338,7 +396,7 @@ cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const G
 template <int D, class T, int BW>
 int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
              const tb_step_params* prm, int nsteps, bool do_bin, bool do_p2g, bool do_grid, bool do_g2p,
-             bool x64 = false) {
+             bool x64 = false, double reorder_threshold = 0.0) {
     auto M = make_dmesh<D, T>(*m);
     auto S = make_scalars<T>(*prm);
     PView<T> P;
@@ -355,9 +413,20 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
     const double* xs64[3] = {P.x64[0], P.x64[1], D == 3 ? P.x64[2] : P.x64[1]};
     cudaError_t e = cudaSuccess;
     if ((do_p2g || do_grid) && (rc = touched_buffers(c, M.nblocks)) != TB_OK) return rc;
+    // reorder_particles!(particles, partition; threshold) after every binning
+    // (the loop of docs/literate/tutorials/taylor_impact.jl:120-127)
+    const bool reorder = do_bin && reorder_threshold > 0.0;
+    std::vector<ReorderField> fields;
+    ReorderArgs RA{};
+    if (reorder) {
+        particle_fields(p, D, sizeof(T), x64, fields);
+        if ((rc = reorder_args(c, part, P.n, reorder_threshold, RA)) != TB_OK) return rc;
+    }
     c->grid_sparse_ok = false;  // the first step of every call runs densely
     for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
         if (do_bin) e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xs, P.n, B, cfg);
+        if (e == cudaSuccess && reorder) e = launch_reorder_score(RA, cfg);
+        if (e == cudaSuccess && reorder) e = launch_reorder_apply(RA, fields.data(), int(fields.size()), cfg);
         if (e == cudaSuccess && do_p2g) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
         if (e == cudaSuccess && do_grid) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
         if (e == cudaSuccess && do_g2p) e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg);
@@ -368,7 +437,8 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
 
 template <class T>
 int dispatch_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                  const tb_step_params* prm, int nsteps, bool b, bool p2g, bool gr, bool g2p, bool x64 = false) {
+                  const tb_step_params* prm, int nsteps, bool b, bool p2g, bool gr, bool g2p, bool x64 = false,
+                  double reorder_threshold = 0.0) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK) return rc;
     if ((rc = check_mesh(c, m)) != TB_OK) return rc;
@@ -377,9 +447,48 @@ int dispatch_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* pa
     if (x64 && (prm->transfer != TB_TRANSFER_FLIP || prm->basis == TB_WLS_BSPLINE_QUADRATIC ||
                 prm->basis == TB_WLS_UGIMP))
         return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs the B-spline / uGIMP FLIP step only");
-    if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
-    if (m->block_log2 == 3) return run_step<2, T, 8>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
-    return run_step<2, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64);
+    if (!(reorder_threshold >= 0.0 && reorder_threshold <= 1.0))
+        return fail(c, TB_ERR_ARG, "reorder threshold must be in [0, 1]");
+    if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64, reorder_threshold);
+    if (m->block_log2 == 3)
+        return run_step<2, T, 8>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64, reorder_threshold);
+    return run_step<2, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64, reorder_threshold);
+}
+
+// reorder_particles!(particles, partition; threshold) on its own: the partition
+// must come from binning these particles. Synchronous (returns whether it
+// reordered); particles outside the mesh are an error when a reorder is due, as
+// on the reference's GPU path (gpu_block_strategy.jl:213-216).
+int do_reorder(tb_ctx* c, tb_particles* p, tb_partition* part, int dim, size_t elem, bool x64, double threshold,
+               int32_t* reordered, double* score) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
+    if (dim != 2 && dim != 3) return fail(c, TB_ERR_ARG, "dim must be 2 or 3");
+    if (!(threshold >= 0.0 && threshold <= 1.0)) return fail(c, TB_ERR_ARG, "threshold must be in [0, 1]");
+    if (p->n < 0 || p->n > 0x7fffffffll) return fail(c, TB_ERR_CAPACITY, "particle count exceeds Int32 capacity");
+    for (int d = 0; d < dim; ++d)
+        if (p->n && !p->x[d]) return fail(c, TB_ERR_ARG, "particles.x[%d] is NULL", d);
+    std::vector<ReorderField> fields;
+    particle_fields(p, dim, elem, x64, fields);
+    ReorderArgs RA{};
+    if ((rc = reorder_args(c, part, p->n, threshold, RA)) != TB_OK) return rc;
+    RA.report_outside = false;
+    const LaunchCfg cfg = cfg_of(c);
+    cudaError_t e = launch_reorder_score(RA, cfg);
+    if (e == cudaSuccess) e = launch_reorder_apply(RA, fields.data(), int(fields.size()), cfg);
+    int dec[2] = {0, 0};
+    double sc = 1.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dec, c->ro_decision, sizeof dec, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sc, c->ro_score, sizeof sc, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "reorder");
+    if (reordered) *reordered = dec[0];
+    if (score) *score = sc;
+    if (dec[1])
+        return fail(c, TB_ERR_ARG, "reorder_particles!: some particles are outside the mesh and were not assigned "
+                                   "to any block; filter them out before reordering on GPU");
+    return TB_OK;
 }
 
 template <class T>
@@ -901,6 +1010,10 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->adj_grid);
     cudaFree(c->tape_cp);
     cudaFree(c->tape_seg);
+    cudaFree(c->ro_scratch);
+    cudaFree(c->ro_acc);
+    cudaFree(c->ro_decision);
+    cudaFree(c->ro_score);
     delete c->prof;
     delete c;
 }
@@ -1011,6 +1124,49 @@ int32_t tb_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
 int32_t tb_step_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
                        const tb_step_params* prm, int32_t nsteps) {
     return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true, true);
+}
+
+int32_t tb_step_reorder_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, int32_t nsteps, double threshold) {
+    return dispatch_step<double>(c, m, p, part, g, prm, nsteps, true, true, true, true, false, threshold);
+}
+int32_t tb_step_reorder_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                            const tb_step_params* prm, int32_t nsteps, double threshold) {
+    return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true, false, threshold);
+}
+int32_t tb_step_reorder_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                               const tb_step_params* prm, int32_t nsteps, double threshold) {
+    return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true, true, threshold);
+}
+
+int32_t tb_reorder_particles_f64(tb_ctx* c, int32_t dim, tb_particles* p, tb_partition* part, double threshold,
+                                 int32_t* reordered) {
+    return do_reorder(c, p, part, dim, sizeof(double), false, threshold, reordered, nullptr);
+}
+int32_t tb_reorder_particles_f32(tb_ctx* c, int32_t dim, tb_particles* p, tb_partition* part, double threshold,
+                                 int32_t* reordered) {
+    return do_reorder(c, p, part, dim, sizeof(float), false, threshold, reordered, nullptr);
+}
+int32_t tb_reorder_particles_f32x64(tb_ctx* c, int32_t dim, tb_particles* p, tb_partition* part, double threshold,
+                                    int32_t* reordered) {
+    return do_reorder(c, p, part, dim, sizeof(float), true, threshold, reordered, nullptr);
+}
+
+int32_t tb_particle_contiguity(tb_ctx* c, const tb_partition* part, int64_t n, double* score) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if (!score) return fail(c, TB_ERR_ARG, "score is NULL");
+    if (n < 0 || n > 0x7fffffffll) return fail(c, TB_ERR_CAPACITY, "particle count exceeds Int32 capacity");
+    ReorderArgs RA{};
+    if ((rc = reorder_args(c, const_cast<tb_partition*>(part), n, 0.0, RA)) != TB_OK) return rc;
+    RA.report_outside = false;
+    cudaError_t e = launch_reorder_score(RA, cfg_of(c));
+    double sc = 1.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sc, c->ro_score, sizeof sc, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "contiguity");
+    *score = sc;
+    return TB_OK;
 }
 
 int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,

@@ -22,7 +22,8 @@ namespace tb {
 enum : int {
     ERR_TILE_RANGE = 1,   // a support window left its block tile
     ERR_GIMP_LENGTH = 2,  // uGIMP requires 0 <= l <= h (gimp.jl:22)
-    ERR_WLS_SINGULAR = 4  // WLS moment matrix not invertible
+    ERR_WLS_SINGULAR = 4,  // WLS moment matrix not invertible
+    ERR_REORDER_OUTSIDE = 8  // a reorder was due but particles lie outside the mesh
 };
 
 template <int D, class T>

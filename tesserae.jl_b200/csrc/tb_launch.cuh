@@ -129,4 +129,29 @@ template <int D, class T>
 cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* grad_w,
                                   long long* window, const LaunchCfg& cfg);
 
+// reorder_particles! (tb_reorder.cu). One particle field: a device array of n
+// elements of `elem` (4 or 8) bytes.
+struct ReorderField {
+    void* ptr;
+    int elem;
+};
+struct ReorderArgs {
+    long long n;
+    int nblocks;
+    int* blockids;         // [n] permuted with the particles
+    int* perm;             // [n] 1-based block-sorted permutation; identity after a reorder
+    const int* counts;     // [nblocks]
+    const int* offsets;    // [nblocks + 1]
+    double threshold;      // reorder when the score is below it (always at >= 1, never at <= 0)
+    unsigned long long* acc;  // [2] scratch: same-block neighbours, non-empty blocks
+    int* decision;         // [2] reorder now; reorder wanted but particles lie outside the mesh
+    double* score;         // [1] contiguity score
+    void* scratch;         // [n] x 8 bytes
+    bool report_outside;   // raise ERR_REORDER_OUTSIDE in the status word when a reorder is refused
+};
+// Score and decision on the device (no host synchronisation).
+cudaError_t launch_reorder_score(const ReorderArgs& a, const LaunchCfg& cfg);
+// Permute `fields`, the block ids and the permutation when decision[0] is set.
+cudaError_t launch_reorder_apply(const ReorderArgs& a, const ReorderField* fields, int nfields, const LaunchCfg& cfg);
+
 }  // namespace tb

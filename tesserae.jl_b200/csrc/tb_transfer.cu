@@ -198,6 +198,10 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
             b /= M.nb[d];
         }
         b = blocklist[bi] - 1;
+        // the block's particle range and this thread's first particle id are
+        // loaded before the tile, so their round trips overlap the tile's
+        const int s0 = offsets[b], s1 = offsets[b + 1];
+        int pnext = (s0 + tid < s1) ? perm[s0 + tid] : 1;
         for (int t = tid; t < TN; t += nth) {
             int node[3], rem = t;
             bool inside = true;
@@ -219,9 +223,9 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
             }
         }
         __syncthreads();
-        const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int j = s0 + tid; j < s1; j += nth) {
-            const long long p = perm[j] - 1;
+            const long long p = pnext - 1;
+            pnext = (j + nth < s1) ? perm[j + nth] : 1;  // next id in flight during this particle
             T x[3] = {T(0), T(0), T(0)}, vp[3];
             double xd[3] = {0.0, 0.0, 0.0};
             if constexpr (X64) {

@@ -6,6 +6,7 @@ C ABI of libtesserae_b200.so.
   P2G(grid, particles, partition, mesh, params) @P2G (m, mv, f sums + grid half)        p2g.jl:66, gpu.jl:196
   G2P(grid, particles, mesh, params)            @G2P (FLIP/APIC + Neo-Hookean)          g2p.jl:71, gpu.jl:226
   step(...)                                     the whole README.md:66-87 loop body, n times
+  reorder_particles(particles, partition, thr)  reorder_particles!                      gpu_block_strategy.jl:194
   adjoint_step / tape_forward / tape_backward   reverse mode (no reference counterpart)
   rollout_grad                                  gradients of a rollout loss w.r.t. v0 and log E
 
@@ -148,13 +149,44 @@ def G2P(grid: Grid, particles: Particles, mesh: CartesianMesh, params, ctx: Cont
 
 
 def step(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params, nsteps: int = 1,
-         ctx: Context | None = None):
-    """`nsteps` fused steps (bin -> P2G -> grid update -> G2P) without host sync."""
+         ctx: Context | None = None, reorder_threshold: float | None = None):
+    """`nsteps` fused steps (bin -> P2G -> grid update -> G2P) without host sync.
+    With `reorder_threshold`, every binning is followed by
+    `reorder_particles!(particles, partition; threshold=reorder_threshold)`,
+    decided on the device."""
     ctx = ctx or _default()
-    rc = ctx.pfn("tb_step", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
-                                                    _ref(partition.struct()), _ref(grid.struct()), _ref(params),
-                                                    int(nsteps))
+    if reorder_threshold is None:
+        rc = ctx.pfn("tb_step", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                        _ref(partition.struct()), _ref(grid.struct()), _ref(params),
+                                                        int(nsteps))
+    else:
+        rc = ctx.pfn("tb_step_reorder", particles, x64_ok=True)(
+            ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()), _ref(partition.struct()), _ref(grid.struct()),
+            _ref(params), int(nsteps), float(reorder_threshold))
     ctx.check(rc, "step")
+
+
+def reorder_particles(particles: Particles, partition: Partition, threshold: float = 1.0,
+                      ctx: Context | None = None) -> bool:
+    """reorder_particles!(particles, partition; threshold) (src/Parallel/gpu_block_strategy.jl:194-202):
+    permute every particle field into the partition's block order when the
+    contiguity score is below `threshold`; returns whether it reordered."""
+    ctx = ctx or _default()
+    done = C.c_int32()
+    rc = ctx.pfn("tb_reorder_particles", particles, x64_ok=True)(ctx.ptr, int(particles.dim), _ref(particles.struct()),
+                                                                 _ref(partition.struct()), float(threshold),
+                                                                 C.byref(done))
+    ctx.check(rc, "reorder_particles!")
+    return bool(done.value)
+
+
+def block_ordered_particle_contiguity(partition: Partition, n: int, ctx: Context | None = None) -> float:
+    """Tesserae.block_ordered_particle_contiguity (src/Parallel/gpu_block_strategy.jl:172-191)."""
+    ctx = ctx or _default()
+    score = C.c_double()
+    ctx.check(ctx.lib.tb_particle_contiguity(ctx.ptr, _ref(partition.struct()), int(n), C.byref(score)),
+              "block_ordered_particle_contiguity")
+    return float(score.value)
 
 
 def rollout_host(particles: Particles, mesh: CartesianMesh, params, nsteps: int, ctx: Context | None = None):
