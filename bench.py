@@ -259,6 +259,13 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
 
     P = host.to("torch", device="cuda", dtype=np.float32)
     runtime.step(G32, P, part, mesh, prm, 3, ctx=ctx)  # warm-up
+    # warm-up of the tape: its checkpoint and segment buffers are allocated once
+    # per context (grow-only) on the first call, outside the timed region
+    P = host.to("torch", device="cuda", dtype=np.float32)
+    runtime.tape_forward(G32, P, part, mesh, prm, 2 * every, every, ctx=ctx)
+    adj_w = tb.Adjoint(n, 3, backend="torch", device="cuda")
+    runtime.tape_backward(G32, P, part, mesh, prm, adj_w, ctx=ctx)
+    del adj_w
     P = host.to("torch", device="cuda", dtype=np.float32)
     fwd_ms = timed(lambda: runtime.step(G32, P, part, mesh, prm, nsteps, ctx=ctx))
     P = host.to("torch", device="cuda", dtype=np.float32)

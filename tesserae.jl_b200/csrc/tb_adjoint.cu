@@ -14,9 +14,10 @@
 // H is the Hessian of the kernel with respect to x_p (per-axis second
 // derivatives of the quadratic B-spline or uGIMP). The forward values (weights,
 // grid velocities) are read in the state type T; every adjoint quantity is FP64.
-// Both particle passes are block-scheduled like the forward G2P: one CTA per
-// non-empty grid block with the block's (BW+3)^D halo tile in shared memory,
-// so the gathers stay on chip; the scatter of 1. uses global FP64 atomics.
+// Both particle passes keep the (BW+3)^D halo tile of the block they work on
+// in shared memory, so the gathers stay on chip; the scatter of 1. uses global
+// FP64 atomics. G2P^T runs one CTA per block, P2G^T one CTA per chunk of 512
+// particles of the block-sorted permutation.
 #include "tb_launch.cuh"
 
 namespace tb {
@@ -115,6 +116,11 @@ __device__ __forceinline__ double det_cof(const double (&F)[3][3], double (&C)[3
 }
 
 constexpr int ADJ_THREADS = 128;
+// P2G backwards walks the block-sorted permutation in chunks of ADJ_CHUNK
+// particles, one chunk per CTA at a time, loading the halo tile of each block
+// the chunk touches: a crowded block is shared by several CTAs and a sparse
+// scene still fills the GPU.
+constexpr int ADJ_CHUNK = 512;
 
 // Block origin (first tile node per axis) of 0-based block b.
 template <int D, class T, int BW>
@@ -169,6 +175,8 @@ __device__ __forceinline__ int tile_slot(const int (&q0)[3], const int (&idx)[3]
 // tile in shared memory for the gathers; the v / vn sensitivities go straight to
 // the global FP64 grid with fire-and-forget atomics (an FP64 shared tile, where
 // all of a block's particles collide on a few hundred nodes, measured 3.7x
+// slower on the sphere scene). One CTA per block, not per chunk: chunks of one
+// crowded block on several SMs scatter to the same nodes at once (measured 1.5x
 // slower on the sphere scene).
 template <int D, class T, int BW>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
@@ -182,7 +190,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
     const double dt = s.dt64, alpha = double(s.alpha);
     const int nactive = totals[0], tid = threadIdx.x;
     for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+      {
         const int b = blocklist[bi] - 1;
+        const int s0 = offsets[b], s1 = offsets[b + 1];
         int org[3];
         block_origin<D, T, BW>(M, b, org);
         for (int t = tid; t < TN; t += ADJ_THREADS) {
@@ -196,7 +206,6 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
             }
         }
         __syncthreads();
-        const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
             const long long p = perm[j] - 1;
             T x[3] = {T(0), T(0), T(0)};
@@ -311,6 +320,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
                 for (int c = 0; c < D; ++c) A.F[r + c * D][p] = Fbn[r][c];
         }
         __syncthreads();
+      }
     }
 }
 
@@ -358,21 +368,26 @@ __global__ void __launch_bounds__(256) adj_grid_kernel(DMesh<D, T> M, GView<T> G
     }
 }
 
-// P2G backwards, one CTA per non-empty block: the block's halo tile of
+// P2G backwards, one CTA per chunk of the permutation: the block's halo tile of
 // (m_bar, mv_bar, f_bar) in shared memory, gathered per particle, then the
 // constitutive adjoint in FP64.
 template <int D, class T, int BW>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s, AdjView A,
                                                               GradGrid GB, const int* __restrict__ totals,
-                                                              const int* __restrict__ blocklist,
+                                                              const int* __restrict__ blockids,
                                                               const int* __restrict__ offsets,
                                                               const int* __restrict__ perm, int* err) {
     constexpr int TS = BW + 3, TN = (D == 3) ? TS * TS * TS : TS * TS;
     constexpr int NC = 1 + 2 * D;
     __shared__ double tg[NC * TN];  // m_bar at [t], mv_bar_d at [(1 + d) TN + t], f_bar_d at [(1 + D + d) TN + t]
-    const int nactive = totals[0], tid = threadIdx.x;
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
-        const int b = blocklist[bi] - 1;
+    const int nassigned = totals[1], tid = threadIdx.x;
+    const int nchunks = (nassigned + ADJ_CHUNK - 1) / ADJ_CHUNK;
+    for (int ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
+      const int c1 = min((ci + 1) * ADJ_CHUNK, nassigned);
+      for (int c0 = ci * ADJ_CHUNK; c0 < c1;) {
+        // the block of the chunk's next particle, and the part of the chunk in it
+        const int b = blockids[perm[c0] - 1] - 1;
+        const int s0 = c0, s1 = min(offsets[b + 1], c1);
         int org[3];
         block_origin<D, T, BW>(M, b, org);
         for (int t = tid; t < TN; t += ADJ_THREADS) {
@@ -386,7 +401,6 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PVi
             }
         }
         __syncthreads();
-        const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
             const long long p = perm[j] - 1;
             T x[3] = {T(0), T(0), T(0)};
@@ -504,6 +518,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PVi
             if (A.lam) A.lam[p] += lamb;
         }
         __syncthreads();
+        c0 = s1;
+      }
     }
 }
 
@@ -519,6 +535,8 @@ cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<
     }
     if (e != cudaSuccess) return e;
     const int bgrid = std::max(1, std::min(M.nblocks, cfg.num_sms * 8));
+    const int cgrid = int(std::max<long long>(1, std::min<long long>((P.n + ADJ_CHUNK - 1) / ADJ_CHUNK,
+                                                                     (long long)cfg.num_sms * 8)));
     const int ngrid = int(std::max<long long>(1, std::min<long long>((M.nnodes + 255) / 256, (long long)cfg.num_sms * 8)));
     if (P.n > 0) {
         KernelScope ks(cfg, "adj_g2p");
@@ -542,7 +560,7 @@ cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<
     }
     if (P.n > 0) {
         KernelScope ks(cfg, "adj_p2g");
-        adj_p2g_kernel<D, T, BW><<<bgrid, ADJ_THREADS, 0, cfg.stream>>>(M, P, s, A, GB, part.totals, part.blocklist,
+        adj_p2g_kernel<D, T, BW><<<cgrid, ADJ_THREADS, 0, cfg.stream>>>(M, P, s, A, GB, part.totals, part.blockids,
                                                                        part.offsets, part.perm, cfg.err);
         ++*cfg.launches;
         e = cudaGetLastError();
