@@ -522,6 +522,87 @@ __device__ __forceinline__ void accumulate_plain(const PlainRec<T>& o, T (&acc)[
     }
 }
 
+// Compact record (interior blocks of a quadratic B-spline, where no window is
+// truncated): [0] m_p [1..3] m_p v_p [4..9] S [10..12] t per axis, the fast
+// path's t = fract(xi - 1/2) (bspline.jl:90-100), [13] unused. 14 words: the
+// row lanes evaluate the 1-D jets from t with the polynomial of
+// bspline_quadratic_poly, so the weights agree with the full record's to
+// rounding. Records are 8-byte aligned (56-byte stride).
+constexpr int CRS = 14;
+
+// Coefficients of the quadratic B-spline slot k as a + t (b + t c) and its
+// derivative e + t f (bspline_quadratic_poly, slot by slot).
+struct SlotPoly {
+    float a, b, c, e, f;
+};
+__device__ __forceinline__ SlotPoly slot_poly(int k) {
+    if (k == 0) return {0.5f, -1.0f, 0.5f, -1.0f, 1.0f};
+    if (k == 1) return {0.5f, 1.0f, -1.0f, 1.0f, -2.0f};
+    return {0.0f, 0.0f, 0.5f, 0.0f, 1.0f};
+}
+
+template <class T>
+struct CompactRec {
+    V2<T> m0, m1, s0, s1, s2, t01, t2;
+};
+
+template <int D, class T>
+__device__ __forceinline__ void load_compact(const T* r, CompactRec<T>& o) {
+    o.m0 = ld2(r + 0);
+    o.m1 = ld2(r + 2);
+    o.s0 = ld2(r + 4);
+    o.s1 = ld2(r + 6);
+    if constexpr (D == 3) o.s2 = ld2(r + 8);
+    o.t01 = ld2(r + 10);
+    if constexpr (D == 3) o.t2 = ld2(r + 12);
+}
+
+template <int D, class T>
+__device__ __forceinline__ void accumulate_compact(const CompactRec<T>& o, const SlotPoly& py, const SlotPoly& pz,
+                                                   T h_inv, T (&acc)[3][1 + 2 * D]) {
+    const T mp = o.m0.a;
+    const T mv[3] = {o.m0.b, o.m1.a, o.m1.b};
+    T S[6] = {o.s0.a, o.s0.b, o.s1.a, o.s1.b, T(0), T(0)};
+    if constexpr (D == 3) {
+        S[4] = o.s2.a;
+        S[5] = o.s2.b;
+    }
+    const T tx = o.t01.a, ty = o.t01.b;
+    const T half = T(0.5);
+    const T wx[3] = {half + tx * (T(-1) + tx * half), half + tx * (T(1) + tx * T(-1)), tx * (tx * half)};
+    const T dx[3] = {(T(-1) + tx) * h_inv, (T(1) + tx * T(-2)) * h_inv, tx * h_inv};
+    const T wy = T(py.a) + ty * (T(py.b) + ty * T(py.c));
+    const T dy = (T(py.e) + ty * T(py.f)) * h_inv;
+    T wyz, dyz, wdz = T(0);
+    if constexpr (D == 3) {
+        const T tz = o.t2.a;
+        const T wz = T(pz.a) + tz * (T(pz.b) + tz * T(pz.c));
+        const T dz = (T(pz.e) + tz * T(pz.f)) * h_inv;
+        wyz = wy * wz;
+        dyz = dy * wz;
+        wdz = wy * dz;
+    } else {
+        wyz = wy;
+        dyz = dy;
+    }
+    T fa[3], fb[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        fa[a] = S[symidx<D>(a, 0)] * wyz;
+        fb[a] = S[symidx<D>(a, 1)] * dyz;
+        if constexpr (D == 3) fb[a] += S[symidx<D>(a, 2)] * wdz;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const T w = wx[i] * wyz;
+        acc[i][0] += w * mp;
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[i][1 + d] += w * mv[d];
+#pragma unroll
+        for (int a = 0; a < D; ++a) acc[i][1 + D + a] += dx[i] * fa[a] + wx[i] * fb[a];
+    }
+}
+
 template <int NC, class T>
 __device__ __forceinline__ void stage_node(T* part, int base, int stride, const T (&a)[NC]) {
 #pragma unroll
@@ -543,8 +624,11 @@ struct PencilShape {
     static constexpr int NPART = NC * NPENCIL * NJK * TS;
 };
 
-template <int D, class T, int BW, int NR, bool X64>
-__global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_pencil_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
+// MODE 0: every block with the full record; 1: compact records, interior
+// blocks only (their halo tile lies inside the mesh, so no window is
+// truncated); 2: full records, the other blocks only.
+template <int D, class T, int BW, int NR, bool X64, int MODE>
+__global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ? 2 : 1)) p2g_pencil_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
                                                                     const int* __restrict__ totals,
                                                                     const int* __restrict__ blocklist,
                                                                     const int* __restrict__ offsets,
@@ -559,9 +643,10 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
     constexpr int CSTR = NPENCIL * NJK * TS;  // stride between components in the staging array
     static_assert(NPENCIL <= 32, "pencil ranking runs in one warp");
 
+    constexpr int RS = (MODE == 1) ? CRS : PRS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* rec = reinterpret_cast<T*>(smem_raw);
-    T* part = rec + NR * PRS;
+    T* part = rec + NR * RS;
     int* gcount = reinterpret_cast<int*>(part + SH::NPART);
     int* gstart = gcount + NG;
     int* pslot = gstart + NG + 1;
@@ -571,6 +656,7 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
     const int jk = lane % NJK, sub = lane / NJK;
     const int sj = jk % 3, sk = (D == 3) ? jk / 3 : 0;
     const bool gimp = s.basis == TB_UGIMP;
+    const SlotPoly py = slot_poly(sj), pz = slot_poly(sk);
 
     for (int g = tid; g < NG; g += NT) gcount[g] = 0;
     __syncthreads();
@@ -585,6 +671,12 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
                 org[d] = (r % M.nb[d]) * BW - 1;
                 r /= M.nb[d];
             }
+        }
+        if constexpr (MODE != 0) {
+            bool interior = true;
+#pragma unroll
+            for (int d = 0; d < D; ++d) interior = interior && org[d] >= 0 && org[d] + TS - 1 <= M.n[d] - 1;
+            if (interior != (MODE == 1)) continue;  // the other kernel's block (uniform over the CTA)
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int b0 = s0; b0 < s1; b0 += NR) {
@@ -705,6 +797,34 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
                 if (grp[u] < 0) continue;
+                if constexpr (MODE == 1) {
+                    // t = fract(xi - 1/2) per axis, as the fast path computes it
+                    T t[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        if constexpr (X64) {
+                            const double xi = (pxd[u][d] - M.xmin64[d]) * M.h_inv64;
+                            const double u64 = xi - 0.5;
+                            T tt = T(u64 - floor(u64));
+                            if (tt >= T(1)) tt = T(1) - T(1) / T(1 << 24);
+                            t[d] = tt;
+                        } else {
+                            const T uu = (px[u][d] - M.xmin[d]) * M.h_inv - T(0.5);
+                            t[d] = uu - floor(uu);
+                        }
+                    }
+                    T* r = rec + (gstart[grp[u]] + rank[u]) * CRS;
+                    const T mp = pm[u];
+                    const T nV = -pV[u];
+                    st2(r + 0, mp, mp * pv[u][0]);
+                    st2(r + 2, mp * pv[u][1], mp * pv[u][2]);
+                    st2(r + 4, nV * psg[u][0], nV * psg[u][1]);
+                    st2(r + 6, nV * psg[u][2], nV * psg[u][3]);
+                    st2(r + 8, nV * psg[u][4], nV * psg[u][5]);
+                    st2(r + 10, t[0], t[1]);
+                    st2(r + 12, t[2], T(0));
+                    continue;
+                }
                 Basis<D, T> B;
                 if constexpr (X64) prepare_basis_x64<D, T>(M, s.basis, pxd[u], pl[u], B, err);
                 else prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err);
@@ -755,17 +875,32 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
                     if (gx < G1) {
                         const int qe = gstart[gbase + gx + 1];
                         int q = qs;
-                        for (; q + 1 < qe; q += 2) {
-                            PlainRec<T> r0, r1;
-                            load_plain<D, T>(rec + q * PRS, sj, sk, r0);
-                            load_plain<D, T>(rec + (q + 1) * PRS, sj, sk, r1);
-                            accumulate_plain<D, T>(r0, acc);
-                            accumulate_plain<D, T>(r1, acc);
-                        }
-                        if (q < qe) {
-                            PlainRec<T> r0;
-                            load_plain<D, T>(rec + q * PRS, sj, sk, r0);
-                            accumulate_plain<D, T>(r0, acc);
+                        if constexpr (MODE == 1) {
+                            for (; q + 1 < qe; q += 2) {
+                                CompactRec<T> r0, r1;
+                                load_compact<D, T>(rec + q * CRS, r0);
+                                load_compact<D, T>(rec + (q + 1) * CRS, r1);
+                                accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
+                                accumulate_compact<D, T>(r1, py, pz, M.h_inv, acc);
+                            }
+                            if (q < qe) {
+                                CompactRec<T> r0;
+                                load_compact<D, T>(rec + q * CRS, r0);
+                                accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
+                            }
+                        } else {
+                            for (; q + 1 < qe; q += 2) {
+                                PlainRec<T> r0, r1;
+                                load_plain<D, T>(rec + q * PRS, sj, sk, r0);
+                                load_plain<D, T>(rec + (q + 1) * PRS, sj, sk, r1);
+                                accumulate_plain<D, T>(r0, acc);
+                                accumulate_plain<D, T>(r1, acc);
+                            }
+                            if (q < qe) {
+                                PlainRec<T> r0;
+                                load_plain<D, T>(rec + q * PRS, sj, sk, r0);
+                                accumulate_plain<D, T>(r0, acc);
+                            }
                         }
                         qs = qe;
                     }
@@ -821,20 +956,21 @@ __global__ void __launch_bounds__(P2G_THREADS, sizeof(T) == 4 ? 2 : 1) p2g_penci
     }
 }
 
-template <int D, class T, int BW, int NR>
+template <int D, class T, int BW, int NR, int MODE>
 size_t pencil_smem_bytes() {
     using SH = PencilShape<D, BW>;
-    return sizeof(T) * (size_t(NR) * PRS + SH::NPART) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
+    const int rs = (MODE == 1) ? CRS : PRS;
+    return sizeof(T) * (size_t(NR) * rs + SH::NPART) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
 }
 
-template <int D, class T, int BW, bool X64>
-cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
-                          const BinBuffers& b, const LaunchCfg& cfg) {
-    // Records per batch: a whole cube3d block (512). FP32: 2 CTAs per SM
-    // (103 KB of shared memory); FP64: 1 CTA per SM.
+template <int D, class T, int BW, bool X64, int MODE>
+cudaError_t launch_pencil_mode(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                               const BinBuffers& b, const LaunchCfg& cfg) {
+    // Records per batch: a whole cube3d block (512). FP32 full records: 2 CTAs per
+    // SM (103 KB of shared memory); compact records: 3 (72 KB); FP64: 1.
     constexpr int NR = 512;
-    auto kern = p2g_pencil_kernel<D, T, BW, NR, X64>;
-    const size_t smem = pencil_smem_bytes<D, T, BW, NR>();
+    auto kern = p2g_pencil_kernel<D, T, BW, NR, X64, MODE>;
+    const size_t smem = pencil_smem_bytes<D, T, BW, NR, MODE>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
@@ -842,10 +978,26 @@ cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2G_THREADS, smem);
     const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
-    KernelScope ks(cfg, "p2g");
     kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
     ++*cfg.launches;
     return cudaGetLastError();
+}
+
+// The quadratic B-spline in the FP32 forms runs two launches: compact records on
+// the interior blocks, full records on the blocks at the mesh boundary (their
+// windows may be truncated). Other bases and FP64 run one full-record launch.
+template <int D, class T, int BW, bool X64>
+cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                          const BinBuffers& b, const LaunchCfg& cfg) {
+    KernelScope ks(cfg, "p2g");
+    if constexpr (sizeof(T) == 4) {
+        if (s.basis == TB_BSPLINE_QUADRATIC) {
+            cudaError_t e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
+            if (e != cudaSuccess) return e;
+            return launch_pencil_mode<D, T, BW, X64, 2>(M, P, G, s, b, cfg);
+        }
+    }
+    return launch_pencil_mode<D, T, BW, X64, 0>(M, P, G, s, b, cfg);
 }
 
 template <int D, class T, int BW, bool GEN, int NR>
