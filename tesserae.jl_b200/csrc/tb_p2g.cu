@@ -609,8 +609,11 @@ __device__ __forceinline__ void stage_node(T* part, int base, int stride, const 
     for (int c = 0; c < NC; ++c) part[base + c * stride] = a[c];
 }
 
-// Staging layout: partial (component c, pencil pc, row jk, tile x) at
-// ((c * NPENCIL + pc) * NJK + jk) * TS + x.
+// Staging layout: partial (component c, row jk, pencil pc, tile x) at
+// ((c * NJK + jk) * NPENCIL + pc) * TS + x. For one row offset jk the pencils
+// (gy, gz) of a tile plane follow each other, so the gather's reads for
+// consecutive tile nodes are consecutive words (no bank conflicts within a
+// plane).
 template <int D, int BW>
 struct PencilShape {
     static constexpr int TS = BW + 3;
@@ -860,7 +863,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                 if (sub >= NSUB || slot >= NPENCIL) continue;
                 const int pc = pslot[slot];
                 const int gbase = G1 * pc;
-                const int pbase = (pc * NJK + jk) * TS;
+                const int pbase = (jk * NPENCIL + pc) * TS;
                 T acc[3][NC];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                         const int gy = tn[1] - jj, gz = (D == 3) ? tn[2] - kk : 0;
                         if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
                         const int pc = gy + G1 * gz;
-                        const int idx = (pc * NJK + jj + 3 * kk) * TS + tn[0];
+                        const int idx = ((jj + 3 * kk) * NPENCIL + pc) * TS + tn[0];
 #pragma unroll
                         for (int c = 0; c < NC; ++c) val[c] += double(part[idx + c * CSTR]);
                     }
