@@ -423,13 +423,25 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
         if ((rc = reorder_args(c, part, P.n, reorder_threshold, RA)) != TB_OK) return rc;
     }
     c->grid_sparse_ok = false;  // the first step of every call runs densely
+    // Inside one call, the G2P of step s counts the particles into blocks for
+    // step s + 1 (the count pass of its binning); the last step does not, so the
+    // partition left to the caller is the last step's own.
+    bool counted = false;
     for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
-        if (do_bin) e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xs, P.n, B, cfg);
+        if (do_bin) {
+            if (counted) e = launch_bin_rest(M.nblocks, P.n, B, cfg);
+            else e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xs, P.n, B, cfg);
+        }
+        const bool count_next = do_bin && do_g2p && s + 1 < nsteps;
+        counted = false;
         if (e == cudaSuccess && reorder) e = launch_reorder_score(RA, cfg);
         if (e == cudaSuccess && reorder) e = launch_reorder_apply(RA, fields.data(), int(fields.size()), cfg);
         if (e == cudaSuccess && do_p2g) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
         if (e == cudaSuccess && do_grid) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
-        if (e == cudaSuccess && do_g2p) e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg);
+        if (e == cudaSuccess && do_g2p) {
+            e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg, count_next);
+            counted = count_next;
+        }
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     return TB_OK;

@@ -147,6 +147,20 @@ __device__ __forceinline__ int findblock(const DMesh<D, T>& M, const T* x) {
     return lin + 1;
 }
 
+// findblock of an FP64 position with the mesh's FP64 xmin and h_inv (the
+// Float64 rule of cartesian.jl:271-285, as findblock<D, double>).
+template <int D, class T>
+__device__ __forceinline__ int findblock_x64(const DMesh<D, T>& M, const double* x) {
+    int lin = 0;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+        const double c = floor((x[d] - M.xmin64[d]) * M.h_inv64);
+        if (!(c >= 0.0 && c <= double(M.n[d] - 2))) return 0;
+        lin = lin * M.nb[d] + (int(c) >> M.L);
+    }
+    return lin + 1;
+}
+
 // Per-axis basis data of one particle: window start/count and the 1-D jets.
 template <class T>
 struct Axis {

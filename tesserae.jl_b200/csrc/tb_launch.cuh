@@ -73,9 +73,13 @@ cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Sc
 template <int D, class T>
 cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const LaunchCfg& cfg);
 
+// With `count_next`, G2P also writes every moved particle's block id for the
+// next step into b.blockids and adds it to b.counts (which the caller zeroes
+// first): the count pass of the next step's binning, so that step runs
+// launch_bin_rest only.
 template <int D, class T, int BW>
 cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
-                       const BinBuffers& b, const LaunchCfg& cfg);
+                       const BinBuffers& b, const LaunchCfg& cfg, bool count_next = false);
 
 // Sparse grid maintenance over node blocks touched now (cur) or in the previous
 // transfer (prev): see tb_transfer.cu.

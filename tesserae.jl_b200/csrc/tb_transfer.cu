@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
                                                        const int* __restrict__ totals,
                                                        const int* __restrict__ blocklist,
                                                        const int* __restrict__ offsets,
-                                                       const int* __restrict__ perm, int* err) {
+                                                       const int* __restrict__ perm, int* err,
+                                                       int* __restrict__ next_bid, int* __restrict__ next_count) {
     constexpr int TS = Tile<D, BW>::TS, TN = Tile<D, BW>::TN;
     // Component-major tile: v_r at [r TN + t], dv_r = (v - vn)_r at [(D + r) TN + t];
     // lanes reading different nodes hit different banks.
@@ -340,9 +341,29 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
                 }
             }
             g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
+            int nb = 0;
             if constexpr (X64) {
+                double xn[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-                for (int d = 0; d < D; ++d) P.x64[d][p] = xd[d] + double(dxs[d]);
+                for (int d = 0; d < D; ++d) {
+                    xn[d] = xd[d] + double(dxs[d]);
+                    P.x64[d][p] = xn[d];
+                }
+                if (next_bid) nb = findblock_x64<D, T>(M, xn);
+            } else {
+                if (next_bid) {
+                    T xn[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                    for (int d = 0; d < D; ++d) xn[d] = x[d] + dxs[d];  // the value g2p_finish stored
+                    nb = findblock<D, T>(M, xn);
+                }
+            }
+            if (next_bid) {
+                // the next step's count pass: warp-aggregated, as bin_count_kernel
+                next_bid[p] = nb;
+                const unsigned act = __activemask();
+                const unsigned peers = __match_any_sync(act, nb);
+                if (nb > 0 && int(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&next_count[nb - 1], __popc(peers));
             }
         }
         __syncthreads();
@@ -503,7 +524,7 @@ cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Sc
 
 template <int D, class T, int BW>
 cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
-                       const BinBuffers& b, const LaunchCfg& cfg) {
+                       const BinBuffers& b, const LaunchCfg& cfg, bool count_next) {
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
     auto kern = gen ? g2p_tile_kernel<D, T, BW, true, false> : g2p_tile_kernel<D, T, BW, false, false>;
@@ -517,12 +538,18 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
     }
     const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), M.nblocks);
     {
-        KernelScope ks(cfg, "g2p");
-        kern<<<grid, 128, 0, cfg.stream>>>(M, G, P, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+        // first: it reads this step's block ids, which the tiled pass below
+        // replaces with the next step's when it counts
+        KernelScope ks(cfg, "g2p_outside");
+        const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
+        g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
     }
-    KernelScope ks(cfg, "g2p_outside");
-    const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
-    g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
+    cudaError_t e = cudaSuccess;
+    if (count_next) e = cudaMemsetAsync(b.counts, 0, sizeof(int) * size_t(M.nblocks), cfg.stream);
+    if (e != cudaSuccess) return e;
+    KernelScope ks(cfg, "g2p");
+    kern<<<grid, 128, 0, cfg.stream>>>(M, G, P, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,
+                                       count_next ? b.blockids : nullptr, count_next ? b.counts : nullptr);
     *cfg.launches += 2;
     return cudaGetLastError();
 }
@@ -595,7 +622,7 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
                                                              const Scalars<T>&, const unsigned char*,          \
                                                              const unsigned char*, const LaunchCfg&);          \
     template cudaError_t launch_g2p<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,         \
-                                              const Scalars<T>&, const BinBuffers&, const LaunchCfg&);
+                                              const Scalars<T>&, const BinBuffers&, const LaunchCfg&, bool);
 
 TB_INST_T(3, double)
 TB_INST_T(3, float)

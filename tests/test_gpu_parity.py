@@ -387,6 +387,33 @@ def test_x64_rejects_other_forms(tb, ctx):
         runtime.G2P(Gd, Pd, mesh, sc.params, ctx=ctx)
 
 
+@pytest.mark.parametrize("dtype,x64", [(np.float64, False), (np.float32, False), (np.float32, True)])
+def test_multistep_partition_equals_fresh_binning(tb, ctx, dtype, x64):
+    """Inside one fused call, each step's G2P counts the particles into blocks
+    for the next step. The partition a 3-step call leaves equals a fresh
+    binning of the positions the third step started from, bit for bit."""
+    from tesserae_b200 import runtime
+    sc, P = small_scene(tb, "cube", np.float64)
+    P.sigma[...] = 0.0
+    mesh, prm = sc.mesh, sc.params
+    parts = []
+    for nsteps in (3, 2):
+        Pd = P.to("torch", device="cuda", dtype=dtype, x64=x64)
+        part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, Pd, part, mesh, prm, nsteps, ctx=ctx)
+        ctx.synchronize()
+        if nsteps == 2:
+            part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+            runtime.update(part, Pd, mesh, ctx=ctx)
+        parts.append(part.numpy())
+    a, b = parts
+    for k in ("blockids", "counts", "offsets", "particleindices"):
+        assert np.array_equal(a[k], b[k]), k
+    na = int(np.sum(b["counts"] > 0))
+    assert np.array_equal(a["blocklist"][:na], b["blocklist"][:na])
+
+
 def test_rollout_host_matches_device_step(tb, ctx):
     from tesserae_b200 import runtime
     sc, P = small_scene(tb, "cube", np.float32)
