@@ -664,8 +664,18 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     for (int g = tid; g < NG; g += NT) gcount[g] = 0;
     __syncthreads();
 
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
-        const int b = blocklist[bi] - 1;
+    // interior block: its halo tile lies inside the mesh, so no window is truncated
+    auto interior_block = [&](int b) {
+        bool in = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const int o = (b % M.nb[d]) * BW - 1;
+            b /= M.nb[d];
+            in = in && o >= 0 && o + TS - 1 <= M.n[d] - 1;
+        }
+        return in;
+    };
+    auto process_block = [&](const int b) {
         int org[3] = {0, 0, 0};
         {
             int r = b;
@@ -674,12 +684,6 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                 org[d] = (r % M.nb[d]) * BW - 1;
                 r /= M.nb[d];
             }
-        }
-        if constexpr (MODE != 0) {
-            bool interior = true;
-#pragma unroll
-            for (int d = 0; d < D; ++d) interior = interior && org[d] >= 0 && org[d] + TS - 1 <= M.n[d] - 1;
-            if (interior != (MODE == 1)) continue;  // the other kernel's block (uniform over the CTA)
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
         for (int b0 = s0; b0 < s1; b0 += NR) {
@@ -955,6 +959,34 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                     if (val[1 + D + d] != 0.0) atomicAdd(G.f[d] + lin, T(val[1 + D + d]));
                 }
             }
+        }
+    };
+
+    if constexpr (MODE == 2) {
+        // The boundary blocks are few: each CTA tests NT block-list entries at
+        // once and keeps the boundary ones in a shared list, instead of one
+        // dependent load per skipped block.
+        __shared__ int blist[NT];
+        __shared__ int bcount;
+        for (int c0 = blockIdx.x * NT; c0 < nactive; c0 += gridDim.x * NT) {
+            if (tid == 0) bcount = 0;
+            __syncthreads();
+            if (c0 + tid < nactive) {
+                const int b = blocklist[c0 + tid] - 1;
+                if (!interior_block(b)) blist[atomicAdd(&bcount, 1)] = b;
+            }
+            __syncthreads();
+            const int nlist = bcount;
+            for (int q = 0; q < nlist; ++q) process_block(blist[q]);
+            __syncthreads();
+        }
+    } else {
+        for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+            const int b = blocklist[bi] - 1;
+            if constexpr (MODE == 1) {
+                if (!interior_block(b)) continue;  // the boundary kernel's block (uniform over the CTA)
+            }
+            process_block(b);
         }
     }
 }
