@@ -102,6 +102,8 @@ struct tb_ctx {
     // reverse mode: FP64 grid sensitivities (13 components x nnodes)
     double* adj_grid = nullptr;
     long long adj_grid_cap = 0;
+    double* adj_coef = nullptr;
+    long long adj_coef_cap = 0;
     // checkpoint tape: states at steps 0, K, 2K, ... and one segment of K states
     char* tape_cp = nullptr;
     long long tape_cp_cap = 0;
@@ -779,6 +781,10 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
     if ((rc = make_adjview(c, adj, D, P.n, A)) != TB_OK) return rc;
     if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
+    if (cudaError_t ce = grow(c->adj_coef, c->adj_coef_cap, std::max<long long>(1, P.n) * (2 * D + D * D));
+        ce != cudaSuccess)
+        return cuda_fail(c, ce, "cudaMalloc scatter coefficients");
+    GB.coef = c->adj_coef;
     if (!part || !part->blocklist || !part->offsets || (P.n && (!part->particleindices || !part->blockids)))
         return fail(c, TB_ERR_ARG, "partition array is NULL");
     const AdjPartition AP{totals, part->blocklist, part->offsets, part->particleindices, part->blockids};
@@ -1020,6 +1026,7 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->touched_cur);
     cudaFree(c->touched_prev);
     cudaFree(c->adj_grid);
+    cudaFree(c->adj_coef);
     cudaFree(c->tape_cp);
     cudaFree(c->tape_seg);
     cudaFree(c->ro_scratch);

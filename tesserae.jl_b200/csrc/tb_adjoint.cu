@@ -15,9 +15,11 @@
 // derivatives of the quadratic B-spline or uGIMP). The forward values (weights,
 // grid velocities) are read in the state type T; every adjoint quantity is FP64.
 // Both particle passes keep the (BW+3)^D halo tile of the block they work on
-// in shared memory, so the gathers stay on chip; the scatter of 1. uses global
-// FP64 atomics. G2P^T runs one CTA per block, P2G^T one CTA per chunk of 512
-// particles of the block-sorted permutation.
+// in shared memory, so the gathers stay on chip, and evaluate their sums over the
+// window as separable moments (one axis at a time). The scatter of 1. is a
+// separate pencil kernel with staged FP64 partials and one global atomic per
+// node and block. The gathers run one CTA per chunk of 512 particles of the
+// block-sorted permutation.
 #include "tb_launch.cuh"
 
 namespace tb {
@@ -66,31 +68,6 @@ __device__ __forceinline__ bool adj_axes(const DMesh<D, T>& M, const Scalars<T>&
         }
     }
     return true;
-}
-
-// w, grad w and the Hessian of w (with respect to x_p) at window slot idx.
-template <int D>
-__device__ __forceinline__ void adj_node(const AdjAxes<D>& A, const int (&idx)[3], double& w, double (&g)[3],
-                                         double (&H)[3][3]) {
-    w = 1.0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) w *= A.val[d][idx[d]];
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        double ga = A.der[a][idx[a]];
-#pragma unroll
-        for (int c = 0; c < D; ++c)
-            if (c != a) ga *= A.val[c][idx[c]];
-        g[a] = ga * A.hi;
-#pragma unroll
-        for (int b = 0; b < D; ++b) {
-            double h = (a == b) ? A.d2[a][idx[a]] : A.der[a][idx[a]] * A.der[b][idx[b]];
-#pragma unroll
-            for (int c = 0; c < D; ++c)
-                if (c != a && c != b) h *= A.val[c][idx[c]];
-            H[a][b] = h * A.hi * A.hi;
-        }
-    }
 }
 
 template <int D>
@@ -171,28 +148,110 @@ __device__ __forceinline__ int tile_slot(const int (&q0)[3], const int (&idx)[3]
                     : (q0[0] + idx[0]) + TS * (q0[1] + idx[1]);
 }
 
-// G2P backwards, one CTA per non-empty block: v and v - vn of the block's halo
-// tile in shared memory for the gathers; the v / vn sensitivities go straight to
-// the global FP64 grid with fire-and-forget atomics (an FP64 shared tile, where
-// all of a block's particles collide on a few hundred nodes, measured 3.7x
-// slower on the sphere scene). One CTA per block, not per chunk: chunks of one
-// crowded block on several SMs scatter to the same nodes at once (measured 1.5x
-// slower on the sphere scene).
+// Per-axis jets of one particle with the mesh scale folded in:
+// J[d][0][k] = N, J[d][1][k] = N' h_inv, J[d][2][k] = N'' h_inv^2 at window slot
+// k (zero past a truncated window and for d >= D).
+template <int D>
+__device__ __forceinline__ void axis_jets(const AdjAxes<D>& A, double (&J)[3][3][3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            J[d][0][k] = d < D ? A.val[d < D ? d : 0][k] : 0.0;
+            J[d][1][k] = d < D ? A.der[d < D ? d : 0][k] * A.hi : 0.0;
+            J[d][2][k] = d < D ? A.d2[d < D ? d : 0][k] * A.hi * A.hi : 0.0;
+        }
+}
+
+// Slot of d2w / dx_a dx_b in a moment vector (see window_moments).
+__host__ __device__ constexpr int hidx(int a, int b) {
+    return a == b ? 4 + a : (a + b == 1 ? 7 : (a + b == 2 ? 8 : 9));
+}
+
+// Moments of one tile field phi over a particle's window: m[0] = sum w phi,
+// m[1 + a] = sum (dw/dx_a) phi and, with ORD 2, m[hidx(a, b)] = sum
+// (d2w/dx_a dx_b) phi, summed over the 3^D window nodes. w is a product of axis
+// kernels, so the sums are contracted one axis at a time (x, then y, then z):
+// 3 multiply-adds per window row and derivative order in x, then a few per row
+// and plane, instead of forming w, grad w and the Hessian at every node.
+// `t0` is the tile index of window slot (0, 0, 0).
+template <int D, int ORD, int TS, class TT>
+__device__ __forceinline__ void window_moments(const TT* __restrict__ phi, int t0, const double (&J)[3][3][3],
+                                               double (&m)[10]) {
+#pragma unroll
+    for (int q = 0; q < 10; ++q) m[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < (D == 3 ? 3 : 1); ++k) {
+        double y00 = 0.0, y10 = 0.0, y01 = 0.0, y20 = 0.0, y02 = 0.0, y11 = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const TT* r = phi + t0 + TS * (j + TS * k);
+            const double f0 = double(r[0]), f1 = double(r[1]), f2 = double(r[2]);
+            const double x0 = J[0][0][0] * f0 + J[0][0][1] * f1 + J[0][0][2] * f2;
+            const double x1 = J[0][1][0] * f0 + J[0][1][1] * f1 + J[0][1][2] * f2;
+            y00 += J[1][0][j] * x0;
+            y10 += J[1][0][j] * x1;
+            y01 += J[1][1][j] * x0;
+            if constexpr (ORD == 2) {
+                const double x2 = J[0][2][0] * f0 + J[0][2][1] * f1 + J[0][2][2] * f2;
+                y20 += J[1][0][j] * x2;
+                y02 += J[1][2][j] * x0;
+                y11 += J[1][1][j] * x1;
+            }
+        }
+        if constexpr (D == 3) {
+            const double z0 = J[2][0][k], z1 = J[2][1][k];
+            m[0] += z0 * y00;
+            m[1] += z0 * y10;
+            m[2] += z0 * y01;
+            m[3] += z1 * y00;
+            if constexpr (ORD == 2) {
+                const double z2 = J[2][2][k];
+                m[hidx(0, 0)] += z0 * y20;
+                m[hidx(1, 1)] += z0 * y02;
+                m[hidx(2, 2)] += z2 * y00;
+                m[hidx(0, 1)] += z0 * y11;
+                m[hidx(0, 2)] += z1 * y10;
+                m[hidx(1, 2)] += z1 * y01;
+            }
+        } else {
+            m[0] = y00;
+            m[1] = y10;
+            m[2] = y01;
+            if constexpr (ORD == 2) {
+                m[hidx(0, 0)] = y20;
+                m[hidx(1, 1)] = y02;
+                m[hidx(0, 1)] = y11;
+            }
+        }
+    }
+}
+
+// G2P backwards, gather half, one CTA per chunk of the permutation: v and
+// v - vn of the block's halo tile in shared memory. Per particle it forms
+// L = sum v (x) grad w and the position sensitivity from window moments, writes
+// the particle sensitivities, and leaves the coefficients of its grid scatter
+//   v_bar_i += w a + Lb grad w,  vn_bar_i += w b
+// (a = v_bar_p (1 - alpha) + dt x_bar + alpha v_bar_p, b = -alpha v_bar_p,
+// Lb = dt F_bar F^T) at its permutation slot for adj_scatter_kernel.
 template <int D, class T, int BW>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
-                                                              AdjView A, GradGrid GB,
+                                                              AdjView A, double* __restrict__ coef,
                                                               const int* __restrict__ totals,
-                                                              const int* __restrict__ blocklist,
+                                                              const int* __restrict__ blockids,
                                                               const int* __restrict__ offsets,
                                                               const int* __restrict__ perm, int* err) {
     constexpr int TS = BW + 3, TN = (D == 3) ? TS * TS * TS : TS * TS;
-    __shared__ T tin[2 * D * TN];         // v_r at [r TN + t], (v - vn)_r at [(D + r) TN + t]
+    __shared__ T tin[2 * D * TN];  // v_r at [r TN + t], (v - vn)_r at [(D + r) TN + t]
     const double dt = s.dt64, alpha = double(s.alpha);
-    const int nactive = totals[0], tid = threadIdx.x;
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
-      {
-        const int b = blocklist[bi] - 1;
-        const int s0 = offsets[b], s1 = offsets[b + 1];
+    const long long n = P.n;
+    const int nassigned = totals[1], tid = threadIdx.x;
+    const int nchunks = (nassigned + ADJ_CHUNK - 1) / ADJ_CHUNK;
+    for (int ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
+      const int c1 = min((ci + 1) * ADJ_CHUNK, nassigned);
+      for (int c0 = ci * ADJ_CHUNK; c0 < c1;) {
+        const int b = blockids[perm[c0] - 1] - 1;
+        const int s0 = c0, s1 = min(offsets[b + 1], c1);
         int org[3];
         block_origin<D, T, BW>(M, b, org);
         for (int t = tid; t < TN; t += ADJ_THREADS) {
@@ -226,42 +285,15 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
                 xb[d] = A.x[d][p];
                 vbp[d] = A.v[d][p];
             }
-            AdjAxes<D> ax;
-            int q0[3];
-            const bool in = adj_axes<D, T>(M, s, x, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err);
-            double L[3][3] = {};
-            if (in) {
-#pragma unroll
-                for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
-#pragma unroll
-                    for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const int idx[3] = {i, jj, k};
-                            if (i >= ax.cnt[0] || jj >= ax.cnt[1] || (D == 3 && k >= ax.cnt[D - 1])) continue;
-                            double w, g[3], H[3][3];
-                            adj_node<D>(ax, idx, w, g, H);
-                            const int t = tile_slot<D, TS>(q0, idx);
-#pragma unroll
-                            for (int r = 0; r < D; ++r) {
-                                const double vi = double(tin[r * TN + t]);
-#pragma unroll
-                                for (int c = 0; c < D; ++c) L[r][c] += vi * g[c];
-                            }
-                        }
-            }
-            double Lb[3][3] = {}, Fbn[3][3] = {};
+            // Lb = dt F_bar F^T does not depend on L
+            double Lb[3][3] = {};
 #pragma unroll
             for (int r = 0; r < D; ++r)
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
-                    double s1v = 0.0, s2v = 0.0;
+                    double s2v = 0.0;
 #pragma unroll
-                    for (int k = 0; k < D; ++k) {
-                        s1v += ((r == k ? 1.0 : 0.0) + dt * L[k][r]) * Fb[k][c];
-                        s2v += Fb[r][k] * F[c][k];
-                    }
-                    Fbn[r][c] = s1v;
+                    for (int k = 0; k < D; ++k) s2v += Fb[r][k] * F[c][k];
                     Lb[r][c] = dt * s2v;
                 }
             double dvb[3] = {0, 0, 0}, vpb[3] = {0, 0, 0};
@@ -270,45 +302,44 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
                 dvb[d] = alpha * vbp[d];
                 vpb[d] = (1.0 - alpha) * vbp[d] + dt * xb[d];
             }
+            AdjAxes<D> ax;
+            int q0[3];
+            const bool in = adj_axes<D, T>(M, s, x, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err);
+            double L[3][3] = {};
             if (in) {
-                long long gbase = 0;
+                double J[3][3][3];
+                axis_jets<D>(ax, J);
+                const int zero[3] = {0, 0, 0};
+                const int t0 = tile_slot<D, TS>(q0, zero);
+                // x_bar += sum_i (vpb . v_i + dvb . dv_i) grad w + H (Lb^T v_i)
 #pragma unroll
-                for (int d = D - 1; d >= 0; --d) gbase = gbase * M.n[d] + ax.lo[d];
+                for (int r = 0; r < D; ++r) {
+                    double mo[10];
+                    window_moments<D, 2, TS>(tin + r * TN, t0, J, mo);
 #pragma unroll
-                for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+                    for (int c = 0; c < D; ++c) L[r][c] = mo[1 + c];
 #pragma unroll
-                    for (int jj = 0; jj < 3; ++jj)
+                    for (int bb = 0; bb < D; ++bb) {
+                        double h = 0.0;
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const int idx[3] = {i, jj, k};
-                            if (i >= ax.cnt[0] || jj >= ax.cnt[1] || (D == 3 && k >= ax.cnt[D - 1])) continue;
-                            double w, g[3], H[3][3];
-                            adj_node<D>(ax, idx, w, g, H);
-                            const int t = tile_slot<D, TS>(q0, idx);
-                            const long long I = gbase + i + (long long)M.n[0] * (jj + (D == 3 ? (long long)M.n[1] * k : 0));
-                            double gb[3] = {0, 0, 0}, wb = 0.0;
+                        for (int c = 0; c < D; ++c) h += Lb[r][c] * mo[hidx(bb, c)];
+                        xb[bb] += vpb[r] * mo[1 + bb] + h;
+                    }
+                    window_moments<D, 1, TS>(tin + (D + r) * TN, t0, J, mo);
 #pragma unroll
-                            for (int r = 0; r < D; ++r) {
-                                const double vi = double(tin[r * TN + t]), dvi = double(tin[(D + r) * TN + t]);
-                                double lg = 0.0;
-#pragma unroll
-                                for (int c = 0; c < D; ++c) {
-                                    lg += Lb[r][c] * g[c];
-                                    gb[c] += Lb[r][c] * vi;
-                                }
-                                atomicAdd(GB.vb[r] + I, w * (vpb[r] + dvb[r]) + lg);
-                                atomicAdd(GB.vnb[r] + I, -w * dvb[r]);
-                                wb += vpb[r] * vi + dvb[r] * dvi;
-                            }
-#pragma unroll
-                            for (int bb = 0; bb < D; ++bb) {
-                                double h = 0.0;
-#pragma unroll
-                                for (int c = 0; c < D; ++c) h += H[bb][c] * gb[c];
-                                xb[bb] += wb * g[bb] + h;
-                            }
-                        }
+                    for (int bb = 0; bb < D; ++bb) xb[bb] += dvb[r] * mo[1 + bb];
+                }
             }
+            double Fbn[3][3] = {};
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    double s1v = 0.0;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) s1v += ((r == k ? 1.0 : 0.0) + dt * L[k][r]) * Fb[k][c];
+                    Fbn[r][c] = s1v;
+                }
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 A.x[d][p] = xb[d];
@@ -318,9 +349,274 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
             for (int r = 0; r < D; ++r)
 #pragma unroll
                 for (int c = 0; c < D; ++c) A.F[r + c * D][p] = Fbn[r][c];
+            double* q = coef + j;
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                q[r * n] = in ? vpb[r] + dvb[r] : 0.0;
+                q[(D + r) * n] = in ? -dvb[r] : 0.0;
+#pragma unroll
+                for (int c = 0; c < D; ++c) q[(2 * D + r * D + c) * n] = in ? Lb[r][c] : 0.0;
+            }
         }
         __syncthreads();
+        c0 = s1;
       }
+    }
+}
+
+// G2P backwards, scatter half: v_bar_i += w a + Lb grad w and vn_bar_i += w b
+// from the coefficients adj_g2p_kernel left per permutation slot. The forward
+// P2G's pencil sweep, in FP64, with the accumulators kept in registers across
+// the batches of a block: per batch of up to SC_NR particles of one block the
+// records are counting-sorted by window start (group); the lane of window row
+// (y, z) of pencil (gy, gz) keeps the row's TS x-nodes in registers and adds
+// every particle of the pencil's groups to the 3 of them its window covers.
+// When the CTA moves to another block, the lanes store their rows to a staging
+// array and one thread per tile node sums the at most 3^(D-1) rows that reach
+// it and adds them to the grid with one global FP64 atomic per non-zero value
+// (no shared atomics). A CTA takes a contiguous range of the permutation, so
+// all batches of a crowded block share one flush.
+constexpr int SC_THREADS = 288;
+constexpr int SC_NR = 768;  // 3 particles per thread in the record pass
+// Record (doubles): [0..2] a [3..5] b [6..14] Lb (r 3 + c) [16..21] x jets
+// (value, h_inv-scaled derivative per slot) [22..27] y jets [28..33] z jets.
+// 34 doubles = 17 x 16 bytes.
+constexpr int SC_RS = 34;
+
+template <int D, int BW>
+struct ScShape {
+    static constexpr int TS = BW + 3;
+    static constexpr int TN = (D == 3) ? TS * TS * TS : TS * TS;
+    static constexpr int NC = 2 * D;
+    static constexpr int G1 = BW + 1;
+    static constexpr int NG = (D == 3) ? G1 * G1 * G1 : G1 * G1;
+    static constexpr int NJK = (D == 3) ? 9 : 3;
+    static constexpr int NSUB = 32 / NJK;
+    static constexpr int NPENCIL = NG / G1;
+    static constexpr int CSTR = NPENCIL * NJK * TS;
+    static constexpr int NPART = NC * CSTR;
+    // records and staging share one region (never live at once)
+    static constexpr int NDBL = (SC_NR * SC_RS > NPART) ? SC_NR * SC_RS : NPART;
+};
+
+template <int D, class T, int BW>
+__global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s,
+                                                                     const double* __restrict__ coef, GradGrid GB,
+                                                                     const int* __restrict__ totals,
+                                                                     const int* __restrict__ blockids,
+                                                                     const int* __restrict__ offsets,
+                                                                     const int* __restrict__ perm, long long per_cta,
+                                                                     int* err) {
+    using SH = ScShape<D, BW>;
+    constexpr int NT = SC_THREADS, NW = NT / 32;
+    constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
+    constexpr int NJK = SH::NJK, NSUB = SH::NSUB, NPENCIL = SH::NPENCIL, CSTR = SH::CSTR;
+    static_assert((NPENCIL + NSUB - 1) / NSUB <= NW, "one pencil per lane");
+    constexpr int ITEMS = (SC_NR + NT - 1) / NT;
+    extern __shared__ __align__(16) double sc_smem[];
+    double* rec = sc_smem;   // batch records, at the thread's slot
+    double* part = sc_smem;  // staged rows at a flush
+    int* gcount = reinterpret_cast<int*>(sc_smem + SH::NDBL);
+    int* gstart = gcount + NG;
+    int* order = gstart + NG + 1;  // record of the q-th particle in group order
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int jk = lane % NJK, sub = lane / NJK;
+    const int sj = jk % 3, sk = (D == 3) ? jk / 3 : 0;
+    const int pc = warp * NSUB + sub;  // this lane's pencil (gy + G1 gz)
+    const bool live = sub < NSUB && pc < NPENCIL;
+    const long long n = P.n;
+    const double hi = double(M.h_inv);
+    const int nassigned = totals[1];
+    for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+    double acc[TS][NC];
+#pragma unroll
+    for (int x = 0; x < TS; ++x)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[x][c] = 0.0;
+    __syncthreads();
+
+    const long long lo_r = min((long long)blockIdx.x * per_cta, (long long)nassigned);
+    const int r0 = int(lo_r), r1 = int(min(lo_r + per_cta, (long long)nassigned));
+    int c0 = r0;
+    int b = c0 < r1 ? blockids[perm[c0] - 1] - 1 : -1;
+    while (c0 < r1) {
+        int org[3];
+        block_origin<D, T, BW>(M, b, org);
+        const int c1 = min(min(offsets[b + 1], r1), c0 + SC_NR);
+        // the next batch's block, loaded early (uniform over the CTA)
+        const int nb_next = c1 < r1 ? blockids[perm[c1] - 1] - 1 : -1;
+        // ---- 1a. particles tid, tid + NT, ...: window start -> group and rank in
+        //      the group; the record goes to the particle's own slot. Every
+        //      global load of the batch is issued before the first use.
+        int grp[ITEMS], rank[ITEMS];
+        long long pid[ITEMS];
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u) {
+            grp[u] = -1;
+            rank[u] = 0;
+            pid[u] = tid + u * NT < c1 - c0 ? perm[c0 + tid + u * NT] - 1 : -1;
+        }
+        T px[ITEMS][3], pl[ITEMS];
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u) {
+            const long long p = pid[u] >= 0 ? pid[u] : 0;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) px[u][d] = (pid[u] >= 0 && d < D) ? P.x[d < D ? d : 0][p] : T(0);
+            pl[u] = (pid[u] >= 0 && P.l) ? P.l[p] : s.gimp_l;
+        }
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u) {
+            if (pid[u] < 0) continue;
+            const int slot = tid + u * NT;
+            const int j = c0 + slot;
+            Basis<D, T> B;
+            if (prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err)) {
+                int gi = 0;
+                bool ok = true;
+#pragma unroll
+                for (int d = D - 1; d >= 0; --d) {
+                    const int q = B.ax[d].lo - org[d];
+                    ok = ok && q >= 0 && q < G1;
+                    gi = gi * G1 + q;
+                }
+                if (ok) {  // (a window outside the tile is reported by the gather kernel)
+                    grp[u] = gi;
+                    rank[u] = atomicAdd(&gcount[gi], 1);
+                    double* r = rec + slot * SC_RS;
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr) {
+                        r[rr] = coef[rr * n + j];
+                        r[3 + rr] = coef[(D + rr) * n + j];
+#pragma unroll
+                        for (int c = 0; c < D; ++c) r[6 + 3 * rr + c] = coef[(2 * D + rr * D + c) * n + j];
+                    }
+#pragma unroll
+                    for (int d = 0; d < D; ++d)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            r[16 + 6 * d + 2 * k] = double(B.ax[d].val[k]);
+                            r[17 + 6 * d + 2 * k] = double(B.ax[d].der[k]) * hi;
+                        }
+                }
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            int carry = 0;
+            for (int g0 = 0; g0 < NG; g0 += 32) {
+                const int g = g0 + lane;
+                const int c = g < NG ? gcount[g] : 0;
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (g < NG) gstart[g] = carry + incl - c;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) gstart[NG] = carry;
+        }
+        __syncthreads();
+        // ---- 1b. group order
+        for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u)
+            if (grp[u] >= 0) order[gstart[grp[u]] + rank[u]] = tid + u * NT;
+        __syncthreads();
+        // ---- 2. the lane's pencil: groups in x order, 3 register nodes each
+        if (live) {
+#pragma unroll
+            for (int gx = 0; gx < G1; ++gx) {
+                const int qe = gstart[G1 * pc + gx + 1];
+                for (int q = gstart[G1 * pc + gx]; q < qe; ++q) {
+                    const double* r = rec + order[q] * SC_RS;
+                    const double2 yj = *reinterpret_cast<const double2*>(r + 22 + 2 * sj);
+                    double wyz, dyz, wdz = 0.0;
+                    if constexpr (D == 3) {
+                        const double2 zk = *reinterpret_cast<const double2*>(r + 28 + 2 * sk);
+                        wyz = yj.x * zk.x;
+                        dyz = yj.y * zk.x;
+                        wdz = yj.x * zk.y;
+                    } else {
+                        wyz = yj.x;
+                        dyz = yj.y;
+                    }
+                    // per component: w a + Lb grad w = wx (a wyz + Lb1 dyz + Lb2 wdz) + dx Lb0 wyz
+                    double AQ[3], Pc[3], Bv[3];
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr) {
+                        double q2 = r[6 + 3 * rr + 1] * dyz;
+                        if constexpr (D == 3) q2 += r[6 + 3 * rr + 2] * wdz;
+                        AQ[rr] = r[rr] * wyz + q2;
+                        Pc[rr] = r[6 + 3 * rr] * wyz;
+                        Bv[rr] = r[3 + rr] * wyz;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const double2 xj = *reinterpret_cast<const double2*>(r + 16 + 2 * i);
+#pragma unroll
+                        for (int rr = 0; rr < D; ++rr) {
+                            acc[gx + i][rr] += xj.x * AQ[rr] + xj.y * Pc[rr];
+                            acc[gx + i][D + rr] += xj.x * Bv[rr];
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        c0 = c1;
+        if (nb_next != b) {
+            // ---- 3. flush the block: rows to the staging array, then per tile
+            //      node the staged rows, one global atomic per non-zero value
+            if (live) {
+                const int pbase = (jk * NPENCIL + pc) * TS;
+#pragma unroll
+                for (int x = 0; x < TS; ++x)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        part[pbase + x + c * CSTR] = acc[x][c];
+                        acc[x][c] = 0.0;
+                    }
+            }
+            __syncthreads();
+            for (int t = tid; t < TN; t += NT) {
+                int node[3] = {0, 0, 0}, tn[3] = {0, 0, 0}, rem = t;
+                bool inside = true;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    tn[d] = rem % TS;
+                    rem /= TS;
+                    node[d] = org[d] + tn[d];
+                    inside = inside && node[d] >= 0 && node[d] < M.n[d];
+                }
+                if (!inside) continue;
+                double val[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) val[c] = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < (D == 3 ? 3 : 1); ++kk)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const int gy = tn[1] - jj, gz = (D == 3) ? tn[2] - kk : 0;
+                        if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
+                        const int idx = ((jj + 3 * kk) * NPENCIL + gy + G1 * gz) * TS + tn[0];
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
+                    }
+                long long lin = 0;
+#pragma unroll
+                for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + node[d];
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    if (val[r] != 0.0) atomicAdd(GB.vb[r] + lin, val[r]);
+                    if (val[D + r] != 0.0) atomicAdd(GB.vnb[r] + lin, val[D + r]);
+                }
+            }
+            __syncthreads();
+        }
+        b = nb_next;
     }
 }
 
@@ -368,12 +664,14 @@ __global__ void __launch_bounds__(256) adj_grid_kernel(DMesh<D, T> M, GView<T> G
     }
 }
 
-// P2G backwards, one CTA per chunk of the permutation: the block's halo tile of
-// (m_bar, mv_bar, f_bar) in shared memory, gathered per particle, then the
-// constitutive adjoint in FP64.
+// P2G backwards, gather half, one CTA per chunk of the permutation: the
+// block's halo tile of (m_bar, mv_bar, f_bar) in shared memory, gathered per
+// particle as window moments into x_bar and v_bar; sigma_bar (D^2) and V_bar go
+// to the scratch at the particle's index for adj_material_kernel.
 template <int D, class T, int BW>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s, AdjView A,
-                                                              GradGrid GB, const int* __restrict__ totals,
+                                                              GradGrid GB, double* __restrict__ sbar,
+                                                              const int* __restrict__ totals,
                                                               const int* __restrict__ blockids,
                                                               const int* __restrict__ offsets,
                                                               const int* __restrict__ perm, int* err) {
@@ -422,104 +720,126 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PVi
                 for (int r = 0; r < D; ++r)
 #pragma unroll
                     for (int c = 0; c < D; ++c) sig[r][c] = double(P.sig[symidx<D>(r, c)][p]);
+                // Window moments of each grid sensitivity field:
+                //   x_bar += m_p sum (m_bar + v . mv_bar + g . f_bar) grad w
+                //            - V_p H sigma f_bar,
+                //   v_bar += m_p sum w mv_bar,  sigma_bar = -V_p sum f_bar (x) grad w,
+                //   V_bar = -sum f_bar . sigma grad w.
+                double J[3][3][3];
+                axis_jets<D>(ax, J);
+                const int zero[3] = {0, 0, 0};
+                const int t0 = tile_slot<D, TS>(q0, zero);
+                double mo[10];
+                window_moments<D, 1, TS>(tg, t0, J, mo);
 #pragma unroll
-                for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+                for (int bb = 0; bb < D; ++bb) xb[bb] += mp * mo[1 + bb];
 #pragma unroll
-                    for (int jj = 0; jj < 3; ++jj)
+                for (int d = 0; d < D; ++d) {
+                    window_moments<D, 1, TS>(tg + (1 + d) * TN, t0, J, mo);
+                    vb[d] += mp * mo[0];
 #pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const int idx[3] = {i, jj, k};
-                            if (i >= ax.cnt[0] || jj >= ax.cnt[1] || (D == 3 && k >= ax.cnt[D - 1])) continue;
-                            double w, g[3], H[3][3];
-                            adj_node<D>(ax, idx, w, g, H);
-                            const int t = tile_slot<D, TS>(q0, idx);
-                            double wb = mp * tg[t];
-                            double gb[3] = {0, 0, 0}, fbv[3] = {0, 0, 0};
+                    for (int bb = 0; bb < D; ++bb) xb[bb] += mp * vp[d] * mo[1 + bb];
+                }
 #pragma unroll
-                            for (int d = 0; d < D; ++d) {
-                                const double pbd = tg[(1 + d) * TN + t];
-                                fbv[d] = tg[(1 + D + d) * TN + t];
-                                wb += mp * (vp[d] * pbd + grav[d] * fbv[d]);
-                                vb[d] += mp * w * pbd;
-                            }
-#pragma unroll
-                            for (int r = 0; r < D; ++r) {
-                                double sg = 0.0;
-#pragma unroll
-                                for (int c = 0; c < D; ++c) {
-                                    sg += sig[r][c] * g[c];
-                                    gb[c] += -Vp * sig[r][c] * fbv[r];
-                                    sb[r][c] += -Vp * fbv[r] * g[c];
-                                }
-                                Vb += -fbv[r] * sg;
-                            }
-#pragma unroll
-                            for (int bb = 0; bb < D; ++bb) {
-                                double h = 0.0;
-#pragma unroll
-                                for (int c = 0; c < D; ++c) h += H[bb][c] * gb[c];
-                                xb[bb] += wb * g[bb] + h;
-                            }
-                        }
-            }
-            // sigma(F) and V = V0 det F backwards (FP64)
-            double F[3][3] = {}, C[3][3] = {};
-            load_F<D, T>(P, p, F);
-            const double J = det_cof<D>(F, C);
-            const double mu = P.mu ? double(P.mu[p]) : s.mu;
-            const double lam = P.lam ? double(P.lam[p]) : s.lam;
-            const double V0 = P.V0 ? double(P.V0[p]) : s.V0_64;
-            double Jb = V0 * Vb, mub = 0.0, lamb = 0.0;
-            double Fb[3][3] = {};
-            if (s.material == 1) {
-                double tr = 0.0;
-#pragma unroll
-                for (int d = 0; d < D; ++d) tr += sb[d][d];
-                lamb = (J - 1.0) * tr;
-                Jb += lam * tr;
-            } else {
-                const double lj = log(J), iJ = 1.0 / J;
-                double st = 0.0, trt = 0.0;
-#pragma unroll
-                for (int r = 0; r < D; ++r)
+                for (int r = 0; r < D; ++r) {
+                    window_moments<D, 2, TS>(tg + (1 + D + r) * TN, t0, J, mo);
 #pragma unroll
                     for (int c = 0; c < D; ++c) {
-                        double bsum = 0.0;
-#pragma unroll
-                        for (int k = 0; k < D; ++k) bsum += F[r][k] * F[c][k];
-                        const double bm = bsum - (r == c ? 1.0 : 0.0);
-                        st += sb[r][c] * (mu * bm + (r == c ? lam * lj : 0.0));
-                        mub += sb[r][c] * iJ * bm;
+                        sb[r][c] += -Vp * mo[1 + c];
+                        Vb += -sig[r][c] * mo[1 + c];
                     }
 #pragma unroll
-                for (int d = 0; d < D; ++d) trt += sb[d][d] * iJ;
-                Jb += -st * iJ * iJ + lam * trt * iJ;
-                lamb = lj * trt;
+                    for (int bb = 0; bb < D; ++bb) {
+                        double h = 0.0;
 #pragma unroll
-                for (int r = 0; r < D; ++r)
-#pragma unroll
-                    for (int c = 0; c < D; ++c) {
-                        double a = 0.0;
-#pragma unroll
-                        for (int k = 0; k < D; ++k) a += (sb[r][k] + sb[k][r]) * F[k][c];
-                        Fb[r][c] = mu * iJ * a;
+                        for (int c = 0; c < D; ++c) h += sig[r][c] * mo[hidx(bb, c)];
+                        xb[bb] += mp * grav[r] * mo[1 + bb] - Vp * h;
                     }
+                }
             }
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 A.x[d][p] += xb[d];
                 A.v[d][p] += vb[d];
             }
+            const long long n = P.n;
 #pragma unroll
             for (int r = 0; r < D; ++r)
 #pragma unroll
-                for (int c = 0; c < D; ++c) A.F[r + c * D][p] += Fb[r][c] + Jb * C[r][c];
-            if (A.mu) A.mu[p] += mub;
-            if (A.lam) A.lam[p] += lamb;
+                for (int c = 0; c < D; ++c) sbar[(r * D + c) * n + p] = sb[r][c];
+            sbar[D * D * n + p] = Vb;
         }
         __syncthreads();
         c0 = s1;
       }
+    }
+}
+
+// sigma(F) and V = V0 det F backwards (FP64), one thread per particle in memory
+// order (particles outside the mesh, block 0, have no P2G part): sigma_bar and
+// V_bar from adj_p2g_kernel into F_bar and the Lame sensitivities.
+template <int D, class T>
+__global__ void __launch_bounds__(256) adj_material_kernel(PView<T> P, Scalars<T> s, AdjView A,
+                                                           const double* __restrict__ sbar,
+                                                           const int* __restrict__ blockids) {
+    const long long n = P.n;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        if (blockids[p] == 0) continue;
+        double sb[3][3] = {};
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) sb[r][c] = sbar[(r * D + c) * n + p];
+        const double Vb = sbar[D * D * n + p];
+        double F[3][3] = {}, C[3][3] = {};
+        load_F<D, T>(P, p, F);
+        const double J = det_cof<D>(F, C);
+        const double mu = P.mu ? double(P.mu[p]) : s.mu;
+        const double lam = P.lam ? double(P.lam[p]) : s.lam;
+        const double V0 = P.V0 ? double(P.V0[p]) : s.V0_64;
+        double Jb = V0 * Vb, mub = 0.0, lamb = 0.0;
+        double Fb[3][3] = {};
+        if (s.material == 1) {
+            double tr = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) tr += sb[d][d];
+            lamb = (J - 1.0) * tr;
+            Jb += lam * tr;
+        } else {
+            const double lj = log(J), iJ = 1.0 / J;
+            double st = 0.0, trt = 0.0;
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    double bsum = 0.0;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) bsum += F[r][k] * F[c][k];
+                    const double bm = bsum - (r == c ? 1.0 : 0.0);
+                    st += sb[r][c] * (mu * bm + (r == c ? lam * lj : 0.0));
+                    mub += sb[r][c] * iJ * bm;
+                }
+#pragma unroll
+            for (int d = 0; d < D; ++d) trt += sb[d][d] * iJ;
+            Jb += -st * iJ * iJ + lam * trt * iJ;
+            lamb = lj * trt;
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) a += (sb[r][k] + sb[k][r]) * F[k][c];
+                    Fb[r][c] = mu * iJ * a;
+                }
+        }
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) A.F[r + c * D][p] += Fb[r][c] + Jb * C[r][c];
+        if (A.mu) A.mu[p] += mub;
+        if (A.lam) A.lam[p] += lamb;
     }
 }
 
@@ -534,16 +854,35 @@ cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<
         if (e == cudaSuccess) e = cudaMemsetAsync(GB.vnb[d], 0, sizeof(double) * size_t(M.nnodes), cfg.stream);
     }
     if (e != cudaSuccess) return e;
-    const int bgrid = std::max(1, std::min(M.nblocks, cfg.num_sms * 8));
     const int cgrid = int(std::max<long long>(1, std::min<long long>((P.n + ADJ_CHUNK - 1) / ADJ_CHUNK,
                                                                      (long long)cfg.num_sms * 8)));
     const int ngrid = int(std::max<long long>(1, std::min<long long>((M.nnodes + 255) / 256, (long long)cfg.num_sms * 8)));
     if (P.n > 0) {
-        KernelScope ks(cfg, "adj_g2p");
-        adj_g2p_kernel<D, T, BW><<<bgrid, ADJ_THREADS, 0, cfg.stream>>>(M, G, P, s, A, GB, part.totals, part.blocklist,
-                                                                       part.offsets, part.perm, cfg.err);
-        ++*cfg.launches;
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        {
+            KernelScope ks(cfg, "adj_g2p");
+            adj_g2p_kernel<D, T, BW><<<cgrid, ADJ_THREADS, 0, cfg.stream>>>(M, G, P, s, A, GB.coef, part.totals,
+                                                                           part.blockids, part.offsets, part.perm,
+                                                                           cfg.err);
+            ++*cfg.launches;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        {
+            using SH = ScShape<D, BW>;
+            auto kern = adj_scatter_kernel<D, T, BW>;
+            const size_t smem = sizeof(double) * size_t(SH::NDBL) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + SC_NR);
+            if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
+                return e;
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SC_THREADS, smem);
+            const long long nbatch = (P.n + SC_NR - 1) / SC_NR;
+            const int sgrid = int(std::max<long long>(1, std::min<long long>(nbatch, (long long)cfg.num_sms * std::max(per_sm, 1))));
+            const long long per_cta = ((nbatch + sgrid - 1) / sgrid) * SC_NR;
+            KernelScope ks(cfg, "adj_scatter");
+            kern<<<sgrid, SC_THREADS, smem, cfg.stream>>>(M, P, s, GB.coef, GB, part.totals, part.blockids, part.offsets,
+                                                          part.perm, per_cta, cfg.err);
+            ++*cfg.launches;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         if (s.alpha != T(1)) {
             const int pgrid = int(std::max<long long>(1, std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8)));
             KernelScope ks2(cfg, "adj_outside");
@@ -559,9 +898,17 @@ cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (P.n > 0) {
-        KernelScope ks(cfg, "adj_p2g");
-        adj_p2g_kernel<D, T, BW><<<cgrid, ADJ_THREADS, 0, cfg.stream>>>(M, P, s, A, GB, part.totals, part.blockids,
-                                                                       part.offsets, part.perm, cfg.err);
+        {
+            KernelScope ks(cfg, "adj_p2g");
+            adj_p2g_kernel<D, T, BW><<<cgrid, ADJ_THREADS, 0, cfg.stream>>>(M, P, s, A, GB, GB.coef, part.totals,
+                                                                           part.blockids, part.offsets, part.perm,
+                                                                           cfg.err);
+            ++*cfg.launches;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        const int pgrid = int(std::max<long long>(1, std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8)));
+        KernelScope ks(cfg, "adj_material");
+        adj_material_kernel<D, T><<<pgrid, 256, 0, cfg.stream>>>(P, s, A, GB.coef, part.blockids);
         ++*cfg.launches;
         e = cudaGetLastError();
     }

@@ -111,6 +111,7 @@ struct GradGrid {
     double* mb;      // d loss / d m_i
     double* pb[3];   // d loss / d mv_i
     double* fb[3];   // d loss / d f_i
+    double* coef;    // per permutation slot: G2P backwards' scatter coefficients (2 D + D^2 arrays of n)
 };
 
 // The partition of the step being reversed (device arrays).
