@@ -265,8 +265,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
             }
         }
         __syncthreads();
+        int pnext = s0 + tid < s1 ? perm[s0 + tid] : 1;
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
-            const long long p = perm[j] - 1;
+            const long long p = pnext - 1;
+            if (j + ADJ_THREADS < s1) pnext = perm[j + ADJ_THREADS];
             T x[3] = {T(0), T(0), T(0)};
 #pragma unroll
             for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
@@ -465,11 +467,25 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
             for (int d = 0; d < 3; ++d) px[u][d] = (pid[u] >= 0 && d < D) ? P.x[d < D ? d : 0][p] : T(0);
             pl[u] = (pid[u] >= 0 && P.l) ? P.l[p] : s.gimp_l;
         }
+        // the coefficients go to the record slot at once (used only if the
+        // window lands in the tile)
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u) {
+            if (pid[u] < 0) continue;
+            const int j = c0 + tid + u * NT;
+            double* r = rec + (tid + u * NT) * SC_RS;
+#pragma unroll
+            for (int rr = 0; rr < D; ++rr) {
+                r[rr] = coef[rr * n + j];
+                r[3 + rr] = coef[(D + rr) * n + j];
+#pragma unroll
+                for (int c = 0; c < D; ++c) r[6 + 3 * rr + c] = coef[(2 * D + rr * D + c) * n + j];
+            }
+        }
 #pragma unroll
         for (int u = 0; u < ITEMS; ++u) {
             if (pid[u] < 0) continue;
             const int slot = tid + u * NT;
-            const int j = c0 + slot;
             Basis<D, T> B;
             if (prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err)) {
                 int gi = 0;
@@ -484,13 +500,6 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
                     grp[u] = gi;
                     rank[u] = atomicAdd(&gcount[gi], 1);
                     double* r = rec + slot * SC_RS;
-#pragma unroll
-                    for (int rr = 0; rr < D; ++rr) {
-                        r[rr] = coef[rr * n + j];
-                        r[3 + rr] = coef[(D + rr) * n + j];
-#pragma unroll
-                        for (int c = 0; c < D; ++c) r[6 + 3 * rr + c] = coef[(2 * D + rr * D + c) * n + j];
-                    }
 #pragma unroll
                     for (int d = 0; d < D; ++d)
 #pragma unroll
@@ -699,8 +708,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PVi
             }
         }
         __syncthreads();
+        int pnext = s0 + tid < s1 ? perm[s0 + tid] : 1;
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
-            const long long p = perm[j] - 1;
+            const long long p = pnext - 1;
+            if (j + ADJ_THREADS < s1) pnext = perm[j + ADJ_THREADS];
             T x[3] = {T(0), T(0), T(0)};
 #pragma unroll
             for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
