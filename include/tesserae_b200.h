@@ -66,7 +66,18 @@ enum tb_basis_kind {
     TB_BSPLINE_QUADRATIC = 0,     /* BSpline(Quadratic()) */
     TB_UGIMP = 1,                 /* uGIMP() */
     TB_WLS_BSPLINE_QUADRATIC = 2, /* WLS(BSpline(Quadratic())), MLS-MPM */
-    TB_WLS_UGIMP = 3              /* WLS(uGIMP()) */
+    TB_WLS_UGIMP = 3,             /* WLS(uGIMP()) */
+    TB_KC_BSPLINE_QUADRATIC = 4,  /* KernelCorrection(BSpline(Quadratic())) (src/Basis/kernelcorrection.jl) */
+    TB_KC_UGIMP = 5               /* KernelCorrection(uGIMP()) */
+};
+
+/* Constitutive models of the recognised G2P equation sets (tb_step_params.material). */
+enum tb_material_kind {
+    TB_MATERIAL_NEOHOOKEAN = 0, /* README.md:85: sigma = (mu (F F^T - I) + lambda log J I) / J, V = V0 det F */
+    TB_MATERIAL_FLUID = 1,      /* weakly compressible fluid p = -K (J - 1), K = lambda, V = V0 det F */
+    TB_MATERIAL_VONMISES = 2    /* docs/src/gpu.md:202-392 (Taylor impact): Hencky elasticity, von Mises
+                                   yield with linear hardening, return map in principal logarithmic
+                                   stretches; V = det(dF) V */
 };
 
 /* Transfer schemes of the recognised @P2G/@G2P equation sets. */
@@ -92,6 +103,8 @@ typedef struct tb_particles {
     void* V0;         /* optional per-particle initial volume */
     void* mu;         /* optional per-particle Lame mu */
     void* lambda;     /* optional per-particle Lame lambda */
+    void* eps_p;      /* equivalent plastic strain (TB_MATERIAL_VONMISES only) */
+    void* Cp_inv[6];  /* inverse plastic right Cauchy-Green tensor, symmetric (TB_MATERIAL_VONMISES only) */
 } tb_particles;
 
 /* Grid fields as SoA component pointers (scalar type T), each of length
@@ -138,10 +151,12 @@ typedef struct tb_step_params {
     double flip_alpha;  /* FLIP blend: v_p = sum w ((1-a) v_i + a (v_p + v_i - vn_i)); 1 = README FLIP */
     int32_t basis;      /* enum tb_basis_kind */
     int32_t transfer;   /* enum tb_transfer_kind */
-    int32_t material;   /* 0 = Neo-Hookean (README.md:85), 1 = weakly compressible fluid p = -K(J-1) with K = lambda */
+    int32_t material;   /* enum tb_material_kind */
     int32_t wall_mask;  /* slip walls: bit 2d = low face of axis d, bit 2d+1 = high face */
     int32_t wall_layers;/* node layers next to each walled face whose normal velocity is zeroed */
     int32_t reserved;
+    double hardening;   /* TB_MATERIAL_VONMISES: linear hardening modulus H */
+    double yield_stress;/* TB_MATERIAL_VONMISES: initial yield stress */
 } tb_step_params;
 
 typedef struct tb_ctx tb_ctx;

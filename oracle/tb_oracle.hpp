@@ -11,6 +11,8 @@
 //   quadratic B-spline, fast and nodewise src/Basis/bspline.jl:28-184
 //   uGIMP                                 src/Basis/gimp.jl:16-40
 //   WLS (MLS-MPM)                         src/Basis/wls.jl:22-84, polynomials.jl:28-29
+//   KernelCorrection                      src/Basis/kernelcorrection.jl:13-64, wls.jl:86-117
+//   von Mises plasticity (Taylor impact)  docs/src/gpu.md:202-392
 //   stable block partition                src/Parallel/cpu_block_strategy.jl:62-190
 //   P2G / grid update / G2P               README.md:71-87, docs/src/gpu.md:296-331,
 //                                         test/transfer.jl:85-136
@@ -353,6 +355,72 @@ inline void wls_correct(const Mesh<D, T>& M, const T* x, Weights<D, T>& W, bool 
             }
 }
 
+// KernelCorrection(kernel) with its default MultiLinear polynomial
+// (src/Basis/kernelcorrection.jl:13-64): the plain kernel on a whole support
+// (3 nodes on every axis), else the weighted least-squares fit with the
+// MultiLinear polynomial (wls.jl:86-117). Without a node filter that fit of a
+// separable kernel is exactly one 1-D fit with P = (1, X_i - x_p) per axis, the
+// moment matrix of a tensor-product polynomial under a product weight being the
+// Kronecker product of the axis moment matrices; the reference evaluates the
+// B-spline case that way (wls.jl:88-103, 177-192). Per axis: a whole B-spline
+// axis takes the closed form M^-1 = diag(1, 4/h^2) (wls.jl:29-49), otherwise
+// M = sum w P P^T is inverted; the corrected value is w (M^-1 P)[0] and its
+// derivative w (M^-1 P)[1] (the jet of P at 0, wls.jl:70-84). The node weight is
+// the product of the axis values, its gradient the product with the derivative
+// on one axis.
+template <int D, class T>
+inline bool kc_values(const Mesh<D, T>& M, const T* x, bool bspline, T lnorm, Weights<D, T>& W) {
+    T val[3][3] = {}, der[3][3] = {};
+    for (int d = 0; d < D; ++d) {
+        T w[3] = {T(0), T(0), T(0)}, r[3] = {T(0), T(0), T(0)};
+        for (int k = 0; k < W.cnt[d]; ++k) {
+            const T X = node_coord(M, d, W.lo[d] + k);
+            const T xn = (x[d] - X) * M.h_inv;
+            T v, g;
+            if (bspline) jet_bspline_quadratic(xn, v, g);
+            else jet_ugimp(xn, lnorm, v, g);
+            w[k] = v;
+            r[k] = X - x[d];
+        }
+        if (bspline && W.cnt[d] == 3) {
+            const T c = T(4) / (M.h * M.h);
+            for (int k = 0; k < 3; ++k) {
+                val[d][k] = w[k];
+                der[d][k] = w[k] * (c * r[k]);
+            }
+        } else {
+            T S0 = T(0), S1 = T(0), S2 = T(0);
+            for (int k = 0; k < W.cnt[d]; ++k) {
+                S0 += w[k];
+                S1 += w[k] * r[k];
+                S2 += w[k] * r[k] * r[k];
+            }
+            const T det = S0 * S2 - S1 * S1;
+            if (det == T(0)) return false;
+            const T i00 = S2 / det, i01 = -S1 / det, i11 = S0 / det;
+            for (int k = 0; k < W.cnt[d]; ++k) {
+                val[d][k] = w[k] * (i00 + i01 * r[k]);
+                der[d][k] = w[k] * (i01 + i11 * r[k]);
+            }
+        }
+    }
+    for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+        for (int j = 0; j < W.cnt[1]; ++j)
+            for (int i = 0; i < W.cnt[0]; ++i) {
+                const int loc[3] = {i, j, k};
+                const int s = i + 3 * j + (D == 3 ? 9 * k : 0);
+                T w = val[0][i];
+                for (int d = 1; d < D; ++d) w = w * val[d][loc[d]];
+                W.w[s] = w;
+                for (int g = 0; g < D; ++g) {
+                    T q = (g == 0 ? der[0][i] : val[0][i]);
+                    for (int d = 1; d < D; ++d) q = q * (g == d ? der[d][loc[d]] : val[d][loc[d]]);
+                    W.dw[s][g] = q;
+                }
+            }
+    return true;
+}
+
 // update_basis_weight! for one particle (basis_weight.jl:638-642).
 template <int D, class T>
 inline void compute_weights(const Mesh<D, T>& M, int basis, const T* x, T l_abs, Weights<D, T>& W) {
@@ -365,13 +433,17 @@ inline void compute_weights(const Mesh<D, T>& M, int basis, const T* x, T l_abs,
         return;
     }
     W.empty = false;
-    bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP || basis == TB_KC_UGIMP);
     T lnorm = gimp ? l_abs / M.h : T(0);
     if (gimp) window_ugimp(M, xi, lnorm, W);
     else window_bspline_quadratic(M, xi, W);
     bool full = true;
     for (int d = 0; d < D; ++d) full = full && (W.cnt[d] == 3);
-    if (basis == TB_BSPLINE_QUADRATIC) {
+    if (basis == TB_KC_BSPLINE_QUADRATIC || basis == TB_KC_UGIMP) {
+        if (full && basis == TB_KC_BSPLINE_QUADRATIC) fast_values(M, xi, W);
+        else if (full) nodewise_values(M, x, W, [lnorm](T a, T& v, T& g) { jet_ugimp(a, lnorm, v, g); });
+        else if (!kc_values(M, x, basis == TB_KC_BSPLINE_QUADRATIC, lnorm, W)) zero_weights(W);
+    } else if (basis == TB_BSPLINE_QUADRATIC) {
         if (full) fast_values(M, xi, W);
         else nodewise_values(M, x, W, [](T a, T& v, T& g) { jet_bspline_quadratic(a, v, g); });
     } else if (basis == TB_WLS_BSPLINE_QUADRATIC) {
@@ -559,6 +631,134 @@ inline void grid_update(const Mesh<D, T>& M, tb_grid& g, const tb_step_params& p
     for (int64_t I = 0; I < M.nnodes; ++I) grid_update_node(M, g, prm, I);
 }
 
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (Golub & Van Loan, Matrix Computations, 4th ed., Algorithms 8.5.1-8.5.3):
+// A = V diag(e) V^T, the columns of V the eigenvectors. Sweeps stop when the
+// off-diagonal part is below 1e-15 of the matrix norm, or after 20 sweeps.
+inline void sym_eigen3(const double (&A)[3][3], double (&e)[3], double (&V)[3][3]) {
+    double a[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            a[r][c] = A[r][c];
+            V[r][c] = (r == c) ? 1.0 : 0.0;
+        }
+    double fro = 0.0;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) fro += a[r][c] * a[r][c];
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        if (off <= 1e-30 * fro) break;
+        const int pq[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+        for (const auto& ij : pq) {
+            const int p = ij[0], q = ij[1];
+            if (a[p][q] == 0.0) continue;
+            // the rotation (c, s) that zeroes a[p][q] (sym.schur2)
+            const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+            const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+            // a <- J^T a J, V <- V J with J = rotation in the (p, q) plane
+            for (int k = 0; k < 3; ++k) {
+                const double akp = a[k][p], akq = a[k][q];
+                a[k][p] = c * akp - sn * akq;
+                a[k][q] = sn * akp + c * akq;
+            }
+            for (int k = 0; k < 3; ++k) {
+                const double apk = a[p][k], aqk = a[q][k];
+                a[p][k] = c * apk - sn * aqk;
+                a[q][k] = sn * apk + c * aqk;
+            }
+            for (int k = 0; k < 3; ++k) {
+                const double vkp = V[k][p], vkq = V[k][q];
+                V[k][p] = c * vkp - sn * vkq;
+                V[k][q] = sn * vkp + c * vkq;
+            }
+        }
+    }
+    for (int k = 0; k < 3; ++k) e[k] = a[k][k];
+}
+
+// The von Mises model of the Taylor impact (docs/src/gpu.md:362-391):
+// Hencky elasticity on the trial left Cauchy-Green tensor b = F Cp^-1 F^T,
+// yield f = sqrt(3/2 tau'.tau') - (tau_y0 + H eps_p) on the principal Kirchhoff
+// deviator, return map Delta gamma = f / (3 mu + H) along df/dtau in principal
+// logarithmic stretches, pressure kappa log J / J with kappa = lambda + 2 mu / 3;
+// returns the Cauchy stress and the updated Cp^-1 = F^-1 b_e F^-T and eps_p.
+inline void vonmises_model(const double (&Cpinv)[3][3], double epn, const double (&F)[3][3], double lam,
+                           double mu, double H, double ty0, double (&sig)[3][3], double (&Cpinv_new)[3][3],
+                           double& ep_new) {
+    const double kappa = lam + 2.0 * mu / 3.0;
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    const double lJ = std::log(J);
+    const double pr = kappa * lJ / J;
+    double FC[3][3] = {}, b[3][3] = {};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) FC[r][c] += F[r][k] * Cpinv[k][c];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) b[r][c] += FC[r][k] * F[c][k];
+    double bs[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) bs[r][c] = 0.5 * (b[r][c] + b[c][r]);
+    double ev[3], n[3][3];
+    sym_eigen3(bs, ev, n);
+    double lst[3], tau[3], tau_tr[3];
+    double tt = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        lst[a] = std::sqrt(ev[a]);
+        tau_tr[a] = 2.0 * mu * std::log(lst[a]) - 2.0 * mu / 3.0 * lJ;
+        tt += tau_tr[a] * tau_tr[a];
+    }
+    const double nrm = std::sqrt(1.5 * tt);
+    const double ftr = nrm - (ty0 + H * epn);
+    double dgam = 0.0, le[3];
+    for (int a = 0; a < 3; ++a) {
+        le[a] = lst[a];
+        tau[a] = tau_tr[a];
+    }
+    if (ftr > 0.0) {
+        dgam = ftr / (3.0 * mu + H);
+        for (int a = 0; a < 3; ++a) {
+            const double deps = dgam * (1.5 * tau_tr[a] / nrm);
+            le[a] = std::exp(std::log(lst[a]) - deps);
+            tau[a] = tau_tr[a] - 2.0 * mu * deps;
+        }
+    }
+    double be[3][3] = {};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 3; ++a) {
+                be[r][c] += le[a] * le[a] * n[r][a] * n[c][a];
+                sig[r][c] = 0.0;
+            }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 3; ++a) sig[r][c] += (tau[a] / J + pr) * n[r][a] * n[c][a];
+    // F^-1 by cofactors
+    double Fi[3][3];
+    Fi[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) / J;
+    Fi[0][1] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) / J;
+    Fi[0][2] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) / J;
+    Fi[1][0] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) / J;
+    Fi[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) / J;
+    Fi[1][2] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) / J;
+    Fi[2][0] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) / J;
+    Fi[2][1] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) / J;
+    Fi[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) / J;
+    double Fb[3][3] = {}, C[3][3] = {};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) Fb[r][c] += Fi[r][k] * be[k][c];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) C[r][c] += Fb[r][k] * Fi[c][k];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) Cpinv_new[r][c] = 0.5 * (C[r][c] + C[c][r]);
+    ep_new = epn + dgam;
+}
+
 // One particle of @G2P (README.md:79-86, test/transfer.jl:112-136, transfer.md:180-184):
 // FLIP/PIC blend or APIC, then F = (I + dt grad v) F in FP64, J = det F,
 // Neo-Hookean sigma = (mu (F F^T - I) + lambda log J I) / J, V = V0 J.
@@ -641,6 +841,29 @@ inline void g2p_particle(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p,
     const double mu = p.mu ? double(CP<T>(p.mu)[i]) : prm.mu;
     const double lam = p.lambda ? double(CP<T>(p.lambda)[i]) : prm.lambda;
     double sig[3][3] = {};
+    if (prm.material == TB_MATERIAL_VONMISES) {
+        // docs/src/gpu.md:352-358: F = dF F, von Mises state update, V = det(dF) V
+        if constexpr (D == 3) {
+            double Cp[3][3], Cpn[3][3], epn = double(CP<T>(p.eps_p)[i]), epo;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) Cp[r][c] = double(CP<T>(p.Cp_inv[symidx<D>(r, c)])[i]);
+            vonmises_model(Cp, epn, Fn, lam, mu, prm.hardening, prm.yield_stress, sig, Cpn, epo);
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c <= r; ++c) {
+                    P<T>(p.sigma[symidx<D>(r, c)])[i] = T(sig[r][c]);
+                    P<T>(p.Cp_inv[symidx<D>(r, c)])[i] = T(Cpn[r][c]);
+                }
+            P<T>(p.eps_p)[i] = T(epo);
+            double dF[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) dF[r][c] = (r == c ? 1.0 : 0.0) + double(gv[r][c]) * dtd;
+            const double jd = dF[0][0] * (dF[1][1] * dF[2][2] - dF[1][2] * dF[2][1]) -
+                              dF[0][1] * (dF[1][0] * dF[2][2] - dF[1][2] * dF[2][0]) +
+                              dF[0][2] * (dF[1][0] * dF[2][1] - dF[1][1] * dF[2][0]);
+            P<T>(p.V)[i] = T(jd * double(CP<T>(p.V)[i]));
+        }
+        return;
+    }
     if (prm.material == 1) {
         for (int d = 0; d < D; ++d) sig[d][d] = lam * (J - 1.0);
     } else {

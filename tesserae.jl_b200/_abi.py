@@ -21,12 +21,15 @@ TB_BSPLINE_QUADRATIC = 0
 TB_UGIMP = 1
 TB_WLS_BSPLINE_QUADRATIC = 2
 TB_WLS_UGIMP = 3
+TB_KC_BSPLINE_QUADRATIC = 4
+TB_KC_UGIMP = 5
 
 TB_TRANSFER_FLIP = 0
 TB_TRANSFER_APIC = 1
 
 MATERIAL_NEOHOOKEAN = 0
 MATERIAL_FLUID = 1
+MATERIAL_VONMISES = 2
 
 VP = C.c_void_p
 
@@ -57,6 +60,8 @@ class tb_particles(C.Structure):
         ("V0", VP),
         ("mu", VP),
         ("lambda_", VP),
+        ("eps_p", VP),
+        ("Cp_inv", VP * 6),
     ]
 
 
@@ -95,6 +100,8 @@ class tb_step_params(C.Structure):
         ("wall_mask", C.c_int32),
         ("wall_layers", C.c_int32),
         ("reserved", C.c_int32),
+        ("hardening", C.c_double),
+        ("yield_stress", C.c_double),
     ]
 
 

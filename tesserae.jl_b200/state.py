@@ -151,7 +151,8 @@ class Particles:
     field except F, which is float64 in both forms. With `x64=True` (float32
     only) the positions are float64 as well: the FP64-position form."""
 
-    FIELDS = ("x", "v", "V", "m", "l", "grad_v", "sigma", "F", "B", "V0", "mu", "lam")
+    FIELDS = ("x", "v", "V", "m", "l", "grad_v", "sigma", "F", "B", "V0", "mu", "lam", "eps_p", "Cp_inv")
+    OPTIONAL = ("m", "l", "B", "V0", "mu", "lam", "eps_p", "Cp_inv")
 
     def __init__(self, n, dim, dtype=np.float64, backend="numpy", device=None, optional=(), x64=False):
         self.n, self.dim, self.dtype = int(n), int(dim), np.dtype(dtype).type
@@ -173,6 +174,13 @@ class Particles:
         self.V0 = a((self.n,)) if "V0" in optional else None
         self.mu = a((self.n,)) if "mu" in optional else None
         self.lam = a((self.n,)) if "lam" in optional else None
+        # von Mises plasticity state: equivalent plastic strain and the inverse
+        # plastic right Cauchy-Green tensor (symmetric, identity at rest)
+        self.eps_p = a((self.n,)) if "eps_p" in optional else None
+        self.Cp_inv = a((nsym(D), self.n)) if "Cp_inv" in optional else None
+        if self.Cp_inv is not None:
+            for k in ((0, 3, 5) if D == 3 else (0, 2)):
+                self.Cp_inv[k] = 1.0
 
     def __len__(self):
         return self.n
@@ -199,6 +207,9 @@ class Particles:
         s.V0 = _ptr(self.V0)
         s.mu = _ptr(self.mu)
         s.lambda_ = _ptr(self.lam)
+        s.eps_p = _ptr(self.eps_p)
+        for k, p in enumerate(_row_ptrs(self.Cp_inv, nsym(D))):
+            s.Cp_inv[k] = p
         return s
 
     def to(self, backend, device=None, dtype=None, x64=None) -> "Particles":
@@ -206,7 +217,7 @@ class Particles:
         (`x64`: float64 positions with a float32 state; default: as self)."""
         dtype = np.dtype(dtype or self.dtype).type
         x64 = self.x64 if x64 is None else bool(x64)
-        opt = tuple(k for k in ("m", "l", "B", "V0", "mu", "lam") if getattr(self, k) is not None)
+        opt = tuple(k for k in self.OPTIONAL if getattr(self, k) is not None)
         out = Particles(self.n, self.dim, dtype, backend, device, optional=opt, x64=x64)
         for k in self.FIELDS:
             src = getattr(self, k)
@@ -373,7 +384,8 @@ def lame(E: float, nu: float) -> tuple[float, float]:
 
 def step_params(dt, mass=0.0, V0=0.0, mu=0.0, lam=0.0, gravity=(0.0, 0.0, 0.0), gimp_l=0.0,
                 flip_alpha=1.0, basis=_abi.TB_BSPLINE_QUADRATIC, transfer=_abi.TB_TRANSFER_FLIP,
-                material=_abi.MATERIAL_NEOHOOKEAN, wall_mask=0, wall_layers=0) -> _abi.tb_step_params:
+                material=_abi.MATERIAL_NEOHOOKEAN, wall_mask=0, wall_layers=0, hardening=0.0,
+                yield_stress=0.0) -> _abi.tb_step_params:
     s = _abi.tb_step_params()
     s.dt, s.mass, s.V0, s.mu, s.lambda_ = dt, mass, V0, mu, lam
     for d in range(3):
@@ -381,4 +393,5 @@ def step_params(dt, mass=0.0, V0=0.0, mu=0.0, lam=0.0, gravity=(0.0, 0.0, 0.0), 
     s.gimp_l, s.flip_alpha = gimp_l, flip_alpha
     s.basis, s.transfer, s.material = basis, transfer, material
     s.wall_mask, s.wall_layers, s.reserved = wall_mask, wall_layers, 0
+    s.hardening, s.yield_stress = hardening, yield_stress
     return s

@@ -94,6 +94,39 @@ def main(ref_root: str):
         cases.append({"kind": "basis_props", "basis": "wls_ugimp", "dim": dim, "h": h, "x": boundary,
                       "l": 0.5 * h / 2, "pu": True, "lfr": True, "truncated": True, "source": src_wls_g})
 
+    # KernelCorrection restores both properties at the boundary (test/basis.jl:449-465)
+    src_kc_i = require(ref, "test/basis.jl", 456, "partition=true, reproduces_linear=true, truncated=false")
+    src_kc_b = require(ref, "test/basis.jl", 460, "partition=true, reproduces_linear=true, truncated=true")
+    src_kc_g = require(ref, "test/basis.jl", 463, "partition=true, reproduces_linear=true, truncated=true")
+    require(ref, "test/basis.jl", 455, "KernelCorrection(BSpline(Quadratic()))")
+    require(ref, "test/basis.jl", 462, "KernelCorrection(uGIMP())")
+    for dim in (2, 3):
+        interior = [0.45 + 0.01 * (i + 1) for i in range(dim)]
+        boundary = [0.02] + interior[1:]
+        h = 0.1
+        cases.append({"kind": "basis_props", "basis": "kc_bspline_quadratic", "dim": dim, "h": h, "x": interior,
+                      "l": 0.0, "pu": True, "lfr": True, "truncated": False, "source": src_kc_i})
+        cases.append({"kind": "basis_props", "basis": "kc_bspline_quadratic", "dim": dim, "h": h, "x": boundary,
+                      "l": 0.0, "pu": True, "lfr": True, "truncated": True, "source": src_kc_b})
+        cases.append({"kind": "basis_props", "basis": "kc_ugimp", "dim": dim, "h": h, "x": boundary,
+                      "l": 0.5 * h / 2, "pu": True, "lfr": True, "truncated": True, "source": src_kc_g})
+
+    # Positivity of KernelCorrection(BSpline(Quadratic()), MultiLinear) near the
+    # boundary (test/basis.jl:566-614): the node's weight is > -sqrt(eps) for
+    # particles on a 1/11 lattice over [max(x0, I - L - 1), min(x1, I + L - 1) - sqrt(eps)]
+    # per axis (L = 1.5, 1-based node index I, unit spacing).
+    require(ref, "test/basis.jl", 574, "step=1/11")
+    require(ref, "test/basis.jl", 572, "BSpline{Quadratic} ? 1.5")
+    for dim, node, lims, line_no in ((2, [2, 2], [[0, 10], [0, 10]], 596), (3, [2, 2, 1], [[0, 10]] * 3, 608)):
+        cases.append({"kind": "kc_positive", "dim": dim, "h": 1.0, "lims": lims, "nodes": [node], "L": 1.5,
+                      "source": require(ref, "test/basis.jl", line_no, "multilin, CartesianIndex(")})
+    for dim, line_no in ((2, 601), (3, 613)):
+        src = require(ref, "test/basis.jl", line_no, "all(i -> is_positive_everywhere(domain, kern, multilin, i)")
+        for I in (([1, 1], [3, 2]) if dim == 2 else ([1, 1, 1], [3, 2, 1])):
+            nodes = [list(t) for t in __import__("itertools").product(*[range(1, k + 1) for k in I])]
+            cases.append({"kind": "kc_positive", "dim": dim, "h": 1.0, "lims": [[0, k] for k in I], "nodes": nodes,
+                          "L": 1.5, "source": src})
+
     # Block-tile containment for 2D meshes of h = 0.02 (test/transfer.jl:941-957)
     cases.append({"kind": "tile_contains", "h": 0.02, "lims": [[0, 1], [0, 1]], "l": 0.01,
                   "bases": ["bspline_quadratic", "ugimp", "wls_bspline_quadratic"],

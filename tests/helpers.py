@@ -18,7 +18,8 @@ def max_rel(a, b, floor):
 
 def basis_kind(abi, name):
     return {"bspline_quadratic": abi.TB_BSPLINE_QUADRATIC, "ugimp": abi.TB_UGIMP,
-            "wls_bspline_quadratic": abi.TB_WLS_BSPLINE_QUADRATIC, "wls_ugimp": abi.TB_WLS_UGIMP}[name]
+            "wls_bspline_quadratic": abi.TB_WLS_BSPLINE_QUADRATIC, "wls_ugimp": abi.TB_WLS_UGIMP,
+            "kc_bspline_quadratic": abi.TB_KC_BSPLINE_QUADRATIC, "kc_ugimp": abi.TB_KC_UGIMP}[name]
 
 
 def reference_partition(mesh, x):

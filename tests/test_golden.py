@@ -102,6 +102,37 @@ def test_basis_properties(tb, oracle, case):
         assert truncated == case["truncated"], case["source"]
 
 
+@pytest.mark.parametrize("case", by_kind("kc_positive"),
+                         ids=lambda c: f"{c['dim']}d-{len(c['nodes'])}nodes-{c['source']}")
+def test_kernel_correction_positive(tb, oracle, case):
+    """The node weight of KernelCorrection(BSpline(Quadratic())) is > -sqrt(eps)
+    for every particle of the 1/11 lattice around the node, as in the
+    reference's positivity test."""
+    dim, L = case["dim"], case["L"]
+    mesh = tb.CartesianMesh(case["h"], *[tuple(l) for l in case["lims"]])
+    eps = np.finfo(np.float64).eps
+    prm = tb.step_params(1.0, basis=tb._abi.TB_KC_BSPLINE_QUADRATIC)
+    for node in case["nodes"]:
+        axes = []
+        for d in range(dim):
+            lo = max(case["lims"][d][0], node[d] - L - 1)
+            hi = min(case["lims"][d][1], node[d] + L - 1) - np.sqrt(eps)
+            axes.append(np.arange(0, int(np.floor((hi - lo) * 11 + 1e-9)) + 1) / 11.0 + lo)
+        pts = np.stack([g.ravel() for g in np.meshgrid(*axes, indexing="ij")])
+        n = pts.shape[1]
+        P = tb.Particles(n, dim)
+        P.x[...] = pts
+        W = tb.generate_basis_weights(dim, n)
+        oracle.update_weights(mesh, P, prm, W)
+        win = W.window.reshape(n, dim, 2)
+        val = np.zeros(n)
+        for i in range(n):
+            loc = [node[d] - win[i, d, 0] for d in range(dim)]  # 0-based slot of the node in the window
+            if all(0 <= loc[d] <= win[i, d, 1] - win[i, d, 0] for d in range(dim)):
+                val[i] = W.w[i][sum(loc[d] * 3 ** d for d in range(dim))]
+        assert np.all(val > -np.sqrt(eps)), (node, case["source"], val.min())
+
+
 def test_tile_contains_every_window(tb, oracle):
     c = by_kind("tile_contains")[0]
     mesh = tb.CartesianMesh(c["h"], *[tuple(l) for l in c["lims"]], block_size_log2=2)
