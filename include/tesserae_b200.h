@@ -262,6 +262,15 @@ int32_t tb_reorder_particles_f32(tb_ctx* ctx, int32_t dim, tb_particles* particl
                                  double threshold, int32_t* reordered);
 int32_t tb_reorder_particles_f32x64(tb_ctx* ctx, int32_t dim, tb_particles* particles, tb_partition* partition,
                                     double threshold, int32_t* reordered);
+/* max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v| (lambda, mu and
+ * m per particle when the arrays are given, else from params): the speed of the
+ * Taylor impact's time step CFL h / c_max (docs/src/gpu.md:283-284), reduced on
+ * the device. Synchronous. `particles` may be in the FP64-position form (x is
+ * not read). */
+int32_t tb_max_wave_speed_f64(tb_ctx* ctx, int32_t dim, const tb_particles* particles,
+                              const tb_step_params* params, double* c_max);
+int32_t tb_max_wave_speed_f32(tb_ctx* ctx, int32_t dim, const tb_particles* particles,
+                              const tb_step_params* params, double* c_max);
 /* block_ordered_particle_contiguity of `n` particles binned into `partition`. Synchronous. */
 int32_t tb_particle_contiguity(tb_ctx* ctx, const tb_partition* partition, int64_t n, double* score);
 /* tb_step_* with reorder_particles!(particles, partition; threshold) after every

@@ -151,6 +151,8 @@ SIGNATURES += [
     ("tb_step_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params), I32]),
     ("tb_rollout_host_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
     ("tb_particle_contiguity", I32, [VP, P(tb_partition), I64, P(C.c_double)]),
+    ("tb_max_wave_speed_f64", I32, [VP, I32, P(tb_particles), P(tb_step_params), P(C.c_double)]),
+    ("tb_max_wave_speed_f32", I32, [VP, I32, P(tb_particles), P(tb_step_params), P(C.c_double)]),
 ]
 for _p in ("f64", "f32", "f32x64"):
     SIGNATURES += [

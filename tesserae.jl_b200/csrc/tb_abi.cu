@@ -118,6 +118,7 @@ struct tb_ctx {
     unsigned long long* ro_scratch = nullptr;
     long long ro_scratch_cap = 0;
     unsigned long long* ro_acc = nullptr;  // [2]
+    unsigned long long* wave_max = nullptr;  // tb_max_wave_speed_* result
     int* ro_decision = nullptr;            // [2]
     double* ro_score = nullptr;            // [1]
 };
@@ -186,18 +187,19 @@ long long mesh_nblocks(const tb_mesh* m) {
 // window against the block width (src/Transfer/runtime.jl:192-229).
 int check_params(tb_ctx* c, const tb_step_params* p) {
     if (!p) return fail(c, TB_ERR_ARG, "params is NULL");
-    if (p->basis < TB_BSPLINE_QUADRATIC || p->basis > TB_WLS_UGIMP)
+    if (p->basis < TB_BSPLINE_QUADRATIC || p->basis > TB_KC_UGIMP)
         return fail(c, TB_ERR_ARG, "unknown basis kind %d", p->basis);
     if (p->transfer != TB_TRANSFER_FLIP && p->transfer != TB_TRANSFER_APIC)
         return fail(c, TB_ERR_ARG, "unknown transfer kind %d", p->transfer);
-    if (p->material != 0 && p->material != 1) return fail(c, TB_ERR_ARG, "unknown material %d", p->material);
+    if (p->material < TB_MATERIAL_NEOHOOKEAN || p->material > TB_MATERIAL_VONMISES)
+        return fail(c, TB_ERR_ARG, "unknown material %d", p->material);
     return TB_OK;
 }
 
 // x64: the FP64-position form (particles.x are double arrays, the rest T).
 template <class T>
 int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool apic, PView<T>& P,
-               bool x64 = false) {
+               bool x64 = false, int material = TB_MATERIAL_NEOHOOKEAN) {
     if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
     if (p->n < 0 || p->n > 0x7fffffffll)
         return fail(c, TB_ERR_CAPACITY, "particle count %lld exceeds the partition's Int32 capacity", (long long)p->n);
@@ -229,6 +231,14 @@ int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool 
     P.V0 = static_cast<const T*>(p->V0);
     P.mu = static_cast<const T*>(p->mu);
     P.lam = static_cast<const T*>(p->lambda);
+    P.eps_p = static_cast<T*>(p->eps_p);
+    for (int k = 0; k < 6; ++k) P.Cp_inv[k] = static_cast<T*>(p->Cp_inv[k]);
+    if (need_state && material == TB_MATERIAL_VONMISES) {
+        if (dim != 3) return fail(c, TB_ERR_UNSUPPORTED, "the von Mises model is three-dimensional");
+        if (p->n && !P.eps_p) return fail(c, TB_ERR_ARG, "the von Mises model needs particles.eps_p");
+        for (int k = 0; k < 6; ++k)
+            if (p->n && !P.Cp_inv[k]) return fail(c, TB_ERR_ARG, "the von Mises model needs particles.Cp_inv[%d]", k);
+    }
     return TB_OK;
 }
 
@@ -314,6 +324,8 @@ int particle_fields(const tb_particles* p, int D, size_t elem, bool x64, std::ve
     add(p->V0, elem);
     add(p->mu, elem);
     add(p->lambda, elem);
+    add(p->eps_p, elem);
+    for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(p->Cp_inv[k], elem);
     return TB_OK;
 }
 
@@ -404,7 +416,8 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
     PView<T> P;
     GView<T> G;
     int rc;
-    if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P, x64)) != TB_OK) return rc;
+    if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P, x64, prm->material)) != TB_OK)
+        return rc;
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
     BinBuffers B;
     if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
@@ -576,7 +589,9 @@ int do_g2p_direct(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p
         return rc;
     PView<T> P;
     GView<T> G;
-    if ((rc = make_pview<T>(c, p, m->dim, true, prm->transfer == TB_TRANSFER_APIC, P)) != TB_OK) return rc;
+    if ((rc = make_pview<T>(c, p, m->dim, true, prm->transfer == TB_TRANSFER_APIC, P, false, prm->material)) !=
+        TB_OK)
+        return rc;
     if ((rc = make_gview<T>(c, g, m->dim, G)) != TB_OK) return rc;
     const LaunchCfg cfg = cfg_of(c);
     cudaError_t e = (m->dim == 3) ? launch_g2p_direct<3, T>(make_dmesh<3, T>(*m), G, P, make_scalars<T>(*prm), cfg)
@@ -601,7 +616,8 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     long long nn = 1;
     for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
     const long long nb = mesh_nblocks(m);
-    // Fields moved: x, v, V, grad_v, sigma (T); F (double); optional m, l, B, V0, mu, lambda (T).
+    // Fields moved: x, v, V, grad_v, sigma (T); F (double); optional m, l, B, V0, mu, lambda (T), and the
+    // von Mises state eps_p, Cp_inv (T, in and out).
     struct Field {
         void** host_slot;
         size_t elem;
@@ -624,6 +640,10 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     add(&host->V0, sizeof(T), false);
     add(&host->mu, sizeof(T), false);
     add(&host->lambda, sizeof(T), false);
+    if (prm->material == TB_MATERIAL_VONMISES) {
+        add(&host->eps_p, sizeof(T), true);
+        for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&host->Cp_inv[k], sizeof(T), true);
+    }
     auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
     size_t bytes = 0;
     for (auto& f : fields) bytes += align(f.elem * size_t(n));
@@ -669,6 +689,8 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
         dev.V0 = remap(&host->V0);
         dev.mu = remap(&host->mu);
         dev.lambda = remap(&host->lambda);
+        dev.eps_p = remap(&host->eps_p);
+        for (int k = 0; k < 6; ++k) dev.Cp_inv[k] = k < (D == 3 ? 6 : 3) ? remap(&host->Cp_inv[k]) : nullptr;
         (void)i;
     }
     tb_grid g{};
@@ -710,6 +732,31 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     return check_device_status(c);
 }
 
+template <class T>
+int do_wave_speed(tb_ctx* c, int32_t dim, const tb_particles* p, const tb_step_params* prm, double* cmax) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_params(c, prm)) != TB_OK) return rc;
+    if (dim != 2 && dim != 3) return fail(c, TB_ERR_ARG, "dim must be 2 or 3");
+    if (!cmax) return fail(c, TB_ERR_ARG, "c_max is NULL");
+    PView<T> P;
+    if ((rc = make_pview<T>(c, p, dim, false, false, P)) != TB_OK) return rc;
+    if (P.n && !P.V) return fail(c, TB_ERR_ARG, "particles.V is NULL");
+    for (int d = 0; d < dim; ++d)
+        if (P.n && !P.v[d]) return fail(c, TB_ERR_ARG, "particles.v[%d] is NULL", d);
+    cudaError_t e = cudaSuccess;
+    if (!c->wave_max) e = cudaMalloc(&c->wave_max, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc wave speed");
+    const auto S = make_scalars<T>(*prm);
+    e = dim == 3 ? launch_wave_speed<3, T>(P, S, c->wave_max, cfg_of(c)) : launch_wave_speed<2, T>(P, S, c->wave_max, cfg_of(c));
+    unsigned long long bits = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, c->wave_max, sizeof bits, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "wave speed");
+    std::memcpy(cmax, &bits, sizeof bits);
+    return TB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // reverse mode
 // ---------------------------------------------------------------------------
@@ -722,6 +769,8 @@ int check_adjoint_params(tb_ctx* c, const tb_step_params* p) {
                     p->basis);
     if (p->transfer != TB_TRANSFER_FLIP)
         return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the FLIP/PIC transfer only");
+    if (p->material == TB_MATERIAL_VONMISES)
+        return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the Neo-Hookean and fluid materials only");
     return TB_OK;
 }
 
@@ -1031,6 +1080,7 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->tape_seg);
     cudaFree(c->ro_scratch);
     cudaFree(c->ro_acc);
+    cudaFree(c->wave_max);
     cudaFree(c->ro_decision);
     cudaFree(c->ro_score);
     delete c->prof;
@@ -1186,6 +1236,15 @@ int32_t tb_particle_contiguity(tb_ctx* c, const tb_partition* part, int64_t n, d
     if (e != cudaSuccess) return cuda_fail(c, e, "contiguity");
     *score = sc;
     return TB_OK;
+}
+
+int32_t tb_max_wave_speed_f64(tb_ctx* c, int32_t dim, const tb_particles* p, const tb_step_params* prm,
+                              double* c_max) {
+    return do_wave_speed<double>(c, dim, p, prm, c_max);
+}
+int32_t tb_max_wave_speed_f32(tb_ctx* c, int32_t dim, const tb_particles* p, const tb_step_params* prm,
+                              double* c_max) {
+    return do_wave_speed<float>(c, dim, p, prm, c_max);
 }
 
 int32_t tb_rollout_host_f64(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_params* prm,

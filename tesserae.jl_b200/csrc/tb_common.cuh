@@ -78,6 +78,8 @@ struct PView {
     const T* V0;
     const T* mu;
     const T* lam;
+    T* eps_p;      // von Mises: equivalent plastic strain
+    T* Cp_inv[6];  // von Mises: inverse plastic right Cauchy-Green tensor (symmetric)
 };
 
 template <class T>
@@ -93,7 +95,7 @@ struct GView {
 template <class T>
 struct Scalars {
     T dt, mass, V0, g[3], gimp_l, alpha;
-    double dt64, V0_64, mu, lam;
+    double dt64, V0_64, mu, lam, hardening, yield_stress;
     int basis, transfer, material, wall_mask, wall_layers;
 };
 
@@ -115,7 +117,17 @@ inline Scalars<T> make_scalars(const tb_step_params& p) {
     s.material = p.material;
     s.wall_mask = p.wall_mask;
     s.wall_layers = p.wall_layers;
+    s.hardening = p.hardening;
+    s.yield_stress = p.yield_stress;
     return s;
+}
+
+// Basis kinds whose support window is uGIMP's, and the KernelCorrection kinds.
+__host__ __device__ inline bool basis_is_gimp(int basis) {
+    return basis == TB_UGIMP || basis == TB_WLS_UGIMP || basis == TB_KC_UGIMP;
+}
+__host__ __device__ inline bool basis_is_kc(int basis) {
+    return basis == TB_KC_BSPLINE_QUADRATIC || basis == TB_KC_UGIMP;
 }
 
 template <int D>
@@ -243,7 +255,7 @@ __device__ __forceinline__ bool axis_window(const DMesh<D, T>& M, int basis, con
         inside = inside && (c >= T(0) && c <= T(M.n[d] - 2));
     }
     if (!inside) return false;
-    const bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    const bool gimp = basis_is_gimp(basis);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         int s, e;
@@ -267,7 +279,7 @@ __device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, co
     T xi[3];
     int lo[3], cnt[3];
     if (!axis_window<D, T>(M, basis, x, lnorm, xi, lo, cnt)) return false;
-    const bool gimp = (basis == TB_UGIMP || basis == TB_WLS_UGIMP);
+    const bool gimp = basis_is_gimp(basis);
     full = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -275,7 +287,7 @@ __device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, co
         ax[d].cnt = cnt[d];
         full = full && (ax[d].cnt == 3);
     }
-    if (basis == TB_BSPLINE_QUADRATIC && full) {
+    if ((basis == TB_BSPLINE_QUADRATIC || basis == TB_KC_BSPLINE_QUADRATIC) && full) {
 #pragma unroll
         for (int d = 0; d < D; ++d) bspline_quadratic_axis(xi[d], ax[d].val, ax[d].der);
         return true;
@@ -290,6 +302,48 @@ __device__ __forceinline__ bool axis_weights(const DMesh<D, T>& M, int basis, co
                 T xn = (x[d] - node_coord(M, d, ax[d].lo + k)) * M.h_inv;
                 if (gimp) jet_ugimp(xn, lnorm, ax[d].val[k], ax[d].der[k]);
                 else jet_bspline_quadratic(xn, ax[d].val[k], ax[d].der[k]);
+            }
+        }
+    }
+    return true;
+}
+
+// KernelCorrection(kernel) with its default MultiLinear polynomial on a
+// support the mesh cuts (src/Basis/kernelcorrection.jl:13-64; a whole support
+// keeps the plain kernel). Without a node filter the MultiLinear weighted
+// least-squares fit of a separable kernel is one 1-D fit with P = (1, X_i - x_p)
+// per axis (the moment matrix of the tensor-product polynomial under a product
+// weight is the Kronecker product of the axis moment matrices), the
+// decomposition the reference evaluates for B-splines (wls.jl:88-103, 177-192).
+// Per axis the kernel values w_k become w_k (M^-1 P_k)[0] and their derivative
+// w_k (M^-1 P_k)[1]; a whole B-spline axis takes the closed form
+// M^-1 = diag(1, 4/h^2) (wls.jl:29-49). `r[d][k]` = X_k - x_p. The derivative is
+// stored in units of xi (times h) like the plain jets. False for a singular fit.
+template <int D, class T>
+__device__ __forceinline__ bool kc_correct(const DMesh<D, T>& M, bool bspline, const T (&r)[3][3], Axis<T>* ax) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        if (bspline && ax[d].cnt == 3) {
+            const T c = T(4) / (M.h * M.h);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ax[d].der[k] = ax[d].val[k] * (c * r[d][k]) * M.h;
+        } else {
+            T S0 = T(0), S1 = T(0), S2 = T(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (k >= ax[d].cnt) continue;
+                S0 += ax[d].val[k];
+                S1 += ax[d].val[k] * r[d][k];
+                S2 += ax[d].val[k] * r[d][k] * r[d][k];
+            }
+            const T det = S0 * S2 - S1 * S1;
+            if (det == T(0)) return false;
+            const T i00 = S2 / det, i01 = -S1 / det, i11 = S0 / det;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const T w = ax[d].val[k];
+                ax[d].val[k] = k < ax[d].cnt ? w * (i00 + i01 * r[d][k]) : T(0);
+                ax[d].der[k] = k < ax[d].cnt ? w * (i01 + i11 * r[d][k]) * M.h : T(0);
             }
         }
     }
@@ -402,7 +456,7 @@ template <int D, class T, bool ALLOW_WLS = true>
 __device__ __forceinline__ bool prepare_basis(const DMesh<D, T>& M, int basis, const T* x, T l_abs,
                                               Basis<D, T>& B, int* err) {
     T lnorm = T(0);
-    if (basis == TB_UGIMP || basis == TB_WLS_UGIMP) {
+    if (basis_is_gimp(basis)) {
         lnorm = l_abs / M.h;
         if (!(lnorm >= T(0) && lnorm <= T(1))) {
             atomicOr(err, ERR_GIMP_LENGTH);
@@ -411,6 +465,17 @@ __device__ __forceinline__ bool prepare_basis(const DMesh<D, T>& M, int basis, c
     }
     bool full = false;
     if (!axis_weights<D, T>(M, basis, x, lnorm, B.ax, full)) return false;
+    if (basis_is_kc(basis) && !full) {
+        T r[3][3] = {};
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[d][k] = node_coord(M, d, B.ax[d].lo + k) - x[d];
+        if (!kc_correct<D, T>(M, basis == TB_KC_BSPLINE_QUADRATIC, r, B.ax)) {
+            atomicOr(err, ERR_WLS_SINGULAR);
+            return false;
+        }
+    }
     B.wls = ALLOW_WLS && (basis == TB_WLS_BSPLINE_QUADRATIC || basis == TB_WLS_UGIMP);
     if constexpr (ALLOW_WLS) if (B.wls) {
         bool closed = (basis == TB_WLS_BSPLINE_QUADRATIC) && full;
@@ -439,7 +504,7 @@ __device__ __forceinline__ bool axis_window_x64(const DMesh<D, T>& M, int basis,
         inside = inside && (c >= 0.0 && c <= double(M.n[d] - 2));
     }
     if (!inside) return false;
-    const bool gimp = basis == TB_UGIMP;
+    const bool gimp = basis_is_gimp(basis);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         int st, e;
@@ -461,7 +526,7 @@ template <int D, class T>
 __device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basis, const double* x, T l_abs,
                                                   Basis<D, T>& B, int* err) {
     double lnorm = 0.0;
-    const bool gimp = basis == TB_UGIMP;
+    const bool gimp = basis_is_gimp(basis);
     if (gimp) {
         lnorm = double(l_abs) / M.h64;
         if (!(lnorm >= 0.0 && lnorm <= 1.0)) {
@@ -505,6 +570,17 @@ __device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basi
             }
         }
     }
+    if (basis_is_kc(basis) && !full) {
+        T r[3][3] = {};
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[d][k] = T(__dadd_rn(M.xmin64[d], __dmul_rn(double(lo[d] + k), M.h64)) - x[d]);
+        if (!kc_correct<D, T>(M, basis == TB_KC_BSPLINE_QUADRATIC, r, B.ax)) {
+            atomicOr(err, ERR_WLS_SINGULAR);
+            return false;
+        }
+    }
     return true;
 }
 
@@ -533,9 +609,169 @@ __device__ __forceinline__ void eval_node(const DMesh<D, T>& M, const Basis<D, T
     }
 }
 
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (Golub & Van Loan, Matrix Computations, 4th ed., Algorithms 8.5.1-8.5.3):
+// A = V diag(e) V^T, eigenvectors in the columns of V; stops when the
+// off-diagonal part falls below 1e-15 of the matrix norm (at most 20 sweeps).
+__device__ __forceinline__ void sym_eigen3(double (&a)[3][3], double (&e)[3], double (&V)[3][3]) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
+    double fro = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fro += a[r][c] * a[r][c];
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        if (off <= 1e-30 * fro) break;
+#pragma unroll
+        for (int pq = 0; pq < 3; ++pq) {
+            const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+            if (a[p][q] == 0.0) continue;
+            const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double akp = a[k][p], akq = a[k][q];
+                a[k][p] = c * akp - sn * akq;
+                a[k][q] = sn * akp + c * akq;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double apk = a[p][k], aqk = a[q][k];
+                a[p][k] = c * apk - sn * aqk;
+                a[q][k] = sn * apk + c * aqk;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double vkp = V[k][p], vkq = V[k][q];
+                V[k][p] = c * vkp - sn * vkq;
+                V[k][q] = sn * vkp + c * vkq;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[k] = a[k][k];
+}
+
+// The von Mises update of the Taylor impact (docs/src/gpu.md:352-391), one
+// particle, FP64 throughout: F = dF F is given. Hencky elasticity on the trial
+// left Cauchy-Green tensor b = F Cp^-1 F^T; yield f = sqrt(3/2 tau'.tau') -
+// (tau_y0 + H eps_p) on the principal Kirchhoff deviator; return map
+// Delta gamma = f / (3 mu + H) along df/dtau in principal logarithmic
+// stretches; pressure kappa log J / J with kappa = lambda + 2 mu / 3. Writes
+// sigma, Cp^-1 = F^-1 b_e F^-T, eps_p and V = det(dF) V. The G2P kernels that
+// call it are instantiated apart from the elastic ones.
+template <class T>
+__device__ __forceinline__ void vonmises_update(const PView<T>& P, const Scalars<T>& s, long long p,
+                                             const double (&F)[3][3], double detdF, double lam, double mu,
+                                             T* sig_out, T* V_out) {
+    const double kappa = lam + 2.0 * mu / 3.0;
+    const double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
+                     F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+                     F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+    const double lJ = log(J);
+    const double pr = kappa * lJ / J;
+    double Cp[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Cp[r][c] = double(P.Cp_inv[symidx<3>(r, c)][p]);
+    double FC[3][3], b[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += F[r][k] * Cp[k][c];
+            FC[r][c] = acc;
+        }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += FC[r][k] * F[c][k];
+            b[r][c] = acc;
+        }
+    double a[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[r][c] = 0.5 * (b[r][c] + b[c][r]);
+    double ev[3], n[3][3];
+    sym_eigen3(a, ev, n);
+    double lst[3], tau_tr[3], tt = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        lst[q] = sqrt(ev[q]);
+        tau_tr[q] = 2.0 * mu * log(lst[q]) - 2.0 * mu / 3.0 * lJ;
+        tt += tau_tr[q] * tau_tr[q];
+    }
+    const double epn = double(P.eps_p[p]);
+    const double nrm = sqrt(1.5 * tt);
+    const double ftr = nrm - (s.yield_stress + s.hardening * epn);
+    double dgam = 0.0, le[3], tau[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        le[q] = lst[q];
+        tau[q] = tau_tr[q];
+    }
+    if (ftr > 0.0) {
+        dgam = ftr / (3.0 * mu + s.hardening);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double deps = dgam * (1.5 * tau_tr[q] / nrm);
+            le[q] = exp(log(lst[q]) - deps);
+            tau[q] = tau_tr[q] - 2.0 * mu * deps;
+        }
+    }
+    double Fi[3][3];
+    Fi[0][0] = (F[1][1] * F[2][2] - F[1][2] * F[2][1]) / J;
+    Fi[0][1] = (F[0][2] * F[2][1] - F[0][1] * F[2][2]) / J;
+    Fi[0][2] = (F[0][1] * F[1][2] - F[0][2] * F[1][1]) / J;
+    Fi[1][0] = (F[1][2] * F[2][0] - F[1][0] * F[2][2]) / J;
+    Fi[1][1] = (F[0][0] * F[2][2] - F[0][2] * F[2][0]) / J;
+    Fi[1][2] = (F[0][2] * F[1][0] - F[0][0] * F[1][2]) / J;
+    Fi[2][0] = (F[1][0] * F[2][1] - F[1][1] * F[2][0]) / J;
+    Fi[2][1] = (F[0][1] * F[2][0] - F[0][0] * F[2][1]) / J;
+    Fi[2][2] = (F[0][0] * F[1][1] - F[0][1] * F[1][0]) / J;
+    // Fi n_q: Cp^-1 = sum_q le_q^2 (Fi n_q) (x) (Fi n_q)
+    double m[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) m[r][q] = Fi[r][0] * n[0][q] + Fi[r][1] * n[1][q] + Fi[r][2] * n[2][q];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) {
+            double sg = 0.0, cp = 0.0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                sg += (tau[q] / J + pr) * n[r][q] * n[c][q];
+                cp += le[q] * le[q] * m[r][q] * m[c][q];
+            }
+            P.sig[symidx<3>(r, c)][p] = T(sg);
+            if (sig_out) sig_out[symidx<3>(r, c)] = T(sg);
+            P.Cp_inv[symidx<3>(r, c)][p] = T(cp);
+        }
+    P.eps_p[p] = T(epn + dgam);
+    const T Vn = T(detdF * double(P.V[p]));
+    P.V[p] = Vn;
+    if (V_out) *V_out = Vn;
+}
+
 // FP64 particle kinematics and constitutive update (README.md:82-86):
 // F = (I + dt grad_v) F, J = det F, sigma by Neo-Hookean or the weakly
-// compressible fluid p = -K (J - 1), V = V0 J. F, J and log J stay in FP64.
+// compressible fluid p = -K (J - 1), V = V0 J; or, in 3D, the von Mises model
+// of the Taylor impact with V = det(I + dt grad_v) V (vonmises_update). F, J
+// and log J stay in FP64.
 template <int D, class T>
 __device__ __forceinline__ void load_F(const PView<T>& P, long long p, double (&F)[3][3]) {
 #pragma unroll
@@ -545,7 +781,7 @@ __device__ __forceinline__ void load_F(const PView<T>& P, long long p, double (&
 }
 
 // F is passed in (loaded early by the caller so the load overlaps the gather).
-template <int D, class T>
+template <int D, class T, bool VM = false>
 __device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars<T>& s, long long p,
                                                 const T (&gv)[3][3], const double (&F)[3][3]) {
     double Fn[3][3];
@@ -574,6 +810,20 @@ __device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars
         for (int c = 0; c < D; ++c) P.F[r + c * D][p] = Fn[r][c];
     const double mu = P.mu ? double(P.mu[p]) : s.mu;
     const double lam = P.lam ? double(P.lam[p]) : s.lam;
+    if constexpr (D == 3 && VM) {
+        {
+            double dF[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) dF[r][c] = (r == c ? 1.0 : 0.0) + double(gv[r][c]) * s.dt64;
+            const double detdF = dF[0][0] * (dF[1][1] * dF[2][2] - dF[1][2] * dF[2][1]) -
+                                 dF[0][1] * (dF[1][0] * dF[2][2] - dF[1][2] * dF[2][0]) +
+                                 dF[0][2] * (dF[1][0] * dF[2][1] - dF[1][1] * dF[2][0]);
+            vonmises_update<T>(P, s, p, Fn, detdF, lam, mu, nullptr, nullptr);
+            return;
+        }
+    }
     if (s.material == 1) {
         const double pr = lam * (J - 1.0);
 #pragma unroll

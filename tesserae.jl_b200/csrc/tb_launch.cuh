@@ -92,6 +92,11 @@ template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
                                       const unsigned char* cur, const unsigned char* prev, const LaunchCfg& cfg);
 
+// max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v| into *out
+// (the bits of a double).
+template <int D, class T>
+cudaError_t launch_wave_speed(const PView<T>& P, const Scalars<T>& s, unsigned long long* out, const LaunchCfg& cfg);
+
 template <int D, class T>
 cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
                               const LaunchCfg& cfg);

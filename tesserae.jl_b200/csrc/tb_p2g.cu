@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     const int nactive = totals[0];
     const int jk = lane % NJK, sub = lane / NJK;
     const int sj = jk % 3, sk = (D == 3) ? jk / 3 : 0;
-    const bool gimp = s.basis == TB_UGIMP;
+    const bool gimp = basis_is_gimp(s.basis);
     const SlotPoly py = slot_poly(sj), pz = slot_poly(sk);
 
     for (int g = tid; g < NG; g += NT) gcount[g] = 0;
@@ -1026,7 +1026,7 @@ cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T
                           const BinBuffers& b, const LaunchCfg& cfg) {
     KernelScope ks(cfg, "p2g");
     if constexpr (sizeof(T) == 4) {
-        if (s.basis == TB_BSPLINE_QUADRATIC) {
+        if (s.basis == TB_BSPLINE_QUADRATIC || s.basis == TB_KC_BSPLINE_QUADRATIC) {
             cudaError_t e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
             if (e != cudaSuccess) return e;
             return launch_pencil_mode<D, T, BW, X64, 2>(M, P, G, s, b, cfg);

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) node_block_kernel(DMesh<D, T> M, GView<T>
 }
 
 // Final per-particle writes of @G2P and the FP64 constitutive update.
-template <int D, class T>
+template <int D, class T, bool VM = false>
 __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& s, long long p, const T* x,
                                            const T* vp, const T* vpic, const T* dvf, const T (&gv)[3][3],
                                            const T* dxs, const T (&Bn)[3][3], const double (&F)[3][3]) {
@@ -173,11 +173,11 @@ __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& 
 #pragma unroll
         for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
     }
-    particle_update<D, T>(P, s, p, gv, F);
+    particle_update<D, T, VM>(P, s, p, gv, F);
 }
 
-template <int D, class T, int BW, bool GEN, bool X64>
-__global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 8 : 4)) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
+template <int D, class T, int BW, bool GEN, bool X64, bool VM = false>
+__global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(T) == 4 ? 8 : 4)) g2p_tile_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
                                                        const int* __restrict__ totals,
                                                        const int* __restrict__ blocklist,
                                                        const int* __restrict__ offsets,
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
                             }
                 }
             }
-            g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
+            g2p_finish<D, T, VM>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
             int nb = 0;
             if constexpr (X64) {
                 double xn[3] = {0.0, 0.0, 0.0};
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(128, GEN ? (sizeof(T) == 4 ? 4 : 2) : (sizeof(
 
 // Particle-parallel G2P reading the grid from global memory: the reference's own
 // G2P schedule (one thread per particle, gpu.jl:226-232); needs no partition.
-template <int D, class T>
+template <int D, class T, bool VM = false>
 __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
                                                          int* err) {
     const bool apic = s.transfer == TB_TRANSFER_APIC;
@@ -431,13 +431,13 @@ __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T>
                         }
                     }
         }
-        g2p_finish<D, T>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
+        g2p_finish<D, T, VM>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
     }
 }
 
 // Particles outside the mesh (block id 0): empty window, so only the particle
 // equations run (v and x keep their values under FLIP).
-template <int D, class T>
+template <int D, class T, bool VM = false>
 __global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T> s, const int* __restrict__ blockids,
                                                           const int* __restrict__ totals) {
     if ((long long)totals[1] >= P.n) return;  // every particle is inside a block
@@ -452,8 +452,29 @@ __global__ void __launch_bounds__(256) g2p_outside_kernel(PView<T> P, Scalars<T>
         }
         double F[3][3];
         load_F<D, T>(P, p, F);
-        g2p_finish<D, T>(P, s, p, x, vp, z, z, gv, z, Bn, F);
+        g2p_finish<D, T, VM>(P, s, p, x, vp, z, z, gv, z, Bn, F);
     }
+}
+
+// c = sqrt((lambda + 2 mu) / (m / V)) + |v| per particle, the Taylor impact's
+// speed for its time step (docs/src/gpu.md:283-284); the maximum goes to *out
+// as the bits of a non-negative double, which order as unsigned integers.
+template <int D, class T>
+__global__ void __launch_bounds__(256) wave_speed_kernel(PView<T> P, Scalars<T> s, unsigned long long* out) {
+    double cmax = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        const double mu = P.mu ? double(P.mu[p]) : s.mu;
+        const double lam = P.lam ? double(P.lam[p]) : s.lam;
+        const double m = P.m ? double(P.m[p]) : double(s.mass);
+        double vv = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) vv += double(P.v[d][p]) * double(P.v[d][p]);
+        const double c = sqrt((lam + 2.0 * mu) / (m / double(P.V[p]))) + sqrt(vv);
+        cmax = fmax(cmax, c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
+    if ((threadIdx.x & 31) == 0 && cmax > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(cmax));
 }
 
 // update!(weights, particles, mesh) with stored values (basis_weight.jl:714-752):
@@ -528,10 +549,17 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
     auto kern = gen ? g2p_tile_kernel<D, T, BW, true, false> : g2p_tile_kernel<D, T, BW, false, false>;
+    const bool vm = s.material == TB_MATERIAL_VONMISES;  // 3D only (checked by the caller)
+    if constexpr (D == 3) {
+        if (vm) kern = gen ? g2p_tile_kernel<D, T, BW, true, false, true> : g2p_tile_kernel<D, T, BW, false, false, true>;
+    }
     if (P.x64[0]) {  // FP64-position form: plain path, FP32 state only (checked by the caller)
         if constexpr (sizeof(T) == 4) {
             if (gen) return cudaErrorInvalidValue;
             kern = g2p_tile_kernel<D, T, BW, false, true>;
+            if constexpr (D == 3) {
+                if (vm) kern = g2p_tile_kernel<D, T, BW, false, true, true>;
+            }
         } else {
             return cudaErrorInvalidValue;
         }
@@ -542,7 +570,10 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
         // replaces with the next step's when it counts
         KernelScope ks(cfg, "g2p_outside");
         const int og = int(std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8));
-        g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
+        if (D == 3 && s.material == TB_MATERIAL_VONMISES)
+            g2p_outside_kernel<D, T, D == 3><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
+        else
+            g2p_outside_kernel<D, T><<<og, 256, 0, cfg.stream>>>(P, s, b.blockids, b.totals);
     }
     cudaError_t e = cudaSuccess;
     if (count_next) e = cudaMemsetAsync(b.counts, 0, sizeof(int) * size_t(M.nblocks), cfg.stream);
@@ -560,7 +591,10 @@ cudaError_t launch_g2p_direct(const DMesh<D, T>& M, const GView<T>& G, const PVi
     if (P.n == 0) return cudaSuccess;
     const int grid = int(std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 32));
     KernelScope ks(cfg, "g2p_direct");
-    g2p_direct_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, G, P, s, cfg.err);
+    if (D == 3 && s.material == TB_MATERIAL_VONMISES)
+        g2p_direct_kernel<D, T, D == 3><<<grid, 128, 0, cfg.stream>>>(M, G, P, s, cfg.err);
+    else
+        g2p_direct_kernel<D, T><<<grid, 128, 0, cfg.stream>>>(M, G, P, s, cfg.err);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -597,6 +631,17 @@ cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, c
 }
 
 template <int D, class T>
+cudaError_t launch_wave_speed(const PView<T>& P, const Scalars<T>& s, unsigned long long* out, const LaunchCfg& cfg) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), cfg.stream);
+    if (e != cudaSuccess || P.n == 0) return e;
+    const int grid = int(std::max<long long>(1, std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8)));
+    KernelScope ks(cfg, "wave_speed");
+    wave_speed_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(P, s, out);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <int D, class T>
 cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* gw,
                                   long long* win, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
@@ -614,7 +659,9 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
     template cudaError_t launch_update_weights<D, T>(const DMesh<D, T>&, const PView<T>&, const Scalars<T>&, \
                                                      T*, T*, long long*, const LaunchCfg&);                  \
     template cudaError_t launch_g2p_direct<D, T>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,       \
-                                                 const Scalars<T>&, const LaunchCfg&);
+                                                 const Scalars<T>&, const LaunchCfg&);                     \
+    template cudaError_t launch_wave_speed<D, T>(const PView<T>&, const Scalars<T>&, unsigned long long*,    \
+                                                 const LaunchCfg&);
 #define TB_INST_TB(D, T, BW)                                                                                 \
     template cudaError_t launch_sparse_zero<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const unsigned char*, \
                                                       const unsigned char*, const LaunchCfg&);                 \

@@ -166,6 +166,34 @@ def step(grid: Grid, particles: Particles, partition: Partition, mesh: Cartesian
     ctx.check(rc, "step")
 
 
+def max_wave_speed(particles: Particles, params, ctx: Context | None = None) -> float:
+    """max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v|, reduced
+    on the device (the speed of the Taylor impact's time step)."""
+    ctx = ctx or _default()
+    out = C.c_double()
+    fn = ctx.fn("tb_max_wave_speed", particles.dtype)
+    ctx.check(fn(ctx.ptr, int(particles.dim), _ref(particles.struct()), _ref(params), C.byref(out)),
+              "max_wave_speed")
+    return float(out.value)
+
+
+def adaptive_steps(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+                   nsteps: int, cfl: float = 0.8, ctx: Context | None = None) -> float:
+    """`nsteps` steps of the Taylor impact's loop (docs/src/gpu.md:281-360):
+    each step takes dt = cfl h / max c from the particles' current state
+    (max_wave_speed, one device reduction and host read per step, as the
+    reference's `maximum(particles.c)`), then runs one step. Returns the time
+    advanced."""
+    ctx = ctx or _default()
+    prm = type(params).from_buffer_copy(params)
+    t = 0.0
+    for _ in range(int(nsteps)):
+        prm.dt = cfl * mesh.h / max_wave_speed(particles, prm, ctx=ctx)
+        step(grid, particles, partition, mesh, prm, 1, ctx=ctx)
+        t += prm.dt
+    return t
+
+
 def reorder_particles(particles: Particles, partition: Partition, threshold: float = 1.0,
                       ctx: Context | None = None) -> bool:
     """reorder_particles!(particles, partition; threshold) (src/Parallel/gpu_block_strategy.jl:194-202):

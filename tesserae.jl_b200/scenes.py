@@ -11,6 +11,9 @@ Scenes:
   clusters3d 3D 512^3, 64 Gaussian clusters, lognormal masses (32M particles)
   sphere3d   3D 64^3 sphere r=0.3, jittered 4^3 per cell (the differentiable rollout)
   dambreak3d 3D 384^3 column [0,0.4]x[0,1]x[0,0.8], 2^3 per cell, WLS(uGIMP) + APIC fluid
+  taylor3d   3D Taylor impact of docs/src/gpu.md:202-392: copper rod at 227 m/s onto a
+             slip floor, KernelCorrection(BSpline(Quadratic())), von Mises plasticity,
+             adaptive time step (~1.48M particles)
 Each takes a `scale` that shrinks the mesh (cells per axis divided by `scale`,
 spacing kept) so tests run the same physics at sizes the oracle finishes fast.
 """
@@ -24,7 +27,7 @@ from . import _abi
 from .state import CartesianMesh, Particles, lame, step_params
 
 SEEDS = {"readme2d": 0, "cube3d": 20260001, "clusters3d": 20260002, "sphere3d": 20260003,
-         "dambreak3d": 20260004}
+         "dambreak3d": 20260004, "taylor3d": 20260005}
 
 
 @dataclass
@@ -216,3 +219,56 @@ def dambreak3d(scale: int = 1) -> Scene:
 
 SCENES = {"readme2d": readme2d, "cube3d": cube3d, "clusters3d": clusters3d, "sphere3d": sphere3d,
           "dambreak3d": dambreak3d}
+
+
+def taylor3d(scale: int = 1, seed: int | None = None) -> Scene:
+    """The Taylor impact of docs/src/gpu.md:202-392: rod R = 3.2 mm, L = 32.4 mm
+    at (0, 0, -227) m/s onto a slip floor (the node layer z = 0 keeps no normal
+    velocity), mesh spacing R/12 over (-3R, 3R)^2 x (0, 1.1 L) (the upper bound
+    expanded to whole cells as CartesianMesh does), E = 117 GPa, nu = 0.35,
+    rho0 = 8.93e3, von Mises with H = 0.1 GPa and tau_y0 = 0.4 GPa,
+    KernelCorrection(BSpline(Quadratic())) weights, FLIP transfer, CFL 0.8 on
+    c = sqrt((lambda + 2 mu) / rho) + |v|, up to t = 80 us (about 1.8k steps).
+    Particles: the reference samples the rod's block of grid nodes with
+    PoissonDiskSampling(spacing = 1/3) (a third-party algorithm not in the
+    reference tree); the stand-in is a lattice of the same spacing (3 per cell
+    per axis) jittered by U[-l/4, l/4], which gives the same count (1.48 M after
+    the cylinder filter). V = block volume / particles before the filter, as the
+    reference sets it. `scale` multiplies the spacing (same rod, 1/scale^3 of the
+    particles)."""
+    R, L = 0.0032, 0.0324
+    h = R / 12 * scale
+    mesh = CartesianMesh(h, (-3 * R, 3 * R), (-3 * R, 3 * R), (0.0, L + 0.1 * L))
+    rng = np.random.default_rng(SEEDS["taylor3d"] if seed is None else seed)
+    # extract(grid.x, (-R,R), (-R,R), (0,L)): the nodes inside the box
+    zmax = np.floor(L / h + 1e-9) * h
+    l = h / 3
+    axx = grid_sampling_axis(-R, R, h, spacing=1 / 3)
+    axz = grid_sampling_axis(0.0, zmax, h, spacing=1 / 3)
+    pts = _lattice([axx, axx, axz])
+    npre = pts.shape[1]
+    Vp = (2 * R) * (2 * R) * zmax / npre
+    pts = pts + rng.uniform(-l / 4, l / 4, size=pts.shape)
+    pts = pts[:, pts[0] ** 2 + pts[1] ** 2 < R * R]
+    n = pts.shape[1]
+    P = Particles(n, 3, np.float64, optional=("eps_p", "Cp_inv"))
+    P.x[...] = pts
+    P.V[...] = Vp
+    P.v[2] = -227.0
+    E, nu, rho0 = 117e9, 0.35, 8.93e3
+    mu, lam = lame(E, nu)
+    prm = step_params(0.0, mass=rho0 * Vp, V0=Vp, mu=mu, lam=lam, basis=_abi.TB_KC_BSPLINE_QUADRATIC,
+                      material=_abi.MATERIAL_VONMISES, wall_mask=1 << 4, wall_layers=1,
+                      hardening=0.1e9, yield_stress=0.4e9)
+    prm.dt = taylor_dt(P.v, P.V, prm.mass, mu, lam, h)
+    return Scene("taylor3d", mesh, P, prm, 1805, {"E": E, "nu": nu, "rho0": rho0, "CFL": 0.8,
+                                                 "t_stop": 80e-6, "n_before_filter": npre})
+
+
+def taylor_dt(v, V, mass, mu, lam, h, cfl=0.8) -> float:
+    """The Taylor impact's time step (docs/src/gpu.md:283-284): CFL h / max c with
+    c = sqrt((lambda + 2 mu) / (m / V)) + |v| over the particles (host arrays)."""
+    c = np.sqrt((lam + 2 * mu) / (mass / np.asarray(V, dtype=np.float64))) + np.linalg.norm(
+        np.asarray(v, dtype=np.float64), axis=0)
+    return float(cfl * h / np.max(c))
+

@@ -108,7 +108,8 @@ def test_bin_2d_and_empty(tb, oracle, ctx):
 # basis weights
 # ---------------------------------------------------------------------------
 
-@pytest.mark.parametrize("basis", ["bspline_quadratic", "ugimp", "wls_bspline_quadratic", "wls_ugimp"])
+@pytest.mark.parametrize("basis", ["bspline_quadratic", "ugimp", "wls_bspline_quadratic", "wls_ugimp",
+                                   "kc_bspline_quadratic", "kc_ugimp"])
 @pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 2e-5)])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_update_weights(tb, oracle, ctx, basis, dtype, tol, dim):
