@@ -629,13 +629,18 @@ struct PencilShape {
 
 // MODE 0: every block with the full record; 1: compact records, interior
 // blocks only (their halo tile lies inside the mesh, so no window is
-// truncated); 2: full records, the other blocks only.
+// truncated), appending every other block it meets to `bnd` (count in
+// `bnd_count`, zeroed before); 2: full records, the blocks of that list, one
+// per CTA at a time (the boundary blocks of a scene can all sit in one stretch
+// of the block list, e.g. a body standing on the mesh floor).
 template <int D, class T, int BW, int NR, bool X64, int MODE>
 __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ? 2 : 1)) p2g_pencil_kernel(DMesh<D, T> M, PView<T> P, GView<T> G, Scalars<T> s,
                                                                     const int* __restrict__ totals,
                                                                     const int* __restrict__ blocklist,
                                                                     const int* __restrict__ offsets,
-                                                                    const int* __restrict__ perm, int* err) {
+                                                                    const int* __restrict__ perm, int* err,
+                                                                    int* __restrict__ bnd,
+                                                                    unsigned long long* __restrict__ bnd_count) {
     using SH = PencilShape<D, BW>;
     constexpr int NT = P2G_THREADS;
     constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
@@ -963,28 +968,16 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     };
 
     if constexpr (MODE == 2) {
-        // The boundary blocks are few: each CTA tests NT block-list entries at
-        // once and keeps the boundary ones in a shared list, instead of one
-        // dependent load per skipped block.
-        __shared__ int blist[NT];
-        __shared__ int bcount;
-        for (int c0 = blockIdx.x * NT; c0 < nactive; c0 += gridDim.x * NT) {
-            if (tid == 0) bcount = 0;
-            __syncthreads();
-            if (c0 + tid < nactive) {
-                const int b = blocklist[c0 + tid] - 1;
-                if (!interior_block(b)) blist[atomicAdd(&bcount, 1)] = b;
-            }
-            __syncthreads();
-            const int nlist = bcount;
-            for (int q = 0; q < nlist; ++q) process_block(blist[q]);
-            __syncthreads();
-        }
+        const int nlist = int(*bnd_count);
+        for (int q = blockIdx.x; q < nlist; q += gridDim.x) process_block(bnd[q]);
     } else {
         for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
             const int b = blocklist[bi] - 1;
             if constexpr (MODE == 1) {
-                if (!interior_block(b)) continue;  // the boundary kernel's block (uniform over the CTA)
+                if (!interior_block(b)) {  // the boundary launch's block (uniform over the CTA)
+                    if (tid == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
+                    continue;
+                }
             }
             process_block(b);
         }
@@ -1013,7 +1006,10 @@ cudaError_t launch_pencil_mode(const DMesh<D, T>& M, const PView<T>& P, const GV
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2G_THREADS, smem);
     const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
-    kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    // the boundary-block list lives in binning scratch that is free until the
+    // next binning: cursors (one int per block) and the first scan partial
+    kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,
+                                                 b.cursors, b.partials);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -1027,7 +1023,9 @@ cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T
     KernelScope ks(cfg, "p2g");
     if constexpr (sizeof(T) == 4) {
         if (s.basis == TB_BSPLINE_QUADRATIC || s.basis == TB_KC_BSPLINE_QUADRATIC) {
-            cudaError_t e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
+            cudaError_t e = cudaMemsetAsync(b.partials, 0, sizeof(unsigned long long), cfg.stream);
+            if (e != cudaSuccess) return e;
+            e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
             if (e != cudaSuccess) return e;
             return launch_pencil_mode<D, T, BW, X64, 2>(M, P, G, s, b, cfg);
         }
