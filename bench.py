@@ -234,6 +234,66 @@ def active_nodes(mesh, particles_np) -> int:
     return int(mask.sum())
 
 
+# The reference's published GPU numbers for the Taylor impact
+# (docs/src/gpu.md:215-220): 1.48M particles, 1.8k steps, RTX 5090.
+TAYLOR_PUBLISHED = {"fp64": 1.48e6 * 1.8e3 / 31.0, "fp32": 1.48e6 * 1.8e3 / 8.0}
+
+
+def taylor_leg(tb, runtime, ctx, steps: int = 200, warmup: int = 5, cpu_steps: int = 2) -> dict:
+    """The Taylor impact of docs/src/gpu.md:202-392 at full size (1.48 M
+    particles, KernelCorrection(BSpline(Quadratic())), von Mises, slip floor):
+    `steps` steps of its adaptive loop (each takes dt = 0.8 h / max c from a
+    device reduction read back on the host, as the reference's
+    `maximum(particles.c)`, then runs one step) after `warmup` steps, timed
+    between CUDA events, in each precision form; against the reference's
+    published RTX 5090 throughput of the same loop. Also the oracle port's FP64
+    step on the host cores over `cpu_steps` steps."""
+    import torch
+    sc = tb.scenes.taylor3d()
+    mesh, prm, host = sc.mesh, sc.params, sc.particles
+    n = host.n
+    out = {"workload": f"Taylor impact (docs/src/gpu.md:202-392): {n} particles, mesh "
+                       f"{'x'.join(str(k) for k in mesh.n_nodes)} nodes (h = R/12), KernelCorrection(BSpline(Quadratic())), "
+                       "von Mises (H = 0.1 GPa, tau_y0 = 0.4 GPa), 227 m/s onto a slip floor, dt = 0.8 h / max c per step",
+           "n_particles": n, "steps": steps, "warmup": warmup, "unit": "particle-steps/s",
+           "published_rtx5090": TAYLOR_PUBLISHED,
+           "note": "each step includes its wave-speed reduction and the host read of max c"}
+    for name, dtype, x64 in (("fp64", np.float64, False), ("fp32", np.float32, False),
+                             ("fp32_x64", np.float32, True)):
+        P = host.to("torch", device="cuda", dtype=dtype, x64=x64)
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.adaptive_steps(G, P, part, mesh, prm, warmup, ctx=ctx)
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t_sim = runtime.adaptive_steps(G, P, part, mesh, prm, steps, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        d = P.numpy()
+        out[name] = {"value": n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "simulated_us": (t_sim * 1e6), "plastic_particles": int(np.sum(d["eps_p"] > 0)),
+                     "max_eps_p": float(np.max(d["eps_p"])), "finite": bool(np.isfinite(d["x"]).all()),
+                     "full_run_s_1805_steps": 1805 * ms * 1e-3 / steps}
+        ref = TAYLOR_PUBLISHED["fp64" if name == "fp64" else "fp32"]
+        out[name]["over_published_rtx5090"] = out[name]["value"] / ref
+        del P, part, G
+        torch.cuda.empty_cache()
+    if cpu_steps > 0:
+        orc = load_oracle(tb).Oracle(tb._abi)
+        Pc = host.to("numpy")
+        Gc = tb.generate_grid(mesh)
+        prm1 = type(prm).from_buffer_copy(prm)
+        orc.step_parallel(mesh, Pc, Gc, prm1, 1)
+        t0 = time.perf_counter()
+        orc.step_parallel(mesh, Pc, Gc, prm1, cpu_steps)
+        cs = time.perf_counter() - t0
+        out["cpu_port"] = {"value": n * cpu_steps / cs, "cores": orc.max_threads(),
+                           "sample": f"{cpu_steps} FP64 steps after 1 warm-up, OpenMP colour-phased restatement"}
+    return out
+
+
 def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions: int = 2) -> dict:
     """Differentiable rollout on the sphere scene (64^3 cells, ~1.9M particles,
     200 steps, checkpoint every 20), mixed FP32 form with FP32 positions (the
@@ -388,6 +448,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rollout leg")
     ap.add_argument("--adj-scale", type=int, default=1, help="shrink the sphere scene of the adjoint leg")
+    ap.add_argument("--no-taylor", action="store_true", help="skip the Taylor impact leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed FP32 leg (for profiler captures); prints a reduced line")
     args = ap.parse_args()
@@ -524,6 +585,7 @@ def main():
     del hostp
 
     adjoint = None if args.no_adjoint else adjoint_leg(tb, runtime, ctx, scale=args.adj_scale)
+    taylor = None if (args.no_taylor or rank != 0) else taylor_leg(tb, runtime, ctx)
 
     if rank != 0:
         if dist is not None:
@@ -585,6 +647,7 @@ def main():
                            "form": FORMS["f32"][2], "accuracy": acc_f32},
         "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
         "adjoint_over_forward": adjoint,
+        "taylor_impact": taylor,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_active_node": per_n,
