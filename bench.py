@@ -234,9 +234,10 @@ def active_nodes(mesh, particles_np) -> int:
     return int(mask.sum())
 
 
-# The reference's published GPU numbers for the Taylor impact
-# (docs/src/gpu.md:215-220): 1.48M particles, 1.8k steps, RTX 5090.
-TAYLOR_PUBLISHED = {"fp64": 1.48e6 * 1.8e3 / 31.0, "fp32": 1.48e6 * 1.8e3 / 8.0}
+# The reference's published GPU numbers for the Taylor impact on an RTX 5090
+# (docs/src/gpu.md:215-220: 31 s FP64, 8 s FP32), as particle-steps/s with the
+# tutorial's 1 472 942 particles and 1 833 steps (taylor_impact.jl:84, 265-267).
+TAYLOR_PUBLISHED = {"fp64": 1472942 * 1833 / 31.0, "fp32": 1472942 * 1833 / 8.0}
 
 
 def taylor_leg(tb, runtime, ctx, steps: int = 200, warmup: int = 5, cpu_steps: int = 2) -> dict:
