@@ -578,10 +578,11 @@ def main():
         runtime.rollout_host(hostp, mesh, prm, S, ctx=ctx)
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    fbytes = hostp.x.nbytes + hostp.v.nbytes + hostp.V.nbytes + hostp.grad_v.nbytes + hostp.sigma.nbytes + \
-        hostp.F.nbytes
-    e2e = {"value": world * n * S * calls / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": fbytes,
-           "d2h_bytes_per_step": fbytes, "mpm_steps_per_call": S,
+    # in: x, v, V, sigma, F (the step's inputs); out: the same and grad_v (written by every G2P)
+    in_bytes = hostp.x.nbytes + hostp.v.nbytes + hostp.V.nbytes + hostp.sigma.nbytes + hostp.F.nbytes
+    out_bytes = in_bytes + hostp.grad_v.nbytes
+    e2e = {"value": world * n * S * calls / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": in_bytes,
+           "d2h_bytes_per_step": out_bytes, "mpm_steps_per_call": S,
            "note": "one bench step = one tb_rollout_host_f32x64 call on pinned host buffers (H2D, S steps, D2H)"}
     del hostp
 

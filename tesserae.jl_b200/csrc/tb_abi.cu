@@ -618,19 +618,23 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     const long long nb = mesh_nblocks(m);
     // Fields moved: x, v, V, grad_v, sigma (T); F (double); optional m, l, B, V0, mu, lambda (T), and the
     // von Mises state eps_p, Cp_inv (T, in and out).
+    // in: copied to the device before the steps; out: copied back after them.
+    // grad_v is written for every particle by every G2P and read by no step, so
+    // it is copied out only.
     struct Field {
         void** host_slot;
         size_t elem;
         bool inout;
+        bool in = true;
     };
     std::vector<Field> fields;
-    auto add = [&](void** slot, size_t elem, bool inout) {
-        if (*slot) fields.push_back({slot, elem, inout});
+    auto add = [&](void** slot, size_t elem, bool inout, bool in = true) {
+        if (*slot) fields.push_back({slot, elem, inout, in});
     };
     for (int d = 0; d < D; ++d) add(&host->x[d], x64 ? sizeof(double) : sizeof(T), true);
     for (int d = 0; d < D; ++d) add(&host->v[d], sizeof(T), true);
     add(&host->V, sizeof(T), true);
-    for (int k = 0; k < D * D; ++k) add(&host->grad_v[k], sizeof(T), true);
+    for (int k = 0; k < D * D; ++k) add(&host->grad_v[k], sizeof(T), true, nsteps == 0);
     for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&host->sigma[k], sizeof(T), true);
     for (int k = 0; k < D * D; ++k) add(&host->F[k], sizeof(double), true);
     if (apic)
@@ -719,8 +723,9 @@ int do_rollout(tb_ctx* c, const tb_mesh* m, tb_particles* host, const tb_step_pa
     part.nblocks = nb;
     cudaError_t e = cudaSuccess;
     for (size_t i = 0; i < fields.size() && e == cudaSuccess; ++i)
-        e = cudaMemcpyAsync(dptr[i], *fields[i].host_slot, fields[i].elem * size_t(n), cudaMemcpyHostToDevice,
-                            c->stream);
+        if (fields[i].in)
+            e = cudaMemcpyAsync(dptr[i], *fields[i].host_slot, fields[i].elem * size_t(n), cudaMemcpyHostToDevice,
+                                c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "rollout H2D");
     rc = dispatch_step<T>(c, m, &dev, &part, &g, prm, nsteps, true, true, true, true, x64);
     if (rc != TB_OK) return rc;
