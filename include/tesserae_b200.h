@@ -285,6 +285,22 @@ int32_t tb_step_reorder_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* part
 int32_t tb_step_reorder_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                                tb_grid* grid, const tb_step_params* params, int32_t nsteps, double threshold);
 
+/* @G2P2G (src/Transfer/g2p2g.jl:98-159) for the FLIP/PIC equation set of the
+ * plain step: one pass doing each particle's G2P (README.md:79-86) and then its
+ * P2G of m, mv, f (README.md:72-74, zeroed first) with the weights of the
+ * position the particle had before the G2P half moved it (the reference binds
+ * one support window for both halves, g2p2g.jl:103-106); the P2G half reads the
+ * updated v, sigma and V; the grid half (README.md:75-76, walls) follows. The
+ * particles are binned into `partition` at their positions on entry. APIC is
+ * refused (TB_ERR_UNSUPPORTED); the _f32x64 form takes FP64 positions as
+ * tb_step_f32x64 does. Asynchronous on the context's stream. */
+int32_t tb_g2p2g_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                     tb_grid* grid, const tb_step_params* params);
+int32_t tb_g2p2g_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                     tb_grid* grid, const tb_step_params* params);
+int32_t tb_g2p2g_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                        tb_grid* grid, const tb_step_params* params);
+
 /* ---- host-buffer rollout (end-to-end form of tb_step_*) ----------------
  * `host` holds HOST pointers (pinned memory recommended) for the particle state;
  * the context stages it into its own device buffers, runs `nsteps` steps and

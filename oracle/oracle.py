@@ -41,6 +41,7 @@ def lib(abi):
         "tbo_p2g": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid), P(abi.tb_step_params)],
         "tbo_grid_update": [C.c_int, P(abi.tb_mesh), P(abi.tb_grid), P(abi.tb_step_params)],
         "tbo_g2p": [C.c_int, P(abi.tb_mesh), P(abi.tb_grid), P(abi.tb_particles), P(abi.tb_step_params)],
+        "tbo_g2p2g": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid), P(abi.tb_step_params)],
         "tbo_step": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid), P(abi.tb_step_params),
                      C.c_int],
         "tbo_step_parallel": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid),
@@ -104,6 +105,10 @@ class Oracle:
     def g2p(self, mesh, grid, particles, params):
         _check(self.L.tbo_g2p(_prec(particles.dtype), C.byref(mesh.struct()), C.byref(grid.struct()),
                               C.byref(particles.struct()), C.byref(params)), "g2p")
+
+    def g2p2g(self, mesh, particles, grid, params):
+        _check(self.L.tbo_g2p2g(_prec(particles.dtype), C.byref(mesh.struct()), C.byref(particles.struct()),
+                                C.byref(grid.struct()), C.byref(params)), "g2p2g")
 
     def step(self, mesh, particles, grid, params, nsteps=1):
         _check(self.L.tbo_step(_prec(particles.dtype), C.byref(mesh.struct()), C.byref(particles.struct()),

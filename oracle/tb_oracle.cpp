@@ -79,6 +79,36 @@ int do_step(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params*
     return TB_OK;
 }
 
+// @G2P2G (src/Transfer/g2p2g.jl:98-159) for the FLIP/PIC equation set: one
+// pass over the particles, each doing its G2P and then its P2G with the weights
+// bound to the position it had before the G2P half moved it (g2p2g.jl:103-106);
+// the P2G half reads the updated v, sigma and V. Its assigned targets m, mv, f
+// are zeroed first, and the grid half of README.md:75-76 runs after the pass
+// (G2P2G_halves, g2p2g.jl:14-18).
+template <int D, class T>
+int do_g2p2g(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm) {
+    if (prm->transfer != TB_TRANSFER_FLIP) return TB_ERR_UNSUPPORTED;
+    auto M = make_mesh<D, T>(*m);
+    zero_p2g_targets(M, *g);
+    T* gmv[3] = {nullptr, nullptr, nullptr};
+    T* gf[3] = {nullptr, nullptr, nullptr};
+    for (int d = 0; d < D; ++d) {
+        gmv[d] = P<T>(g->mv[d]);
+        gf[d] = P<T>(g->f[d]);
+    }
+    for (int64_t i = 0; i < p->n; ++i) {
+        T x0[3] = {T(0), T(0), T(0)};
+        for (int d = 0; d < D; ++d) x0[d] = CP<T>(p->x[d])[i];
+        g2p_particle<D, T>(M, *g, *p, *prm, i);
+        ParticleIn<D, T> q;
+        load_particle<D, T>(*p, *prm, i, q);
+        for (int d = 0; d < D; ++d) q.x[d] = x0[d];
+        p2g_particle<D, T, void>(M, *prm, q, P<T>(g->m), gmv, gf);
+    }
+    grid_update<D, T>(M, *g, *prm);
+    return TB_OK;
+}
+
 // Multithreaded step following the reference CPU path: partition update with
 // per-thread histograms (cpu_block_strategy.jl:89-190), colour-phased block
 // scatter (region.jl:212-256), parallel grid half and parallel G2P
@@ -220,6 +250,10 @@ int tbo_grid_update(int prec, const tb_mesh* m, tb_grid* g, const tb_step_params
 
 int tbo_g2p(int prec, const tb_mesh* m, const tb_grid* g, tb_particles* p, const tb_step_params* prm) {
     TBO_DISPATCH(do_g2p, m, g, p, prm);
+}
+
+int tbo_g2p2g(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm) {
+    TBO_DISPATCH(do_g2p2g, m, p, g, prm);
 }
 
 int tbo_step(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm, int nsteps) {

@@ -152,6 +152,9 @@ SIGNATURES += [
     ("tb_rollout_host_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
     ("tb_particle_contiguity", I32, [VP, P(tb_partition), I64, P(C.c_double)]),
     ("tb_max_wave_speed_f64", I32, [VP, I32, P(tb_particles), P(tb_step_params), P(C.c_double)]),
+    ("tb_g2p2g_f64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params)]),
+    ("tb_g2p2g_f32", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params)]),
+    ("tb_g2p2g_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params)]),
     ("tb_max_wave_speed_f32", I32, [VP, I32, P(tb_particles), P(tb_step_params), P(C.c_double)]),
 ]
 for _p in ("f64", "f32", "f32x64"):

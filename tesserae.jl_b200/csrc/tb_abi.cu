@@ -103,6 +103,8 @@ struct tb_ctx {
     double* adj_grid = nullptr;
     long long adj_grid_cap = 0;
     double* adj_coef = nullptr;
+    char* g2p2g_x = nullptr;  // tb_g2p2g_*: the new positions until the P2G half has run
+    long long g2p2g_x_cap = 0;
     long long adj_coef_cap = 0;
     // checkpoint tape: states at steps 0, K, 2K, ... and one segment of K states
     char* tape_cp = nullptr;
@@ -762,6 +764,75 @@ int do_wave_speed(tb_ctx* c, int32_t dim, const tb_particles* p, const tb_step_p
     return TB_OK;
 }
 
+// @G2P2G for the FLIP/PIC equation set (src/Transfer/g2p2g.jl:98-159): the
+// particles are binned at their current positions; G2P runs with its new
+// positions going to context scratch, so the P2G half (m, mv, f, zeroed first)
+// still weighs every particle at the position it had before the G2P half
+// moved it, as the reference binds one support window for both halves
+// (g2p2g.jl:103-106), and reads the updated v, sigma, V; the grid half follows;
+// the new positions then replace x.
+template <int D, class T, int BW>
+int g2p2g_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+               const tb_step_params* prm, bool x64) {
+    const auto M = make_dmesh<D, T>(*m);
+    const auto S = make_scalars<T>(*prm);
+    PView<T> P;
+    GView<T> G;
+    int rc;
+    if ((rc = make_pview<T>(c, p, D, true, false, P, x64, prm->material)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    BinBuffers B;
+    if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
+    if ((rc = touched_buffers(c, M.nblocks)) != TB_OK) return rc;
+    const size_t xe = x64 ? sizeof(double) : sizeof(T);
+    cudaError_t e = grow(c->g2p2g_x, c->g2p2g_x_cap,
+                         std::max<long long>(1, P.n) * D * (long long)xe);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc g2p2g positions");
+    const LaunchCfg cfg = cfg_of(c);
+    char* xs = c->g2p2g_x;
+    PView<T> Pg = P;  // G2P's view: new positions to the scratch, which starts as x
+    for (int d = 0; d < D && e == cudaSuccess; ++d) {
+        void* dst = xs + size_t(d) * size_t(P.n) * xe;
+        const void* src = x64 ? static_cast<const void*>(P.x64[d]) : static_cast<const void*>(P.x[d]);
+        e = cudaMemcpyAsync(dst, src, size_t(P.n) * xe, cudaMemcpyDeviceToDevice, c->stream);
+        if (x64) Pg.x64_out[d] = static_cast<double*>(dst);
+        else Pg.x_out[d] = static_cast<T*>(dst);
+    }
+    if (e == cudaSuccess) {
+        const T* xsrc[3] = {P.x[0], P.x[1], D == 3 ? P.x[2] : P.x[1]};
+        const auto M64 = make_dmesh<D, double>(*m);
+        const double* xs64[3] = {P.x64[0], P.x64[1], D == 3 ? P.x64[2] : P.x64[1]};
+        e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xsrc, P.n, B, cfg);
+    }
+    c->grid_sparse_ok = false;  // dense zero and grid half, as the first step of a call
+    if (e == cudaSuccess) e = launch_g2p<D, T, BW>(M, G, Pg, S, B, cfg, false);
+    if (e == cudaSuccess) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
+    if (e == cudaSuccess) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
+    for (int d = 0; d < D && e == cudaSuccess; ++d) {
+        void* dst = x64 ? static_cast<void*>(P.x64[d]) : static_cast<void*>(P.x[d]);
+        e = cudaMemcpyAsync(dst, xs + size_t(d) * size_t(P.n) * xe, size_t(P.n) * xe, cudaMemcpyDeviceToDevice,
+                            c->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "g2p2g");
+    return TB_OK;
+}
+
+template <class T>
+int dispatch_g2p2g(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                   const tb_step_params* prm, bool x64) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    if ((rc = check_params(c, prm)) != TB_OK) return rc;
+    if (prm->transfer != TB_TRANSFER_FLIP)
+        return fail(c, TB_ERR_UNSUPPORTED, "g2p2g runs the FLIP/PIC equation set only");
+    if (x64 && (prm->basis == TB_WLS_BSPLINE_QUADRATIC || prm->basis == TB_WLS_UGIMP))
+        return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs the B-spline / uGIMP step only");
+    if (m->dim == 3) return g2p2g_impl<3, T, 4>(c, m, p, part, g, prm, x64);
+    if (m->block_log2 == 3) return g2p2g_impl<2, T, 8>(c, m, p, part, g, prm, x64);
+    return g2p2g_impl<2, T, 4>(c, m, p, part, g, prm, x64);
+}
+
 // ---------------------------------------------------------------------------
 // reverse mode
 // ---------------------------------------------------------------------------
@@ -1081,6 +1152,7 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->touched_prev);
     cudaFree(c->adj_grid);
     cudaFree(c->adj_coef);
+    cudaFree(c->g2p2g_x);
     cudaFree(c->tape_cp);
     cudaFree(c->tape_seg);
     cudaFree(c->ro_scratch);
@@ -1198,6 +1270,19 @@ int32_t tb_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
 int32_t tb_step_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
                        const tb_step_params* prm, int32_t nsteps) {
     return dispatch_step<float>(c, m, p, part, g, prm, nsteps, true, true, true, true, true);
+}
+
+int32_t tb_g2p2g_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                     const tb_step_params* prm) {
+    return dispatch_g2p2g<double>(c, m, p, part, g, prm, false);
+}
+int32_t tb_g2p2g_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                     const tb_step_params* prm) {
+    return dispatch_g2p2g<float>(c, m, p, part, g, prm, false);
+}
+int32_t tb_g2p2g_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                        const tb_step_params* prm) {
+    return dispatch_g2p2g<float>(c, m, p, part, g, prm, true);
 }
 
 int32_t tb_step_reorder_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,

@@ -80,6 +80,10 @@ struct PView {
     const T* lam;
     T* eps_p;      // von Mises: equivalent plastic strain
     T* Cp_inv[6];  // von Mises: inverse plastic right Cauchy-Green tensor (symmetric)
+    // Where G2P stores the new positions when they must not replace x yet
+    // (G2P2G: its P2G half weighs at the old ones); NULL = in place.
+    T* x_out[3];
+    double* x64_out[3];
 };
 
 template <class T>

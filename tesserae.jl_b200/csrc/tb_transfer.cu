@@ -171,7 +171,7 @@ __device__ __forceinline__ void g2p_finish(const PView<T>& P, const Scalars<T>& 
         for (int c = 0; c < D; ++c) P.gv[r + c * D][p] = gv[r][c];
     if (P.x[0]) {  // the FP64-position form writes x itself
 #pragma unroll
-        for (int d = 0; d < D; ++d) P.x[d][p] = x[d] + dxs[d];
+        for (int d = 0; d < D; ++d) (P.x_out[0] ? P.x_out[d] : P.x[d])[p] = x[d] + dxs[d];
     }
     particle_update<D, T, VM>(P, s, p, gv, F);
 }
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
                     xn[d] = xd[d] + double(dxs[d]);
-                    P.x64[d][p] = xn[d];
+                    (P.x64_out[0] ? P.x64_out[d] : P.x64[d])[p] = xn[d];
                 }
                 if (next_bid) nb = findblock_x64<D, T>(M, xn);
             } else {

@@ -166,6 +166,17 @@ def step(grid: Grid, particles: Particles, partition: Partition, mesh: Cartesian
     ctx.check(rc, "step")
 
 
+def g2p2g(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
+          ctx: Context | None = None):
+    """@G2P2G (src/Transfer/g2p2g.jl) for the FLIP/PIC equation set: each
+    particle's G2P, then its P2G of m, mv, f with the weights of its position
+    before the G2P moved it, then the grid half; binned into `partition` first."""
+    ctx = ctx or _default()
+    rc = ctx.pfn("tb_g2p2g", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params))
+    ctx.check(rc, "g2p2g")
+
+
 def max_wave_speed(particles: Particles, params, ctx: Context | None = None) -> float:
     """max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v|, reduced
     on the device (the speed of the Taylor impact's time step)."""
