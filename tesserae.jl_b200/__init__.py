@@ -8,10 +8,10 @@ calls the CUDA kernels through the C ABI declared in include/tesserae_b200.h.
 from . import _abi
 from .state import (Adjoint, BasisWeights, CartesianMesh, Grid, Particles, Partition, generate_basis_weights,
                     generate_grid, lame, step_params)
-from . import scenes
+from . import export, scenes
 
 __all__ = ["_abi", "Adjoint", "BasisWeights", "CartesianMesh", "Grid", "Particles", "Partition", "generate_basis_weights",
-           "generate_grid", "lame", "step_params", "scenes"]
+           "generate_grid", "lame", "step_params", "scenes", "export"]
 
 
 def __getattr__(name):
