@@ -5,8 +5,9 @@
 //      v = vn + dt f / m guarded by m != 0, then the slip-wall slices.
 // G2P  (src/Transfer/gpu.jl:226-232, README.md:79-86): one CTA per non-empty
 //      block stages the block's (v, v - vn) tile in shared memory and gathers
-//      for each particle of the block; particles outside the mesh (empty window)
-//      are updated by a particle-parallel pass.
+//      for each particle of the block (3D FP32: packed FP32x2 FMAs over the
+//      component pairs of a node-major tile); particles outside the mesh (empty
+//      window) are updated by a particle-parallel pass.
 #include "tb_launch.cuh"
 
 namespace tb {
@@ -184,9 +185,27 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
                                                        const int* __restrict__ perm, int* err,
                                                        int* __restrict__ next_bid, int* __restrict__ next_count) {
     constexpr int TS = Tile<D, BW>::TS, TN = Tile<D, BW>::TN;
-    // Component-major tile: v_r at [r TN + t], dv_r = (v - vn)_r at [(D + r) TN + t];
-    // lanes reading different nodes hit different banks.
-    __shared__ T tile[2 * D * TN];
+    // 3D FP32: node-major, (v_x, v_y, v_z, dv_x) as a float4 at [t] and (dv_y, dv_z)
+    // as a float2 after the TN float4s, dv = v - vn: two vector loads per node,
+    // whose halves feed packed FP32x2 FMAs. Otherwise component-major: v_r at
+    // [r TN + t], dv_r at [(D + r) TN + t]; lanes reading different nodes hit
+    // different banks.
+    constexpr bool VEC = (D == 3 && sizeof(T) == 4);
+    __shared__ __align__(16) T tile[2 * D * TN];
+    auto node_vals = [&](int t, T (&vi)[3], T (&dvi)[3]) {
+        if constexpr (VEC) {
+            const float4 a = reinterpret_cast<const float4*>(tile)[t];
+            const float2 c = reinterpret_cast<const float2*>(tile + 4 * TN)[t];
+            vi[0] = a.x; vi[1] = a.y; vi[2] = a.z;
+            dvi[0] = a.w; dvi[1] = c.x; dvi[2] = c.y;
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                vi[d] = tile[d * TN + t];
+                dvi[d] = tile[(D + d) * TN + t];
+            }
+        }
+    };
     const int nactive = totals[0];
     const int tid = threadIdx.x, nth = blockDim.x;
     const bool apic = s.transfer == TB_TRANSFER_APIC;
@@ -215,12 +234,22 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
             }
 #pragma unroll
             for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + (inside ? node[d] : 0);
+            T vi[3] = {T(0), T(0), T(0)}, dvi[3] = {T(0), T(0), T(0)};
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                const T vi = inside ? G.v[d][lin] : T(0);
+                vi[d] = inside ? G.v[d][lin] : T(0);
                 const T vni = inside ? G.vn[d][lin] : T(0);
-                tile[d * TN + t] = vi;
-                tile[(D + d) * TN + t] = vi - vni;
+                dvi[d] = vi[d] - vni;
+            }
+            if constexpr (VEC) {
+                reinterpret_cast<float4*>(tile)[t] = make_float4(vi[0], vi[1], vi[2], dvi[0]);
+                reinterpret_cast<float2*>(tile + 4 * TN)[t] = make_float2(dvi[1], dvi[2]);
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    tile[d * TN + t] = vi[d];
+                    tile[(D + d) * TN + t] = dvi[d];
+                }
             }
         }
         __syncthreads();
@@ -256,6 +285,61 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
                 }
                 if (!ok) {
                     atomicOr(err, ERR_TILE_RANGE);
+                } else if constexpr (!GEN && VEC) {
+                    // The separable contraction below with the component pairs of the
+                    // node-major tile in packed FP32x2 FMAs; every lane of a pair is
+                    // the scalar form's FMA with the same operands in the same order.
+                    float gx[3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) gx[i] = B.ax[0].der[i] * M.h_inv;
+                    const float4* tA = reinterpret_cast<const float4*>(tile);
+                    const float2* tB = reinterpret_cast<const float2*>(tile + 4 * TN);
+                    const float2 z2 = make_float2(0.f, 0.f);
+                    // (vpic_x, vpic_y), (vpic_z, dvf_x), (dvf_y, dvf_z), (gv_xc, gv_yc) per column c, gv_zc
+                    float2 p01 = z2, p2d0 = z2, d12 = z2, g0 = z2, g1 = z2, g2 = z2;
+                    float g0z = 0.f, g1z = 0.f, g2z = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int jj = 0; jj < 3; ++jj) {
+                            float2 Av01 = z2, Av2d0 = z2, Ad12 = z2, Ag01 = z2;
+                            float Ag2 = 0.f;
+                            const int t0 = q0[0] + TS * ((q0[1] + jj) + TS * (q0[2] + k));
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) {
+                                const float4 a = tA[t0 + i];
+                                const float2 c = tB[t0 + i];
+                                const float2 v01 = make_float2(a.x, a.y);
+                                const float2 wxx = make_float2(B.ax[0].val[i], B.ax[0].val[i]);
+                                const float2 gxx = make_float2(gx[i], gx[i]);
+                                Av01 = __ffma2_rn(wxx, v01, Av01);
+                                Av2d0 = __ffma2_rn(wxx, make_float2(a.z, a.w), Av2d0);
+                                Ad12 = __ffma2_rn(wxx, c, Ad12);
+                                Ag01 = __ffma2_rn(gxx, v01, Ag01);
+                                Ag2 = __fmaf_rn(gx[i], a.z, Ag2);
+                            }
+                            const float wyz = B.ax[1].val[jj] * B.ax[2].val[k];
+                            const float dyz = (B.ax[1].der[jj] * M.h_inv) * B.ax[2].val[k];
+                            const float wdz = B.ax[1].val[jj] * (B.ax[2].der[k] * M.h_inv);
+                            const float2 W = make_float2(wyz, wyz), DY = make_float2(dyz, dyz),
+                                         DZ = make_float2(wdz, wdz);
+                            p01 = __ffma2_rn(W, Av01, p01);
+                            p2d0 = __ffma2_rn(W, Av2d0, p2d0);
+                            d12 = __ffma2_rn(W, Ad12, d12);
+                            g0 = __ffma2_rn(W, Ag01, g0);
+                            g0z = __fmaf_rn(wyz, Ag2, g0z);
+                            g1 = __ffma2_rn(DY, Av01, g1);
+                            g1z = __fmaf_rn(dyz, Av2d0.x, g1z);
+                            g2 = __ffma2_rn(DZ, Av01, g2);
+                            g2z = __fmaf_rn(wdz, Av2d0.x, g2z);
+                        }
+                    vpic[0] = p01.x; vpic[1] = p01.y; vpic[2] = p2d0.x;
+                    dvf[0] = p2d0.y; dvf[1] = d12.x; dvf[2] = d12.y;
+                    gv[0][0] = g0.x; gv[1][0] = g0.y; gv[2][0] = g0z;
+                    gv[0][1] = g1.x; gv[1][1] = g1.y; gv[2][1] = g1z;
+                    gv[0][2] = g2.x; gv[1][2] = g2.y; gv[2][2] = g2z;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) dxs[d] = vpic[d] * s.dt;
                 } else if constexpr (!GEN) {
                     // Separable contraction: sum over the x-slot first, then weight
                     // the partial sums with the y (and z) factors.
@@ -318,13 +402,12 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
                                 for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
                                 T w, dw[3];
                                 eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
-                                const T* nd = tile + t;
-                                T vi[3];
+                                T vi[3], dvi[3];
+                                node_vals(t, vi, dvi);
 #pragma unroll
                                 for (int d = 0; d < D; ++d) {
-                                    vi[d] = nd[d * TN];
                                     vpic[d] += w * vi[d];
-                                    dvf[d] += w * nd[(D + d) * TN];
+                                    dvf[d] += w * dvi[d];
                                     dxs[d] += (w * vi[d]) * s.dt;
                                 }
 #pragma unroll
