@@ -625,6 +625,12 @@ struct PencilShape {
     static constexpr int NSUB = 32 / NJK;
     static constexpr int NPENCIL = NG / G1;
     static constexpr int NPART = NC * NPENCIL * NJK * TS;
+    // Records of pencil pc start skew * pc words after their slot: pencils of
+    // equal size (multiples of 8 records on a regular lattice) would otherwise
+    // put the records a warp's three pencils read together in the same banks.
+    // 2 words keeps 8-byte records loads aligned, 4 the 16-byte ones of FP32
+    // full records.
+    static constexpr int skew(int mode, int tsize) { return (mode == 1 || tsize == 8) ? 2 : 4; }
 };
 
 // MODE 0: every block with the full record; 1: compact records, interior
@@ -653,8 +659,9 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
 
     constexpr int RS = (MODE == 1) ? CRS : PRS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int SKW = SH::skew(MODE, sizeof(T));
     T* rec = reinterpret_cast<T*>(smem_raw);
-    T* part = rec + NR * RS;
+    T* part = rec + NR * RS + SKW * NPENCIL;
     int* gcount = reinterpret_cast<int*>(part + SH::NPART);
     int* gstart = gcount + NG;
     int* pslot = gstart + NG + 1;
@@ -825,7 +832,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                             t[d] = uu - floor(uu);
                         }
                     }
-                    T* r = rec + (gstart[grp[u]] + rank[u]) * CRS;
+                    T* r = rec + (gstart[grp[u]] + rank[u]) * CRS + SKW * (grp[u] / G1);
                     const T mp = pm[u];
                     const T nV = -pV[u];
                     st2(r + 0, mp, mp * pv[u][0]);
@@ -840,7 +847,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                 Basis<D, T> B;
                 if constexpr (X64) prepare_basis_x64<D, T>(M, s.basis, pxd[u], pl[u], B, err);
                 else prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err);
-                T* r = rec + (gstart[grp[u]] + rank[u]) * PRS;
+                T* r = rec + (gstart[grp[u]] + rank[u]) * PRS + SKW * (grp[u] / G1);
                 const T mp = pm[u];
                 const T nV = -pV[u];
                 const T* v = pv[u];
@@ -873,6 +880,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                 const int pc = pslot[slot];
                 const int gbase = G1 * pc;
                 const int pbase = (jk * NPENCIL + pc) * TS;
+                const T* prec = rec + SKW * pc;  // this pencil's records (skewed)
                 T acc[3][NC];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
@@ -890,27 +898,27 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                         if constexpr (MODE == 1) {
                             for (; q + 1 < qe; q += 2) {
                                 CompactRec<T> r0, r1;
-                                load_compact<D, T>(rec + q * CRS, r0);
-                                load_compact<D, T>(rec + (q + 1) * CRS, r1);
+                                load_compact<D, T>(prec + q * CRS, r0);
+                                load_compact<D, T>(prec + (q + 1) * CRS, r1);
                                 accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
                                 accumulate_compact<D, T>(r1, py, pz, M.h_inv, acc);
                             }
                             if (q < qe) {
                                 CompactRec<T> r0;
-                                load_compact<D, T>(rec + q * CRS, r0);
+                                load_compact<D, T>(prec + q * CRS, r0);
                                 accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
                             }
                         } else {
                             for (; q + 1 < qe; q += 2) {
                                 PlainRec<T> r0, r1;
-                                load_plain<D, T>(rec + q * PRS, sj, sk, r0);
-                                load_plain<D, T>(rec + (q + 1) * PRS, sj, sk, r1);
+                                load_plain<D, T>(prec + q * PRS, sj, sk, r0);
+                                load_plain<D, T>(prec + (q + 1) * PRS, sj, sk, r1);
                                 accumulate_plain<D, T>(r0, acc);
                                 accumulate_plain<D, T>(r1, acc);
                             }
                             if (q < qe) {
                                 PlainRec<T> r0;
-                                load_plain<D, T>(rec + q * PRS, sj, sk, r0);
+                                load_plain<D, T>(prec + q * PRS, sj, sk, r0);
                                 accumulate_plain<D, T>(r0, acc);
                             }
                         }
@@ -988,7 +996,8 @@ template <int D, class T, int BW, int NR, int MODE>
 size_t pencil_smem_bytes() {
     using SH = PencilShape<D, BW>;
     const int rs = (MODE == 1) ? CRS : PRS;
-    return sizeof(T) * (size_t(NR) * rs + SH::NPART) + sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
+    return sizeof(T) * (size_t(NR) * rs + SH::skew(MODE, sizeof(T)) * SH::NPENCIL + SH::NPART) +
+           sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
 }
 
 template <int D, class T, int BW, bool X64, int MODE>
