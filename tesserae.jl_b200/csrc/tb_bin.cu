@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256) bin_scatter_kernel(const int* __restrict_
     if (b > 0) perm_tmp[base + rank] = int(p);
 }
 
-constexpr int FIX_THREADS = 128;
+constexpr int FIX_THREADS = 256;
 constexpr int FIX_SMEM_KEYS = 2048;
 
 __device__ __forceinline__ int next_pow2(int v) {
@@ -163,6 +163,38 @@ __device__ __forceinline__ int next_pow2(int v) {
     return k;
 }
 
+// Exclusive scan of one int per thread over the CTA (blockDim = FIX_THREADS);
+// `total` gets the sum. Two barriers; `wsum` holds the warp sums.
+__device__ __forceinline__ int fix_excl_scan(int v, int* wsum, int& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    int wprefix = 0;
+    total = 0;
+#pragma unroll
+    for (int q = 0; q < FIX_THREADS / 32; ++q) {
+        const int w = wsum[q];
+        wprefix += q < wid ? w : 0;
+        total += w;
+    }
+    __syncthreads();
+    return wprefix + incl - v;
+}
+
+// Blocks of more than FIXW_RUNS runs, one CTA per block. Runs are found in
+// segment order, their keys (scatter warp id << 32 | run index) bitonic-sorted,
+// the output start of each run is the prefix sum of the run lengths in sorted
+// order, and the segment is copied element-parallel (each element to its run's
+// place), all in shared memory when the padded key count fits; above that
+// (more than FIX_SMEM_KEYS runs) the keys are sorted in the block's own region
+// [2s, 2s + 2n) of the global scratch (next_pow2(k) <= 2n, segments disjoint)
+// and each thread copies whole runs.
 __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __restrict__ totals,
                                                                 const int* __restrict__ blocklist,
                                                                 const int* __restrict__ offsets,
@@ -170,10 +202,13 @@ __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __res
                                                                 const int* __restrict__ S, int* __restrict__ perm,
                                                                 unsigned long long* __restrict__ gscratch) {
     __shared__ unsigned long long sbuf[FIX_SMEM_KEYS];
+    __shared__ int hpos[FIX_SMEM_KEYS + 1];  // run starts, segment order
+    __shared__ int hout[FIX_SMEM_KEYS];      // output start of each run, segment order
     __shared__ int kcount;
     __shared__ int wsum[FIX_THREADS / 32];
     const int nactive = totals[0];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int tid = threadIdx.x;
+    auto is_head = [](const int* seg, int j, int v) { return j == 0 || (seg[j - 1] >> 5) != (v >> 5); };
     for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
         const int b = blocklist[bi] - 1;
         const int s = offsets[b];
@@ -181,27 +216,82 @@ __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __res
         const int* seg = S + s;
         int* out = perm + s;
         // Run heads: the first element, and every element whose warp id differs
-        // from its predecessor's. Key = (warp id << 32) | position in segment.
-        // First count them to pick the buffer: shared memory when the padded key
-        // count fits, else the block's own region [2s, 2s + 2n) of the global
-        // scratch (next_pow2(k) <= 2n, and segments are disjoint).
-        if (tid == 0) kcount = 0;
-        __syncthreads();
+        // from its predecessor's.
         int myheads = 0;
-        for (int j = tid; j < n; j += FIX_THREADS)
-            myheads += (j == 0) || ((seg[j - 1] >> 5) != (seg[j] >> 5));
-        if (myheads) atomicAdd(&kcount, myheads);
-        __syncthreads();
-        const int k = kcount;
+        for (int j = tid; j < n; j += FIX_THREADS) myheads += is_head(seg, j, seg[j]);
+        int k;
+        fix_excl_scan(myheads, wsum, k);
         const int K = next_pow2(k);
-        unsigned long long* buf = (K <= FIX_SMEM_KEYS) ? sbuf : gscratch + 2ll * s;
-        __syncthreads();
+        if (K <= FIX_SMEM_KEYS) {
+            // 1. heads in segment order: positions and keys
+            int rbase = 0;
+            for (int j0 = 0; j0 < n; j0 += FIX_THREADS) {
+                const int j = j0 + tid;
+                const int v = j < n ? seg[j] : 0;
+                const int h = (j < n && is_head(seg, j, v)) ? 1 : 0;
+                int tot;
+                const int r = rbase + fix_excl_scan(h, wsum, tot);
+                if (h) {
+                    hpos[r] = j;
+                    sbuf[r] = ((unsigned long long)(unsigned)(v >> 5) << 32) | (unsigned)r;
+                }
+                rbase += tot;
+            }
+            if (tid == 0) hpos[k] = n;
+            for (int t = k + tid; t < K; t += FIX_THREADS) sbuf[t] = ~0ull;
+            __syncthreads();
+            // 2. bitonic sort of the K keys (ascending)
+            for (int size = 2; size <= K; size <<= 1) {
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    for (int i = tid; i < (K >> 1); i += FIX_THREADS) {
+                        const int lo = (i / stride) * 2 * stride + (i % stride);
+                        const int hi = lo + stride;
+                        const bool asc = (lo & size) == 0;
+                        const unsigned long long a = sbuf[lo], c = sbuf[hi];
+                        if ((a > c) == asc) {
+                            sbuf[lo] = c;
+                            sbuf[hi] = a;
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            // 3. output start of each run: lengths summed in sorted order
+            int obase = 0;
+            for (int i0 = 0; i0 < k; i0 += FIX_THREADS) {
+                const int i = i0 + tid;
+                int r = 0, len = 0;
+                if (i < k) {
+                    r = int(sbuf[i] & 0xffffffffull);
+                    len = hpos[r + 1] - hpos[r];
+                }
+                int tot;
+                const int st = obase + fix_excl_scan(len, wsum, tot);
+                if (i < k) hout[r] = st;
+                obase += tot;
+            }
+            __syncthreads();
+            // 4. element-parallel copy: an element's run is the number of heads at
+            //    or before it, minus one
+            rbase = 0;
+            for (int j0 = 0; j0 < n; j0 += FIX_THREADS) {
+                const int j = j0 + tid;
+                const int v = j < n ? seg[j] : 0;
+                const int h = (j < n && is_head(seg, j, v)) ? 1 : 0;
+                int tot;
+                const int r = rbase + fix_excl_scan(h, wsum, tot) + h - 1;
+                if (j < n) out[hout[r] + (j - hpos[r])] = v + 1;
+                rbase += tot;
+            }
+            __syncthreads();
+            continue;
+        }
+        unsigned long long* buf = gscratch + 2ll * s;
         if (tid == 0) kcount = 0;
         __syncthreads();
         for (int j = tid; j < n; j += FIX_THREADS) {
             const int v = seg[j];
-            const bool head = (j == 0) || ((seg[j - 1] >> 5) != (v >> 5));
-            if (head) {
+            if (is_head(seg, j, v)) {
                 const int idx = atomicAdd(&kcount, 1);
                 buf[idx] = ((unsigned long long)(unsigned)(v >> 5) << 32) | (unsigned)j;
             }
@@ -237,26 +327,12 @@ __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __res
                 len = 1;
                 while (j0 + len < n && (seg[j0 + len] >> 5) == w) ++len;
             }
-            // block exclusive scan of len
-            int incl = len;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            if (lane == 31) wsum[wid] = incl;
-            __syncthreads();
-            int wprefix = 0, total = 0;
-#pragma unroll
-            for (int q = 0; q < FIX_THREADS / 32; ++q) {
-                if (q < wid) wprefix += wsum[q];
-                total += wsum[q];
-            }
-            const int excl = base + wprefix + incl - len;
+            int total;
+            const int excl = base + fix_excl_scan(len, wsum, total);
             for (int t = 0; t < len; ++t) out[excl + t] = seg[j0 + t] + 1;
             base += total;
-            __syncthreads();
         }
+        __syncthreads();
     }
 }
 
@@ -268,6 +344,7 @@ __global__ void __launch_bounds__(FIX_THREADS) bin_fixup_kernel(const int* __res
 // element-parallel, each element to its run's place. A block with more runs is appended to an
 // overflow list that bin_fixup_kernel then sorts.
 constexpr int FIXW_RUNS = 64;
+constexpr int FIXW_U = 8;  // chunks of 32 ids loaded together
 constexpr int FIXW_THREADS = 256;
 
 __global__ void __launch_bounds__(FIXW_THREADS) bin_fixup_warp_kernel(const int* __restrict__ totals,
@@ -292,19 +369,39 @@ __global__ void __launch_bounds__(FIXW_THREADS) bin_fixup_warp_kernel(const int*
         const int* seg = S + s;
         int* out = perm + s;
         int nruns = 0;
-        for (int j0 = 0; j0 < n; j0 += 32) {
-            const int j = j0 + lane;
-            const int v = j < n ? seg[j] : 0;
-            int prev = __shfl_up_sync(full, v, 1);
-            if (lane == 0) prev = j0 > 0 ? seg[j0 - 1] : -1;
-            const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
-            const unsigned hm = __ballot_sync(full, head);
-            const int idx = nruns + __popc(hm & below);
-            if (head && idx < FIXW_RUNS) {
-                hpos[w][idx] = j;
-                hkey[w][idx] = v >> 5;
+        // A run is at most 32 long, so a longer segment has too many runs: hand it
+        // over without walking it (one warp reading thousands of ids serially was
+        // most of the fix-up time of crowded scenes), and stop walking at the
+        // first run past the limit.
+        if (n > FIXW_RUNS * 32) nruns = FIXW_RUNS + 1;
+        // The segment is read FIXW_U chunks of 32 at a time, all loads of a batch
+        // issued before any is used; the predecessor of a chunk's first element
+        // is lane 31 of the chunk before.
+        int last = -1;
+        for (int J0 = 0; J0 < n && nruns <= FIXW_RUNS; J0 += 32 * FIXW_U) {
+            int vv[FIXW_U];
+#pragma unroll
+            for (int u = 0; u < FIXW_U; ++u) {
+                const int j = J0 + 32 * u + lane;
+                vv[u] = j < n ? seg[j] : 0;
             }
-            nruns += __popc(hm);
+#pragma unroll
+            for (int u = 0; u < FIXW_U; ++u) {
+                const int j0 = J0 + 32 * u;
+                if (j0 >= n) break;
+                const int j = j0 + lane, v = vv[u];
+                int prev = __shfl_up_sync(full, v, 1);
+                if (lane == 0) prev = last;
+                last = __shfl_sync(full, v, 31);
+                const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
+                const unsigned hm = __ballot_sync(full, head);
+                const int idx = nruns + __popc(hm & below);
+                if (head && idx < FIXW_RUNS) {
+                    hpos[w][idx] = j;
+                    hkey[w][idx] = v >> 5;
+                }
+                nruns += __popc(hm);
+            }
         }
         if (nruns > FIXW_RUNS) {
             if (lane == 0) overflow[atomicAdd(noverflow, 1ull)] = b + 1;
@@ -325,16 +422,28 @@ __global__ void __launch_bounds__(FIXW_THREADS) bin_fixup_warp_kernel(const int*
         // copy element-parallel: the run of element j is the number of heads at
         // or before j, minus one
         int rbase = 0;
-        for (int j0 = 0; j0 < n; j0 += 32) {
-            const int j = j0 + lane;
-            const int v = j < n ? seg[j] : 0;
-            int prev = __shfl_up_sync(full, v, 1);
-            if (lane == 0) prev = j0 > 0 ? seg[j0 - 1] : -1;
-            const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
-            const unsigned hm = __ballot_sync(full, head);
-            const int r = rbase + __popc(hm & (below | (1u << lane))) - 1;
-            if (j < n) out[hout[w][r] + (j - hpos[w][r])] = v + 1;
-            rbase += __popc(hm);
+        last = -1;
+        for (int J0 = 0; J0 < n; J0 += 32 * FIXW_U) {
+            int vv[FIXW_U];
+#pragma unroll
+            for (int u = 0; u < FIXW_U; ++u) {
+                const int j = J0 + 32 * u + lane;
+                vv[u] = j < n ? seg[j] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < FIXW_U; ++u) {
+                const int j0 = J0 + 32 * u;
+                if (j0 >= n) break;
+                const int j = j0 + lane, v = vv[u];
+                int prev = __shfl_up_sync(full, v, 1);
+                if (lane == 0) prev = last;
+                last = __shfl_sync(full, v, 31);
+                const bool head = j < n && (j == 0 || (prev >> 5) != (v >> 5));
+                const unsigned hm = __ballot_sync(full, head);
+                const int r = rbase + __popc(hm & (below | (1u << lane))) - 1;
+                if (j < n) out[hout[w][r] + (j - hpos[w][r])] = v + 1;
+                rbase += __popc(hm);
+            }
         }
         __syncwarp();
     }
