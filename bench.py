@@ -412,7 +412,7 @@ def run_reference(args, rank: int, world: int):
     tb = load_package()
     om = load_oracle(tb)
     oracle = om.Oracle(tb._abi)
-    sc = tb.scenes.cube3d(scale=args.scale)
+    sc = tb.scenes.block_ordered(tb.scenes.cube3d(scale=args.scale))  # the order the B200 arm times
     mesh, prm = sc.mesh, sc.params
     P = sc.particles
     G = tb.generate_grid(mesh)
@@ -480,7 +480,6 @@ def main():
     mesh, prm = sc.mesh, sc.params
     host64 = sc.particles
     n = host64.n
-    x0 = host64.x.copy()
 
     def barrier():
         if dist is not None:
@@ -504,6 +503,28 @@ def main():
         e1.record()
         barrier()
         return e0.elapsed_time(e1), ctx.launches - l0
+
+    # The headline form with the particles in generation order (column-major
+    # lattice), timed before they are put in block order for every other leg.
+    gen_order = None
+    if not args.quick:
+        dtype, x64, _ = FORMS["x64"]
+        P = host64.to("torch", device="cuda", dtype=dtype, x64=x64)
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, P, part, mesh, prm, args.warmup, ctx=ctx)
+        ctx.synchronize()
+        score = runtime.block_ordered_particle_contiguity(part, n, ctx=ctx)
+        ms, _ = timed_steps(P, G, part, args.steps)
+        ms = max_over_ranks(ms)
+        gen_order = {"value": world * n * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                     "contiguity": score,
+                     "order": "generation order (column-major lattice), headline form"}
+        del P, part, G
+        torch.cuda.empty_cache()
+    # reorder_particles! once after the first binning (docs/src/parallel.md:47-57)
+    tb.scenes.block_ordered(sc)
+    x0 = host64.x.copy()
 
     results = {}
     forms = ("x64",) if args.quick else ("x64", "f32", "f64")
@@ -643,11 +664,16 @@ def main():
                                "Neo-Hookean E=1e6 nu=0.3, gravity, dt=5e-5; one MPM step per bench step",
                    "n_particles": n, "scale": args.scale, "form": FORMS["x64"][2],
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (3.1 GB particle state per replica)"},
+                   "l2": "inputs larger than L2 (3.1 GB particle state per replica)",
+                   "particle_order": "block order: reorder_particles! once after the first binning, as "
+                                     "docs/src/parallel.md:47-57 sets up a GPU run (the reference arm and "
+                                     "the CPU baseline time the same order; generation order under "
+                                     "generation_order)"},
         "accuracy": acc,
         "fp32_positions": {"value": world * n * args.steps / (f32["ms"] * 1e-3), "ms_per_step": f32["ms"] / args.steps,
                            "form": FORMS["f32"][2], "accuracy": acc_f32},
         "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
+        "generation_order": gen_order,
         "adjoint_over_forward": adjoint,
         "taylor_impact": taylor,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -118,6 +118,22 @@ def _sort_by_block(mesh: CartesianMesh, pts: np.ndarray) -> np.ndarray:
     return np.argsort(b, kind="stable")
 
 
+def block_ordered(scene: Scene) -> Scene:
+    """`scene` with its particles stored in block order, in place: the order
+    `reorder_particles!(particles, partition)` leaves them in after the first
+    `update!(partition, particles.x)`, the set-up docs/src/parallel.md:47-57
+    gives for GPU runs. Every particle field is permuted alike; the particles
+    themselves are unchanged."""
+    P = scene.particles
+    order = _sort_by_block(scene.mesh, P.x)
+    for k in Particles.FIELDS:
+        a = getattr(P, k)
+        if a is not None:
+            a[...] = a[..., order]
+    scene.meta["particle_order"] = "block"
+    return scene
+
+
 def clusters3d(scale: int = 1, n_total: int = 32 * 1024 * 1024, seed: int | None = None) -> Scene:
     """512^3 cells (h = 1/512), n_total particles from 64 Gaussian clusters
     (sigma = 0.02, centres U[0.2, 0.8]^3), masses rho0 V0 lognormal(0, 0.5),

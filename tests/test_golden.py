@@ -173,3 +173,21 @@ def test_partition_lists_ascending(tb, oracle):
     assert np.array_equal(part.offsets, offsets)
     assert na == len(blocklist) and np.array_equal(part.blocklist[:na], blocklist)
     assert nass == len(perm) and np.array_equal(part.particleindices[:nass], perm)
+
+
+def test_block_ordered_scene_is_the_partition_order(tb, oracle):
+    """scenes.block_ordered stores the particles in the order reorder_particles!
+    leaves them in (gpu_block_strategy.jl:204-238): after it, the oracle's
+    partition lists the particles 1..n in order, and the particle set (positions
+    with their velocities) is unchanged."""
+    sc = tb.scenes.cube3d(scale=16)
+    before = {tuple(np.r_[sc.particles.x[:, p], sc.particles.v[:, p]]) for p in range(sc.particles.n)}
+    part0 = tb.Partition(sc.mesh, sc.particles.n)
+    oracle.bin(sc.mesh, sc.particles, part0)
+    assert not np.array_equal(part0.particleindices, np.arange(1, sc.particles.n + 1))
+    tb.scenes.block_ordered(sc)
+    part = tb.Partition(sc.mesh, sc.particles.n)
+    oracle.bin(sc.mesh, sc.particles, part)
+    assert np.array_equal(part.particleindices, np.arange(1, sc.particles.n + 1))
+    after = {tuple(np.r_[sc.particles.x[:, p], sc.particles.v[:, p]]) for p in range(sc.particles.n)}
+    assert before == after
