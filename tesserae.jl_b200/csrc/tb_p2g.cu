@@ -603,6 +603,62 @@ __device__ __forceinline__ void accumulate_compact(const CompactRec<T>& o, const
     }
 }
 
+// 3D FP32 compact record, laid out for packed FP32x2 arithmetic (S = -V sigma in
+// Tensorial order 11 21 31 22 32 33 = S0..S5):
+//   (m, m v_x) (m v_y, m v_z) (S0, S1) (S1, S3) (S2, S4) (S5, t_z) (t_x, t_y)
+// so that f_xy = dx (S0, S1) wyz + wx ((S1, S3) dyz + (S2, S4) wdz) is pairwise.
+struct PairRec {
+    float2 m0, m1, sa, sb, sc, s5z, txy;
+};
+__device__ __forceinline__ void load_pair_rec(const float* r, PairRec& o) {
+    o.m0 = *reinterpret_cast<const float2*>(r + 0);
+    o.m1 = *reinterpret_cast<const float2*>(r + 2);
+    o.sa = *reinterpret_cast<const float2*>(r + 4);
+    o.sb = *reinterpret_cast<const float2*>(r + 6);
+    o.sc = *reinterpret_cast<const float2*>(r + 8);
+    o.s5z = *reinterpret_cast<const float2*>(r + 10);
+    o.txy = *reinterpret_cast<const float2*>(r + 12);
+}
+// Per x-node of a row lane: (m, m v_x), (m v_y, m v_z), (f_x, f_y) and f_z.
+struct PairAcc {
+    float2 a01, a23, f01;
+    float f2;
+};
+__device__ __forceinline__ void accumulate_pair(const PairRec& o, const SlotPoly& py, const SlotPoly& pz, float h_inv,
+                                                PairAcc (&acc)[3]) {
+    const float tx = o.txy.x, ty = o.txy.y, tz = o.s5z.y;
+    const float2 t2 = make_float2(tx, tx);
+    // (wx_i, wx_i) and (dx_i, dx_i): the B-spline factors of the three x slots
+    const float2 wx0 = __ffma2_rn(t2, __ffma2_rn(t2, make_float2(0.5f, 0.5f), make_float2(-1.f, -1.f)),
+                                  make_float2(0.5f, 0.5f));
+    const float2 wx1 = __ffma2_rn(t2, __ffma2_rn(t2, make_float2(-1.f, -1.f), make_float2(1.f, 1.f)),
+                                  make_float2(0.5f, 0.5f));
+    const float2 wx2 = __fmul2_rn(t2, __fmul2_rn(t2, make_float2(0.5f, 0.5f)));
+    const float2 hh = make_float2(h_inv, h_inv);
+    const float2 dx0 = __fmul2_rn(__fadd2_rn(t2, make_float2(-1.f, -1.f)), hh);
+    const float2 dx1 = __fmul2_rn(__ffma2_rn(t2, make_float2(-2.f, -2.f), make_float2(1.f, 1.f)), hh);
+    const float2 dx2 = __fmul2_rn(t2, hh);
+    const float wy = py.a + ty * (py.b + ty * py.c);
+    const float dy = (py.e + ty * py.f) * h_inv;
+    const float wz = pz.a + tz * (pz.b + tz * pz.c);
+    const float dz = (pz.e + tz * pz.f) * h_inv;
+    const float wyz = wy * wz, dyz = dy * wz, wdz = wy * dz;
+    const float2 WYZ = make_float2(wyz, wyz);
+    const float2 fa01 = __fmul2_rn(o.sa, WYZ);
+    const float2 fb01 = __ffma2_rn(o.sc, make_float2(wdz, wdz), __fmul2_rn(o.sb, make_float2(dyz, dyz)));
+    const float fa2 = o.sc.x * wyz;
+    const float fb2 = __fmaf_rn(o.s5z.x, wdz, o.sc.y * dyz);
+    const float2 wxs[3] = {wx0, wx1, wx2}, dxs[3] = {dx0, dx1, dx2};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float2 w = __fmul2_rn(wxs[i], WYZ);
+        acc[i].a01 = __ffma2_rn(w, o.m0, acc[i].a01);
+        acc[i].a23 = __ffma2_rn(w, o.m1, acc[i].a23);
+        acc[i].f01 = __ffma2_rn(dxs[i], fa01, __ffma2_rn(wxs[i], fb01, acc[i].f01));
+        acc[i].f2 = __fmaf_rn(dxs[i].x, fa2, __fmaf_rn(wxs[i].x, fb2, acc[i].f2));
+    }
+}
+
 template <int NC, class T>
 __device__ __forceinline__ void stage_node(T* part, int base, int stride, const T (&a)[NC]) {
 #pragma unroll
@@ -660,6 +716,8 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     constexpr int RS = (MODE == 1) ? CRS : PRS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int SKW = SH::skew(MODE, sizeof(T));
+    // 3D FP32 compact records: packed FP32x2 accumulation (PairRec layout)
+    constexpr bool PAIRS = (MODE == 1 && D == 3 && sizeof(T) == 4);
     T* rec = reinterpret_cast<T*>(smem_raw);
     T* part = rec + NR * RS + SKW * NPENCIL;
     int* gcount = reinterpret_cast<int*>(part + SH::NPART);
@@ -835,6 +893,16 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                     T* r = rec + (gstart[grp[u]] + rank[u]) * CRS + SKW * (grp[u] / G1);
                     const T mp = pm[u];
                     const T nV = -pV[u];
+                    if constexpr (PAIRS) {
+                        st2(r + 0, mp, mp * pv[u][0]);
+                        st2(r + 2, mp * pv[u][1], mp * pv[u][2]);
+                        st2(r + 4, nV * psg[u][0], nV * psg[u][1]);
+                        st2(r + 6, nV * psg[u][1], nV * psg[u][3]);
+                        st2(r + 8, nV * psg[u][2], nV * psg[u][4]);
+                        st2(r + 10, nV * psg[u][5], t[2]);
+                        st2(r + 12, t[0], t[1]);
+                        continue;
+                    }
                     st2(r + 0, mp, mp * pv[u][0]);
                     st2(r + 2, mp * pv[u][1], mp * pv[u][2]);
                     st2(r + 4, nV * psg[u][0], nV * psg[u][1]);
@@ -881,55 +949,93 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
                 const int gbase = G1 * pc;
                 const int pbase = (jk * NPENCIL + pc) * TS;
                 const T* prec = rec + SKW * pc;  // this pencil's records (skewed)
-                T acc[3][NC];
+                if constexpr (PAIRS) {
+                    PairAcc pa[3];
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) acc[i][c] = T(0);
-                // The groups of the pencil in x order; two records of a group are
-                // loaded before either is accumulated. After group gx the x-node
-                // gx is final (later groups start further right).
-                int qs = gstart[gbase];
-#pragma unroll
-                for (int gx = 0; gx < G1 + 2; ++gx) {
-                    if (gx < G1) {
-                        const int qe = gstart[gbase + gx + 1];
-                        int q = qs;
-                        if constexpr (MODE == 1) {
-                            for (; q + 1 < qe; q += 2) {
-                                CompactRec<T> r0, r1;
-                                load_compact<D, T>(prec + q * CRS, r0);
-                                load_compact<D, T>(prec + (q + 1) * CRS, r1);
-                                accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
-                                accumulate_compact<D, T>(r1, py, pz, M.h_inv, acc);
-                            }
-                            if (q < qe) {
-                                CompactRec<T> r0;
-                                load_compact<D, T>(prec + q * CRS, r0);
-                                accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
-                            }
-                        } else {
-                            for (; q + 1 < qe; q += 2) {
-                                PlainRec<T> r0, r1;
-                                load_plain<D, T>(prec + q * PRS, sj, sk, r0);
-                                load_plain<D, T>(prec + (q + 1) * PRS, sj, sk, r1);
-                                accumulate_plain<D, T>(r0, acc);
-                                accumulate_plain<D, T>(r1, acc);
-                            }
-                            if (q < qe) {
-                                PlainRec<T> r0;
-                                load_plain<D, T>(prec + q * PRS, sj, sk, r0);
-                                accumulate_plain<D, T>(r0, acc);
-                            }
-                        }
-                        qs = qe;
+                    for (int i = 0; i < 3; ++i) {
+                        pa[i].a01 = pa[i].a23 = pa[i].f01 = make_float2(0.f, 0.f);
+                        pa[i].f2 = 0.f;
                     }
-                    stage_node<NC, T>(part, pbase + gx, CSTR, acc[0]);
+                    const float* frec = reinterpret_cast<const float*>(prec);
+                    int qs = gstart[gbase];
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        acc[0][c] = acc[1][c];
-                        acc[1][c] = acc[2][c];
-                        acc[2][c] = T(0);
+                    for (int gx = 0; gx < G1 + 2; ++gx) {
+                        if (gx < G1) {
+                            const int qe = gstart[gbase + gx + 1];
+                            int q = qs;
+                            for (; q + 1 < qe; q += 2) {
+                                PairRec r0, r1;
+                                load_pair_rec(frec + q * CRS, r0);
+                                load_pair_rec(frec + (q + 1) * CRS, r1);
+                                accumulate_pair(r0, py, pz, M.h_inv, pa);
+                                accumulate_pair(r1, py, pz, M.h_inv, pa);
+                            }
+                            if (q < qe) {
+                                PairRec r0;
+                                load_pair_rec(frec + q * CRS, r0);
+                                accumulate_pair(r0, py, pz, M.h_inv, pa);
+                            }
+                            qs = qe;
+                        }
+                        const T a0[NC] = {pa[0].a01.x, pa[0].a01.y, pa[0].a23.x, pa[0].a23.y,
+                                          pa[0].f01.x, pa[0].f01.y, pa[0].f2};
+                        stage_node<NC, T>(part, pbase + gx, CSTR, a0);
+                        pa[0] = pa[1];
+                        pa[1] = pa[2];
+                        pa[2].a01 = pa[2].a23 = pa[2].f01 = make_float2(0.f, 0.f);
+                        pa[2].f2 = 0.f;
+                    }
+                } else {
+                    T acc[3][NC];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) acc[i][c] = T(0);
+                    // The groups of the pencil in x order; two records of a group are
+                    // loaded before either is accumulated. After group gx the x-node
+                    // gx is final (later groups start further right).
+                    int qs = gstart[gbase];
+#pragma unroll
+                    for (int gx = 0; gx < G1 + 2; ++gx) {
+                        if (gx < G1) {
+                            const int qe = gstart[gbase + gx + 1];
+                            int q = qs;
+                            if constexpr (MODE == 1) {
+                                for (; q + 1 < qe; q += 2) {
+                                    CompactRec<T> r0, r1;
+                                    load_compact<D, T>(prec + q * CRS, r0);
+                                    load_compact<D, T>(prec + (q + 1) * CRS, r1);
+                                    accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
+                                    accumulate_compact<D, T>(r1, py, pz, M.h_inv, acc);
+                                }
+                                if (q < qe) {
+                                    CompactRec<T> r0;
+                                    load_compact<D, T>(prec + q * CRS, r0);
+                                    accumulate_compact<D, T>(r0, py, pz, M.h_inv, acc);
+                                }
+                            } else {
+                                for (; q + 1 < qe; q += 2) {
+                                    PlainRec<T> r0, r1;
+                                    load_plain<D, T>(prec + q * PRS, sj, sk, r0);
+                                    load_plain<D, T>(prec + (q + 1) * PRS, sj, sk, r1);
+                                    accumulate_plain<D, T>(r0, acc);
+                                    accumulate_plain<D, T>(r1, acc);
+                                }
+                                if (q < qe) {
+                                    PlainRec<T> r0;
+                                    load_plain<D, T>(prec + q * PRS, sj, sk, r0);
+                                    accumulate_plain<D, T>(r0, acc);
+                                }
+                            }
+                            qs = qe;
+                        }
+                        stage_node<NC, T>(part, pbase + gx, CSTR, acc[0]);
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            acc[0][c] = acc[1][c];
+                            acc[1][c] = acc[2][c];
+                            acc[2][c] = T(0);
+                        }
                     }
                 }
             }
