@@ -90,6 +90,8 @@ struct tb_ctx {
     // touched node blocks of the last two transfers (sparse grid zero/update)
     unsigned char* touched_cur = nullptr;
     unsigned char* touched_prev = nullptr;
+    int* touched_list = nullptr;  // [nblocks] blocks with cur or prev set, count in touched_count
+    int* touched_count = nullptr;
     long long touched_cap = 0;
     const void* grid_key = nullptr;  // grid.m of the grid the flags describe
     long long grid_nblocks = 0;
@@ -365,6 +367,10 @@ int touched_buffers(tb_ctx* c, long long nb) {
         if ((e = grow(c->touched_cur, cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched flags");
         cap = c->touched_cap;
         if ((e = grow(c->touched_prev, cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched flags");
+        cap = c->touched_cap;
+        if ((e = grow(c->touched_list, cap, nb)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched list");
+        long long one = c->touched_count ? 1 : 0;
+        if ((e = grow(c->touched_count, one, 1)) != cudaSuccess) return cuda_fail(c, e, "cudaMalloc touched count");
         c->touched_cap = nb;
         c->grid_sparse_ok = false;
     }
@@ -387,7 +393,9 @@ cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, co
     if (e == cudaSuccess && !known) e = cudaMemsetAsync(c->touched_prev, 0, size_t(M.nblocks), cfg.stream);
     if (e == cudaSuccess) e = launch_mark_touched(D, M.nb, B, c->touched_cur, M.nblocks, cfg);
     if (e == cudaSuccess)
-        e = known ? launch_sparse_zero<D, T, BW>(M, G, c->touched_cur, c->touched_prev, cfg)
+        e = launch_touched_list(c->touched_cur, c->touched_prev, M.nblocks, c->touched_list, c->touched_count, cfg);
+    if (e == cudaSuccess)
+        e = known ? launch_sparse_zero<D, T, BW>(M, G, c->touched_list, c->touched_count, cfg)
                   : launch_grid_zero<D, T>(M, G, cfg);
     if (e == cudaSuccess) e = launch_p2g<D, T, BW>(M, P, G, S, B, cfg);
     c->grid_key = G.m;
@@ -405,7 +413,8 @@ cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const G
     const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks &&
                        !c->grid_dense_pending;
     c->grid_dense_pending = false;
-    if (known) return launch_sparse_grid_update<D, T, BW>(M, G, S, c->touched_cur, c->touched_prev, cfg);
+    if (known)
+        return launch_sparse_grid_update<D, T, BW>(M, G, S, c->touched_cur, c->touched_list, c->touched_count, cfg);
     return launch_grid_update<D, T>(M, G, S, cfg);
 }
 
@@ -1150,6 +1159,8 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->roll_buf);
     cudaFree(c->touched_cur);
     cudaFree(c->touched_prev);
+    cudaFree(c->touched_list);
+    cudaFree(c->touched_count);
     cudaFree(c->adj_grid);
     cudaFree(c->adj_coef);
     cudaFree(c->g2p2g_x);

@@ -85,12 +85,16 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
 // transfer (prev): see tb_transfer.cu.
 cudaError_t launch_mark_touched(int dim, const int* nbv, const BinBuffers& b, unsigned char* cur, int nblocks,
                                 const LaunchCfg& cfg);
+// The node blocks with cur or prev set, compacted into list[0 .. *count).
+cudaError_t launch_touched_list(const unsigned char* cur, const unsigned char* prev, int nblocks, int* list,
+                                int* count, const LaunchCfg& cfg);
 template <int D, class T, int BW>
-cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const unsigned char* cur,
-                               const unsigned char* prev, const LaunchCfg& cfg);
+cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const int* list, const int* count,
+                               const LaunchCfg& cfg);
 template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
-                                      const unsigned char* cur, const unsigned char* prev, const LaunchCfg& cfg);
+                                      const unsigned char* cur, const int* list, const int* count,
+                                      const LaunchCfg& cfg);
 
 // max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v| into *out
 // (the bits of a double).

@@ -91,18 +91,38 @@ __global__ void __launch_bounds__(128) mark_touched_kernel(const int* __restrict
     }
 }
 
-// One warp per node block. mode 0: zero m, mv, f where cur|prev; mode 1: grid
-// update where cur, zero v, vn where prev only.
+// The node blocks marked in cur or prev, compacted into a list (one atomic per
+// warp; the order of the list does not matter, every block is processed on its
+// own), so the zero and update passes visit the touched blocks only instead of
+// testing every block's flags.
+__global__ void __launch_bounds__(256) touched_list_kernel(const unsigned char* __restrict__ cur,
+                                                           const unsigned char* __restrict__ prev, int nblocks,
+                                                           int* __restrict__ list, int* __restrict__ count) {
+    const int lane = threadIdx.x & 31;
+    for (int B0 = blockIdx.x * blockDim.x; B0 < nblocks; B0 += gridDim.x * blockDim.x) {
+        const int B = B0 + threadIdx.x;
+        const bool t = B < nblocks && (cur[B] | prev[B]);
+        const unsigned m = __ballot_sync(0xffffffffu, t);
+        int base = 0;
+        if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (t) list[base + __popc(m & ((1u << lane) - 1u))] = B;
+    }
+}
+
+// One warp per listed node block. mode 0: zero m, mv, f; mode 1: grid update
+// where cur, zero v, vn where the block was touched by the previous transfer only.
 template <int D, class T, int BW, int MODE>
-__global__ void __launch_bounds__(256) node_block_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s,
-                                                         const unsigned char* __restrict__ cur,
-                                                         const unsigned char* __restrict__ prev) {
+__global__ void __launch_bounds__(256) node_list_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s,
+                                                        const unsigned char* __restrict__ cur,
+                                                        const int* __restrict__ list, const int* __restrict__ count) {
     constexpr int NPB = (D == 3) ? BW * BW * BW : BW * BW;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int B = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; B < M.nblocks; B += warps) {
-        const bool c = cur[B] != 0, pv = prev[B] != 0;
-        if (!c && !pv) continue;
+    const int nlist = *count;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nlist; w += warps) {
+        const int B = list[w];
+        const bool c = MODE == 1 ? cur[B] != 0 : true;
         const int bx = B % M.nb[0], by = (B / M.nb[0]) % M.nb[1], bz = (D == 3) ? B / (M.nb[0] * M.nb[1]) : 0;
         for (int q = lane; q < NPB; q += 32) {
             int idx[3];
@@ -693,22 +713,34 @@ cudaError_t launch_mark_touched(int dim, const int* nbv, const BinBuffers& b, un
     return cudaGetLastError();
 }
 
+cudaError_t launch_touched_list(const unsigned char* cur, const unsigned char* prev, int nblocks, int* list,
+                                int* count, const LaunchCfg& cfg) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), cfg.stream);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min((nblocks + 255) / 256, cfg.num_sms * 8));
+    KernelScope ks(cfg, "grid_mark");
+    touched_list_kernel<<<grid, 256, 0, cfg.stream>>>(cur, prev, nblocks, list, count);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
 template <int D, class T, int BW>
-cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const unsigned char* cur,
-                               const unsigned char* prev, const LaunchCfg& cfg) {
+cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const int* list, const int* count,
+                               const LaunchCfg& cfg) {
     const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_zero");
-    node_block_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, cur, prev);
+    node_list_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, nullptr, list, count);
     ++*cfg.launches;
     return cudaGetLastError();
 }
 
 template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
-                                      const unsigned char* cur, const unsigned char* prev, const LaunchCfg& cfg) {
+                                      const unsigned char* cur, const int* list, const int* count,
+                                      const LaunchCfg& cfg) {
     const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_update");
-    node_block_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, prev);
+    node_list_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, list, count);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -746,11 +778,11 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
     template cudaError_t launch_wave_speed<D, T>(const PView<T>&, const Scalars<T>&, unsigned long long*,    \
                                                  const LaunchCfg&);
 #define TB_INST_TB(D, T, BW)                                                                                 \
-    template cudaError_t launch_sparse_zero<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const unsigned char*, \
-                                                      const unsigned char*, const LaunchCfg&);                 \
+    template cudaError_t launch_sparse_zero<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const int*,         \
+                                                      const int*, const LaunchCfg&);                           \
     template cudaError_t launch_sparse_grid_update<D, T, BW>(const DMesh<D, T>&, const GView<T>&,              \
                                                              const Scalars<T>&, const unsigned char*,          \
-                                                             const unsigned char*, const LaunchCfg&);          \
+                                                             const int*, const int*, const LaunchCfg&);        \
     template cudaError_t launch_g2p<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,         \
                                               const Scalars<T>&, const BinBuffers&, const LaunchCfg&, bool);
 
