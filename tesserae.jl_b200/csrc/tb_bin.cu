@@ -7,8 +7,8 @@
 //   scan     3 launches over packed (count | nonempty << 32) 64-bit sums: tile
 //            reduce, single-CTA spine, tile rescan writing offsets, cursors,
 //            the compacted block list and the totals [nactive, nassigned]
-//   scatter  one thread per particle: a warp reserves one run per distinct
-//            block with a single atomic and writes its particles in lane order
+//   scatter  a warp takes 4 chunks of 32 ids and reserves one run per (chunk,
+//            distinct block) with a single atomic, writing the particles in lane order
 //   fixup    one warp per non-empty block: the block's segment is a set of runs,
 //            one per scatter warp (32 consecutive particle ids), each ascending;
 //            the runs are ranked by warp id and copied in order. Blocks of more
@@ -140,18 +140,35 @@ __global__ void __launch_bounds__(256) scan_finalize_kernel(const int* __restric
     }
 }
 
+// Each warp scatters SCAT_IT chunks of 32 consecutive ids: all their block ids
+// are loaded, and all their run reservations issued, before any is waited for
+// (one round trip each instead of one per chunk). A chunk still reserves one
+// run per block, so the runs the fix-up orders are those of one warp per chunk.
+constexpr int SCAT_IT = 4;
 __global__ void __launch_bounds__(256) bin_scatter_kernel(const int* __restrict__ blockids, long long n,
                                                           int* __restrict__ cursors, int* __restrict__ perm_tmp) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = p < n ? blockids[p] : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int leader = __ffs(peers) - 1;
-    const int rank = __popc(peers & lanemask_lt());
-    int base = 0;
-    if (b > 0 && lane == leader) base = atomicAdd(&cursors[b - 1], __popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (b > 0) perm_tmp[base + rank] = int(p);
+    const long long c0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32ll * SCAT_IT);
+    int b[SCAT_IT];
+#pragma unroll
+    for (int u = 0; u < SCAT_IT; ++u) {
+        const long long p = c0 + 32 * u + lane;
+        b[u] = p < n ? blockids[p] : -1;
+    }
+    unsigned peers[SCAT_IT];
+    int base[SCAT_IT];
+#pragma unroll
+    for (int u = 0; u < SCAT_IT; ++u) {
+        peers[u] = __match_any_sync(full, b[u]);
+        base[u] = 0;
+        if (b[u] > 0 && lane == __ffs(peers[u]) - 1) base[u] = atomicAdd(&cursors[b[u] - 1], __popc(peers[u]));
+    }
+#pragma unroll
+    for (int u = 0; u < SCAT_IT; ++u) {
+        const int bb = __shfl_sync(full, base[u], __ffs(peers[u]) - 1);
+        if (b[u] > 0) perm_tmp[bb + __popc(peers[u] & lanemask_lt())] = int(c0 + 32 * u + lane);
+    }
 }
 
 constexpr int FIX_THREADS = 256;
@@ -480,7 +497,8 @@ cudaError_t launch_bin_rest(int nb, long long n, const BinBuffers& b, const Laun
     if (n > 0) {
         {
             KernelScope ks(cfg, "bin_scatter");
-            bin_scatter_kernel<<<grid_for(n, 256), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors, b.perm_tmp);
+            bin_scatter_kernel<<<grid_for(n, 256 * SCAT_IT), 256, 0, cfg.stream>>>(b.blockids, n, b.cursors,
+                                                                                  b.perm_tmp);
         }
         // Blocks of more than FIXW_RUNS runs go to an overflow list kept in the
         // cursor array (free once the scatter is done), its length in partials[0].
