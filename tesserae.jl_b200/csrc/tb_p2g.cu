@@ -5,37 +5,41 @@
 // One CTA per non-empty grid block (grid-stride over the device block list).
 // The block's particles reach the (BW+3)^D-node halo tile [BW b - 1, BW b + BW + 1]
 // per axis; every support window starts at one of (BW+1)^D tile positions
-// ("groups"; particles of a group share their window).
+// ("groups"; particles of a group share their window). Two kernels share this
+// schedule.
 //
-// Per batch of up to NR particles of the block (one batch for a cube3d block):
-//   1. each thread evaluates the basis of its particles once (per-axis values
-//      and h_inv-scaled derivatives, zero past a truncated window) and writes a
-//      record (m_p, m_p v_p, S = -V_p sigma_p, the axis jets; for WLS/APIC also
-//      x_p, v_p, the moment inverse and B_p) to shared memory, then the batch is
-//      counting-sorted by group;
-//   2. a lane walks a pencil of groups along x (same window start in y, z)
-//      for one (y, z) row of the window and keeps the row's 3 x-nodes in
-//      registers; 9 rows x 3 pencils fill a warp in 3D (3 rows x 10 in 2D).
-//      Per particle and row the factors wy*wz, dy*wz, wy*dz and the force rows
-//      a = S[:,0] wy wz, b = S[:,1] dy wz + S[:,2] wy dz are formed once, so
-//      each of the row's nodes costs w = wx wyz, m += w m_p, mv += w (m_p v_p),
-//      f += dx a + wx b;
-//   3. after each group the x-node the window leaves for good is added to the
-//      shared tile and the row shifts one node (the pencil loop is unrolled, so
-//      the shift is a register rename): a pencil of G groups adds (G + 2) x 9
-//      node sums instead of 27 G. Lanes of a warp touch distinct nodes; only
-//      warps collide.
-// The tile accumulates in FP64 in both forms. For FP32 data this is the
-// compensated accumulation: FP64 holds the exact sum of up to 2^29 FP32 terms of
-// equal exponent, costs the same 8 bytes per value as a (hi, lo) FP32 Kahan pair,
-// and a shared-memory f64 atomic add runs at 1.8x the rate of an FP32 atomic add
-// followed by an exact two-sum of its rounding error (1.50 vs 0.84 T op/s
-// measured on B200). A plain FP32 tile without compensation would save 0.45 ms
-// of a 4.9 ms cube3d step. After the last batch the tile is flushed with one global
-// atomic per non-zero node value (gravity, sum w m g = g sum w m, is added there
-// from the tile mass). (Writing the tiles to a staging array and summing the at
-// most 2^D tiles of each node in a fused grid pass was measured slower on
-// cube3d: 3.26 vs 3.04 ms for P2G plus the grid work.)
+// p2g_pencil_kernel (B-spline, uGIMP, KernelCorrection; FLIP/PIC). Per batch of
+// up to NR particles of the block (one batch for a cube3d block):
+//   1. every global load of the batch is issued first; each thread finds its
+//      particles' groups and ranks within them (shared counters, then a group
+//      scan), and writes a record per particle at its group-sorted slot: on
+//      interior blocks (no window clipped) a compact 14-word record (m_p,
+//      m_p v_p, S = -V_p sigma_p, the in-window offset t; in 3D FP32 laid out
+//      for packed FP32x2 arithmetic), else the full 28-word record with the
+//      axis jets. Each pencil's records start 2 words further on, so the
+//      pencils a warp sweeps together read distinct banks;
+//   2. a lane walks a pencil of groups along x (same window start in y, z) for
+//      one (y, z) row of the window and keeps the row's 3 x-nodes in registers;
+//      9 rows x 3 pencils fill a warp in 3D (3 rows x 10 in 2D). Per particle
+//      and row the factors wy*wz, dy*wz, wy*dz and the force rows
+//      a = S[:,0] wy wz, b = S[:,1] dy wz + S[:,2] wy dz are formed once, so each
+//      of the row's nodes costs w = wx wyz, m += w m_p, mv += w (m_p v_p),
+//      f += dx a + wx b; after each group the x-node the window leaves for good
+//      is stored to the lane's own slot of a staging array (plain stores) and
+//      the row shifts one node (a register rename in the unrolled loop);
+//   3. one thread per tile node sums the at most 9 staged partials that reach
+//      it in FP64 and adds the node to the grid with one global atomic per
+//      non-zero value (gravity, sum w m g = g sum w m, from the summed mass).
+//   Interior blocks run in one launch (MODE 1), which appends every other block
+//   to a list that a second launch (MODE 2, full records) then takes one block
+//   per CTA; MODE 0 takes every block with full records.
+//
+// p2g_group_kernel (WLS weights, APIC): the same group sort and pencil sweep
+// with the general per-node weight (moment inverse, APIC affine term), the
+// rows' x-nodes added to an FP64 shared tile with shared atomics, and the tile
+// flushed with one global atomic per non-zero node value. FP64 holds the exact
+// sum of up to 2^29 FP32 terms of equal exponent, at the same 8 bytes per value
+// as a (hi, lo) FP32 Kahan pair.
 #include "tb_launch.cuh"
 
 namespace tb {
