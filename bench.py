@@ -400,6 +400,13 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
         "backward_ms_per_step": bwd_ms / nsteps,
         "grad_v0_norm": gnorm_v, "grad_logE_norm": gnorm_logE,
         "backward_kernels_ms_per_step": {k: v[1] / every for k, v in sorted(kt.items())},
+        # the backward step's two parts: the forward recomputed from the last
+        # checkpoint (binning, P2G, grid, G2P kernels) and the adjoint kernels
+        "backward_split": {
+            "recompute_ms_per_step": sum(v[1] for k, v in kt.items() if not k.startswith("adj_")) / every,
+            "adjoint_kernels_ms_per_step": sum(v[1] for k, v in kt.items() if k.startswith("adj_")) / every,
+            "adjoint_kernels_over_forward": sum(v[1] for k, v in kt.items() if k.startswith("adj_")) / every
+                                            / (fwd_ms / nsteps)},
         "fd_check": {"against": "central differences of the FP64 device rollout, L = sum c . x_T, random c",
                      "max_rel_err": max(ch["rel_err_f64"] for ch in checks),
                      "max_rel_err_fp32_tape": max(ch["rel_err_f32"] for ch in checks), "directions": checks},
