@@ -160,6 +160,23 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.source}
 
 
+def max_over_ranks(v: float, dist=None, device: str = "cuda") -> float:
+    """The max of a per-rank time over all ranks (every rank gets it): the
+    job-level time of N replicas. `dist` is torch.distributed or None (one rank)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, n: int, steps: int, ms: float) -> float:
+    """Whole-job particle-steps/s of `world` replicas of an n-particle workload
+    that each ran `steps` steps, the slowest in `ms` milliseconds."""
+    return world * n * steps / (ms * 1e-3)
+
+
 def measured_peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -493,12 +510,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def max_over_ranks_here(v: float) -> float:
+        return max_over_ranks(v, dist, "cuda")
 
     def timed_steps(P, G, part, K):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -523,8 +536,8 @@ def main():
         ctx.synchronize()
         score = runtime.block_ordered_particle_contiguity(part, n, ctx=ctx)
         ms, _ = timed_steps(P, G, part, args.steps)
-        ms = max_over_ranks(ms)
-        gen_order = {"value": world * n * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+        ms = max_over_ranks_here(ms)
+        gen_order = {"value": job_throughput(world, n, args.steps, ms), "ms_per_step": ms / args.steps,
                      "contiguity": score,
                      "order": "generation order (column-major lattice), headline form"}
         del P, part, G
@@ -544,7 +557,7 @@ def main():
         ctx.synchronize()
         with ClockSampler(local) as clk:
             ms, launches = timed_steps(P, G, part, args.steps)
-        ms = max_over_ranks(ms)
+        ms = max_over_ranks_here(ms)
         # per-kernel device time, profiled separately (events add launch gaps)
         ctx.profile(True)
         runtime.step(G, P, part, mesh, prm, 3, ctx=ctx)
@@ -557,7 +570,7 @@ def main():
     if args.quick:
         if rank == 0:
             hd = results["x64"]
-            print(json.dumps({"metric": METRIC, "value": world * n * args.steps / (hd["ms"] * 1e-3),
+            print(json.dumps({"metric": METRIC, "value": job_throughput(world, n, args.steps, hd["ms"]),
                               "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
                               "warmup": args.warmup, "ms_per_step": hd["ms"] / args.steps, "quick": True,
                               "kernels_ms_per_step": {k: v[1] / 3 for k, v in sorted(hd["kernels"].items())}}),
@@ -605,11 +618,11 @@ def main():
     for _ in range(calls):
         runtime.rollout_host(hostp, mesh, prm, S, ctx=ctx)
     barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks_here(time.perf_counter() - t0)
     # in: x, v, V, sigma, F (the step's inputs); out: the same and grad_v (written by every G2P)
     in_bytes = hostp.x.nbytes + hostp.v.nbytes + hostp.V.nbytes + hostp.sigma.nbytes + hostp.F.nbytes
     out_bytes = in_bytes + hostp.grad_v.nbytes
-    e2e = {"value": world * n * S * calls / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": in_bytes,
+    e2e = {"value": job_throughput(world, n, S * calls, 1e3 * e2e_s), "unit": "particle-steps/s", "h2d_bytes_per_step": in_bytes,
            "d2h_bytes_per_step": out_bytes, "mpm_steps_per_call": S,
            "note": "one bench step = one tb_rollout_host_f32x64 call on pinned host buffers (H2D, S steps, D2H)"}
     del hostp
@@ -656,7 +669,7 @@ def main():
     f32, f64 = results["f32"], results["f64"]
     out = {
         "metric": METRIC,
-        "value": world * n * args.steps / (hd["ms"] * 1e-3),
+        "value": job_throughput(world, n, args.steps, hd["ms"]),
         "unit": "particle-steps/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -677,9 +690,9 @@ def main():
                                      "the CPU baseline time the same order; generation order under "
                                      "generation_order)"},
         "accuracy": acc,
-        "fp32_positions": {"value": world * n * args.steps / (f32["ms"] * 1e-3), "ms_per_step": f32["ms"] / args.steps,
+        "fp32_positions": {"value": job_throughput(world, n, args.steps, f32["ms"]), "ms_per_step": f32["ms"] / args.steps,
                            "form": FORMS["f32"][2], "accuracy": acc_f32},
-        "fp64_plain": {"value": world * n * args.steps / (f64["ms"] * 1e-3), "ms_per_step": f64["ms"] / args.steps},
+        "fp64_plain": {"value": job_throughput(world, n, args.steps, f64["ms"]), "ms_per_step": f64["ms"] / args.steps},
         "generation_order": gen_order,
         "adjoint_over_forward": adjoint,
         "taylor_impact": taylor,
