@@ -97,6 +97,7 @@ struct tb_ctx {
     long long grid_nblocks = 0;
     bool grid_sparse_ok = false;     // the flags describe every non-zero node of grid_key
     bool grid_dense_pending = false; // last P2G zeroed densely: the next grid half runs densely too
+    bool grid_zeroed = false;        // the last grid half zeroed m, mv, f of its blocks once read
     EventProfiler* prof = nullptr;
     // context-owned state for tb_rollout_host_*
     void* roll_buf = nullptr;
@@ -388,13 +389,16 @@ template <int D, class T, int BW>
 cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G,
                           const Scalars<T>& S, const BinBuffers& B, const LaunchCfg& cfg) {
     const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks;
+    // after a grid half that zeroed its blocks once read, every P2G target is zero
+    const bool zeroed = known && c->grid_zeroed;
+    c->grid_zeroed = false;
     std::swap(c->touched_cur, c->touched_prev);
     cudaError_t e = cudaMemsetAsync(c->touched_cur, 0, size_t(M.nblocks), cfg.stream);
     if (e == cudaSuccess && !known) e = cudaMemsetAsync(c->touched_prev, 0, size_t(M.nblocks), cfg.stream);
     if (e == cudaSuccess) e = launch_mark_touched(D, M.nb, B, c->touched_cur, M.nblocks, cfg);
     if (e == cudaSuccess)
         e = launch_touched_list(c->touched_cur, c->touched_prev, M.nblocks, c->touched_list, c->touched_count, cfg);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && !zeroed)
         e = known ? launch_sparse_zero<D, T, BW>(M, G, c->touched_list, c->touched_count, cfg)
                   : launch_grid_zero<D, T>(M, G, cfg);
     if (e == cudaSuccess) e = launch_p2g<D, T, BW>(M, P, G, S, B, cfg);
@@ -406,15 +410,23 @@ cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, co
 }
 
 // Grid half: over the touched node blocks when the flags describe this grid
-// (zeroing v and vn of blocks touched only before), else over every node.
+// (zeroing v and vn of blocks touched only before), else over every node. With
+// zero_after (a later step of the same call scatters into this grid again, so
+// the caller cannot see m, mv, f in between) the sparse half also zeroes m, mv,
+// f of the blocks it reads, and the next P2G skips its zero pass.
 template <int D, class T, int BW>
 cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& S,
-                                        const LaunchCfg& cfg) {
+                                        const LaunchCfg& cfg, bool zero_after = false) {
     const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks &&
                        !c->grid_dense_pending;
     c->grid_dense_pending = false;
-    if (known)
-        return launch_sparse_grid_update<D, T, BW>(M, G, S, c->touched_cur, c->touched_list, c->touched_count, cfg);
+    c->grid_zeroed = false;
+    if (known) {
+        const cudaError_t e = launch_sparse_grid_update<D, T, BW>(M, G, S, c->touched_cur, c->touched_list,
+                                                                  c->touched_count, cfg, zero_after);
+        c->grid_zeroed = zero_after && e == cudaSuccess;
+        return e;
+    }
     return launch_grid_update<D, T>(M, G, S, cfg);
 }
 
@@ -449,6 +461,7 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
         if ((rc = reorder_args(c, part, P.n, reorder_threshold, RA)) != TB_OK) return rc;
     }
     c->grid_sparse_ok = false;  // the first step of every call runs densely
+    c->grid_zeroed = false;
     // Inside one call, the G2P of step s counts the particles into blocks for
     // step s + 1 (the count pass of its binning); the last step does not, so the
     // partition left to the caller is the last step's own.
@@ -463,12 +476,14 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
         if (e == cudaSuccess && reorder) e = launch_reorder_score(RA, cfg);
         if (e == cudaSuccess && reorder) e = launch_reorder_apply(RA, fields.data(), int(fields.size()), cfg);
         if (e == cudaSuccess && do_p2g) e = p2g_with_zero<D, T, BW>(c, M, P, G, S, B, cfg);
-        if (e == cudaSuccess && do_grid) e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg);
+        if (e == cudaSuccess && do_grid)
+            e = grid_update_sparse_or_dense<D, T, BW>(c, M, G, S, cfg, do_p2g && s + 1 < nsteps);
         if (e == cudaSuccess && do_g2p) {
             e = launch_g2p<D, T, BW>(M, G, P, S, B, cfg, count_next);
             counted = count_next;
         }
     }
+    c->grid_zeroed = false;  // a P2G outside this call zeroes for itself
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     return TB_OK;
 }

@@ -94,7 +94,7 @@ cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const in
 template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
                                       const unsigned char* cur, const int* list, const int* count,
-                                      const LaunchCfg& cfg);
+                                      const LaunchCfg& cfg, bool zero_after = false);
 
 // max over the particles of sqrt((lambda + 2 mu) / (m / V)) + |v| into *out
 // (the bits of a double).

@@ -111,11 +111,14 @@ __global__ void __launch_bounds__(256) touched_list_kernel(const unsigned char* 
 }
 
 // One warp per listed node block. mode 0: zero m, mv, f; mode 1: grid update
-// where cur, zero v, vn where the block was touched by the previous transfer only.
+// where cur, zero v, vn where the block was touched by the previous transfer only;
+// with zero_after, m, mv and f of the cur blocks are zeroed once read (the next
+// P2G of the same call then needs no zero pass).
 template <int D, class T, int BW, int MODE>
 __global__ void __launch_bounds__(256) node_list_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s,
                                                         const unsigned char* __restrict__ cur,
-                                                        const int* __restrict__ list, const int* __restrict__ count) {
+                                                        const int* __restrict__ list, const int* __restrict__ count,
+                                                        int zero_after) {
     constexpr int NPB = (D == 3) ? BW * BW * BW : BW * BW;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -161,6 +164,14 @@ __global__ void __launch_bounds__(256) node_list_kernel(DMesh<D, T> M, GView<T> 
                     }
                     G.vn[d][I] = vn;
                     G.v[d][I] = v;
+                }
+                if (zero_after && c) {
+                    G.m[I] = T(0);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        G.mv[d][I] = T(0);
+                        G.f[d][I] = T(0);
+                    }
                 }
             }
         }
@@ -729,7 +740,7 @@ cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const in
                                const LaunchCfg& cfg) {
     const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_zero");
-    node_list_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, nullptr, list, count);
+    node_list_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, nullptr, list, count, 0);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -737,10 +748,10 @@ cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const in
 template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
                                       const unsigned char* cur, const int* list, const int* count,
-                                      const LaunchCfg& cfg) {
+                                      const LaunchCfg& cfg, bool zero_after) {
     const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_update");
-    node_list_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, list, count);
+    node_list_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, list, count, zero_after ? 1 : 0);
     ++*cfg.launches;
     return cudaGetLastError();
 }
@@ -782,7 +793,7 @@ cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const
                                                       const int*, const LaunchCfg&);                           \
     template cudaError_t launch_sparse_grid_update<D, T, BW>(const DMesh<D, T>&, const GView<T>&,              \
                                                              const Scalars<T>&, const unsigned char*,          \
-                                                             const int*, const int*, const LaunchCfg&);        \
+                                                             const int*, const int*, const LaunchCfg&, bool);  \
     template cudaError_t launch_g2p<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,         \
                                               const Scalars<T>&, const BinBuffers&, const LaunchCfg&, bool);
 
