@@ -191,3 +191,19 @@ def test_block_ordered_scene_is_the_partition_order(tb, oracle):
     assert np.array_equal(part.particleindices, np.arange(1, sc.particles.n + 1))
     after = {tuple(np.r_[sc.particles.x[:, p], sc.particles.v[:, p]]) for p in range(sc.particles.n)}
     assert before == after
+
+
+def test_block_order_is_the_same_workload(tb, oracle):
+    """The bench stores the particles in block order: the same particles advance
+    the same way (2 FP64 oracle steps), up to the order of the P2G sums."""
+    a = tb.scenes.cube3d(scale=16)
+    b = tb.scenes.block_ordered(tb.scenes.cube3d(scale=16))
+    order = tb.scenes._sort_by_block(a.mesh, a.particles.x)
+    assert np.array_equal(b.particles.x, a.particles.x[:, order])
+    for sc in (a, b):
+        G = tb.generate_grid(sc.mesh)
+        oracle.step_parallel(sc.mesh, sc.particles, G, sc.params, 2, 1)
+    for k in ("x", "v", "F"):
+        ref = getattr(a.particles, k)[..., order]
+        got = getattr(b.particles, k)
+        assert np.allclose(got, ref, rtol=0, atol=1e-12 * np.abs(ref).max()), k
