@@ -14,9 +14,10 @@
  * Precision forms (the `_f64` / `_f32` suffix):
  *   _f64  "plain": every array is double. Drop-in for `gpu_preserve` data.
  *   _f32  "mixed": every array is float EXCEPT the deformation gradient F,
- *         which stays double; weights, P2G and G2P run in FP32, the P2G
- *         shared-memory tiles accumulate the FP32 contributions in FP64
- *         (compensated accumulation), and F update, det F and log J run in
+ *         which stays double; weights, P2G and G2P run in FP32 (each P2G lane
+ *         sums its particles' contributions to a node in plain FP32 registers;
+ *         the few partial sums that reach a node are added in FP64 before the
+ *         one global atomic per node), and F update, det F and log J run in
  *         FP64. Drop-in for `gpu` (Float32-cast) data plus an FP64 F array.
  *
  * Index conventions follow the reference (Julia, column-major, 1-based):
@@ -148,7 +149,8 @@ typedef struct tb_step_params {
     double lambda;      /* Lame lambda when particles.lambda == NULL */
     double gravity[3];  /* body acceleration added to f as w m g */
     double gimp_l;      /* uGIMP particle length when particles.l == NULL */
-    double flip_alpha;  /* FLIP blend: v_p = sum w ((1-a) v_i + a (v_p + v_i - vn_i)); 1 = README FLIP */
+    double flip_alpha;  /* FLIP blend: v_p = (1-a) sum w v_i + a (v_p + sum w (v_i - vn_i)), the blend of
+                           test/transfer.jl:111-133; 1 = README FLIP (v_p += sum w (v_i - vn_i)) */
     int32_t basis;      /* enum tb_basis_kind */
     int32_t transfer;   /* enum tb_transfer_kind */
     int32_t material;   /* enum tb_material_kind */
@@ -377,10 +379,13 @@ int32_t tb_tape_backward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* par
  * TB_NOALLOC_MAX_PARTICLES particles or TB_NOALLOC_MAX_BLOCKS grid blocks are
  * rejected with TB_ERR_CAPACITY. It runs on the current device and `stream`,
  * synchronises `stream` once to read the totals, and writes a message into
- * `errbuf` (may be NULL) on error. The first call on a device looks the scratch
- * up (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the scratch: calls that overlap on the GPU race, so serialise
- * them. */
+ * `errbuf` (may be NULL) on error. Every call looks the scratch up with
+ * cudaGetSymbolAddress on the current device (so a device reset, which may move
+ * it, is harmless). The first call on a device may load the library's device
+ * code (lazy loading), which is when the driver reserves the array: make one
+ * warm-up call per device during start-up, before any stream capture; later
+ * calls allocate nothing. All calls share the scratch: calls that overlap on
+ * the GPU race, so serialise them. */
 #define TB_NOALLOC_MAX_PARTICLES (1 << 20)
 #define TB_NOALLOC_MAX_BLOCKS (1 << 20)
 int32_t tb_bin_particles_noalloc(const tb_mesh* mesh, const tb_particles* particles, int32_t precision,

@@ -6,12 +6,13 @@ weights, the block partition and the recognised @P2G / @G2P equation sets) that
 calls the CUDA kernels through the C ABI declared in include/tesserae_b200.h.
 """
 from . import _abi
-from .state import (Adjoint, BasisWeights, CartesianMesh, Grid, Particles, Partition, generate_basis_weights,
-                    generate_grid, lame, step_params)
+from .state import (Adjoint, BasisWeights, CartesianMesh, Grid, GridSampling, Particles, Partition,
+                    generate_basis_weights, generate_grid, generate_particles, generate_points, lame, step_params)
 from . import export, scenes
 
-__all__ = ["_abi", "Adjoint", "BasisWeights", "CartesianMesh", "Grid", "Particles", "Partition", "generate_basis_weights",
-           "generate_grid", "lame", "step_params", "scenes", "export"]
+__all__ = ["_abi", "Adjoint", "BasisWeights", "CartesianMesh", "Grid", "GridSampling", "Particles", "Partition",
+           "generate_basis_weights", "generate_grid", "generate_particles", "generate_points", "lame", "step_params",
+           "scenes", "export"]
 
 
 def __getattr__(name):

@@ -17,7 +17,6 @@
 // serialise them. The array keeps the previous call's contents; every scratch
 // word a call reads is written earlier in the same call, so nothing is cleared.
 #include <cstdio>
-#include <mutex>
 
 #include "tb_launch.cuh"
 
@@ -38,36 +37,28 @@ constexpr size_t kBytes = kOffTotals + 256;
 
 __device__ __align__(256) unsigned char tb_noalloc_scratch[kBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
-
 void report(char* errbuf, int32_t errlen, const char* msg) {
     if (errbuf && errlen > 0) std::snprintf(errbuf, size_t(errlen), "%s", msg);
 }
 
 // Device address of the scratch array on the current device. In host code the
-// symbol names a host-side stand-in, so the address is looked up once per
-// device (with that device current) and cached.
-int scratch_address(int device, void** out, char* errbuf, int32_t errlen) {
-    if (device < 0 || device >= kMaxDevices) {
-        report(errbuf, errlen, "tb_bin_particles_noalloc: device ordinal out of range");
-        return TB_ERR_ARG;
+// symbol names a host-side stand-in, so the address is looked up with the
+// device current. It is looked up on every call, not cached: after
+// cudaDeviceReset (or any teardown of the primary context) the module is
+// loaded again and the array can move. Once the module is loaded the lookup
+// allocates nothing; the first call on a device may load the module (lazy
+// loading), which is when the driver reserves the array.
+int scratch_address(void** out, char* errbuf, int32_t errlen) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, tb_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "tb_bin_particles_noalloc: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+        report(errbuf, errlen, msg);
+        return TB_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, tb_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            char msg[256];
-            std::snprintf(msg, sizeof msg, "tb_bin_particles_noalloc: cudaGetSymbolAddress failed: %s",
-                          cudaGetErrorString(e));
-            report(errbuf, errlen, msg);
-            return TB_ERR_CUDA;
-        }
-        g_addr[device] = p;
-    }
-    *out = g_addr[device];
+    *out = p;
     return TB_OK;
 }
 
@@ -166,7 +157,7 @@ extern "C" int32_t tb_bin_particles_noalloc(const tb_mesh* mesh, const tb_partic
         return TB_ERR_CUDA;
     }
     void* scratch = nullptr;
-    const int rc = scratch_address(device, &scratch, errbuf, errlen);
+    const int rc = scratch_address(&scratch, errbuf, errlen);
     if (rc != TB_OK) return rc;
     unsigned char* s = static_cast<unsigned char*>(scratch);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -738,7 +738,7 @@ cudaError_t launch_touched_list(const unsigned char* cur, const unsigned char* p
 template <int D, class T, int BW>
 cudaError_t launch_sparse_zero(const DMesh<D, T>& M, const GView<T>& G, const int* list, const int* count,
                                const LaunchCfg& cfg) {
-    const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
+    const int grid = int(std::max(1ll, std::min((M.nblocks * 32ll + 255) / 256, cfg.num_sms * 16ll)));
     KernelScope ks(cfg, "grid_zero");
     node_list_kernel<D, T, BW, 0><<<grid, 256, 0, cfg.stream>>>(M, G, Scalars<T>{}, nullptr, list, count, 0);
     ++*cfg.launches;
@@ -749,7 +749,7 @@ template <int D, class T, int BW>
 cudaError_t launch_sparse_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s,
                                       const unsigned char* cur, const int* list, const int* count,
                                       const LaunchCfg& cfg, bool zero_after) {
-    const int grid = std::max(1, std::min((M.nblocks * 32 + 255) / 256, cfg.num_sms * 16));
+    const int grid = int(std::max(1ll, std::min((M.nblocks * 32ll + 255) / 256, cfg.num_sms * 16ll)));
     KernelScope ks(cfg, "grid_update");
     node_list_kernel<D, T, BW, 1><<<grid, 256, 0, cfg.stream>>>(M, G, s, cur, list, count, zero_after ? 1 : 0);
     ++*cfg.launches;

@@ -24,7 +24,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from .state import CartesianMesh, Particles, lame, step_params
+from .state import CartesianMesh, GridSampling, Particles, generate_points, lame, step_params
 
 SEEDS = {"readme2d": 0, "cube3d": 20260001, "clusters3d": 20260002, "sphere3d": 20260003,
          "dambreak3d": 20260004, "taylor3d": 20260005}
@@ -59,8 +59,7 @@ def readme2d(scale: int = 1) -> Scene:
     h = 0.01
     L = 1.0 / scale
     mesh = CartesianMesh(h, (0.0, L), (0.0, L))
-    ax = grid_sampling_axis(0.0, L, h)
-    pts = _lattice([ax, ax])
+    pts = generate_points(GridSampling(), mesh)
     npre = pts.shape[1]
     V0 = (L * L) / npre
     rho0, E, nu = 1e3, 500.0, 0.3
@@ -90,9 +89,8 @@ def cube3d(scale: int = 1, seed: int | None = None) -> Scene:
     L = cells * h
     mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
     lpart = h / 2
-    k = np.arange(cells // 2, 3 * cells // 2)  # particles per axis inside [L/4, 3L/4]
-    ax = (2.0 * k + 1.0) * (lpart / 2.0)
-    pts = _lattice([ax, ax, ax])
+    # GridSampling over the mesh, kept inside the centre cube [L/4, 3L/4]^3
+    pts = generate_points(GridSampling(), mesh, box=[(L / 4, 3 * L / 4)] * 3)
     n = pts.shape[1]
     rng = np.random.default_rng(SEEDS["cube3d"] if seed is None else seed)
     P = Particles(n, 3, np.float64)
@@ -186,8 +184,7 @@ def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
     L = cells * h
     mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
     rng = np.random.default_rng(SEEDS["sphere3d"] if seed is None else seed)
-    ax = grid_sampling_axis(0.0, L, h, spacing=0.25)
-    pts = _lattice([ax, ax, ax])
+    pts = generate_points(GridSampling(0.25), mesh)
     c, r = 0.5 * L, 0.3 * L
     keep = np.sum((pts - c) ** 2, axis=0) < r * r
     pts = pts[:, keep]
@@ -219,8 +216,7 @@ def dambreak3d(scale: int = 1) -> Scene:
     h = 1.0 / 384
     L = cells * h
     mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
-    axx = grid_sampling_axis(0.0, L, h)
-    pts = _lattice([axx[axx < 0.4 * L], axx, axx[axx < 0.8 * L]])
+    pts = generate_points(GridSampling(), mesh, box=[(0.0, 0.4 * L), None, (0.0, 0.8 * L)])
     n = pts.shape[1]
     P = Particles(n, 3, np.float64, optional=("B",))
     P.x[...] = pts

@@ -363,6 +363,58 @@ class BasisWeights:
         return s
 
 
+@dataclass(frozen=True)
+class GridSampling:
+    """GridSampling(spacing = 1/2) (src/particles.jl:3-11): particles aligned with
+    the grid at `spacing * h`, so `spacing = 1/k` gives k^dim particles per cell."""
+
+    spacing: float = 0.5
+
+
+def generate_points(alg: GridSampling, mesh: CartesianMesh, box=None) -> np.ndarray:
+    """The sample points of `alg` over `mesh` (src/particles.jl:13-18), shape
+    (dim, n) in the reference's column-major order: per axis
+    `(xmin + l/2):l:xmax` with `l = spacing * h`. `box` (one (lo, hi) pair per
+    axis, or None) keeps the points with lo <= x <= hi on every axis: the same
+    points, in the same order, as filtering the whole lattice with that box,
+    without forming it (the lattice of a 256^3 mesh at 2 per cell per axis has
+    134 M points)."""
+    if not isinstance(alg, GridSampling):
+        raise TypeError("generate_points: only GridSampling is on the B200 path "
+                        "(PoissonDiskSampling is the third-party PoissonDiskSampling.jl)")
+    l = float(alg.spacing) * mesh.h
+    axes = []
+    for d in range(mesh.dim):
+        xmin = mesh.xmin[d]
+        xmax = mesh.xmin[d] + (mesh.n_nodes[d] - 1) * mesh.h
+        # Julia's (xmin + l/2):l:xmax: the largest k with xmin + l/2 + k l <= xmax
+        n = int(np.floor((xmax - (xmin + l / 2)) / l + 1e-9)) + 1
+        ax = xmin + (2.0 * np.arange(n) + 1.0) * (l / 2.0)
+        if box is not None and box[d] is not None:
+            lo, hi = box[d]
+            ax = ax[(ax >= lo) & (ax <= hi)]
+        axes.append(ax)
+    grids = np.meshgrid(*axes, indexing="ij")
+    return np.stack([g.reshape(-1, order="F") for g in grids])
+
+
+def generate_particles(mesh: CartesianMesh, alg: GridSampling = GridSampling(), dtype=np.float64,
+                       optional=(), backend="numpy", device=None, x64=False, box=None) -> Particles:
+    """generate_particles(ParticleProp, mesh; alg) (src/particles.jl:112-118): a
+    zero-initialised particle state (F = I, Cp_inv = I) with one particle per
+    sample point of `alg`, positions set from the points. The reference's
+    default `alg` is PoissonDiskSampling, a third-party algorithm that is not
+    on this path; GridSampling is the default here. `optional` names the
+    optional fields to allocate (m, l, B, V0, mu, lam, eps_p, Cp_inv); `box` is
+    the box filter of `generate_points`."""
+    pts = generate_points(alg, mesh, box)
+    P = Particles(pts.shape[1], mesh.dim, np.float64, optional=optional)
+    P.x[...] = pts
+    if backend == "numpy" and np.dtype(dtype) == np.float64 and not x64:
+        return P
+    return P.to(backend, device=device, dtype=dtype, x64=x64)
+
+
 def generate_grid(mesh: CartesianMesh, dtype=np.float64, backend="numpy", device=None) -> Grid:
     return Grid(mesh, dtype, backend, device)
 

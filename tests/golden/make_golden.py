@@ -5,7 +5,7 @@ are taken from the literal expectations in its test files and doctests. For each
 case this script checks that the cited reference line still says what the case
 records (provenance), then writes the case. Run from the repository root:
 
-    python tests/golden/make_golden.py [path/to/Tesserae.jl]
+    python tests/golden/make_golden.py path/to/Tesserae.jl
 
 The JSON is committed; tests read only the JSON.
 """
@@ -127,6 +127,14 @@ def main(ref_root: str):
             cases.append({"kind": "kc_positive", "dim": dim, "h": 1.0, "lims": [[0, k] for k in I], "nodes": nodes,
                           "L": 1.5, "source": src})
 
+    # generate_particles doctest (src/particles.jl:79-89): GridSampling() on
+    # CartesianMesh(0.5, (0,3), (0,2)) gives 96 particles, the first at (0.125, 0.125)
+    require(ref, "src/particles.jl", 79, "CartesianMesh(0.5, (0,3), (0,2))")
+    require(ref, "src/particles.jl", 81, "alg=GridSampling()")
+    require(ref, "src/particles.jl", 86, "(x = [0.125, 0.125]")
+    cases.append({"kind": "grid_sampling", "h": 0.5, "lims": [[0, 3], [0, 2]], "spacing": 0.5, "n": 96,
+                  "first": [0.125, 0.125], "source": require(ref, "src/particles.jl", 89, "96-element")})
+
     # Block-tile containment for 2D meshes of h = 0.02 (test/transfer.jl:941-957)
     cases.append({"kind": "tile_contains", "h": 0.02, "lims": [[0, 1], [0, 1]], "l": 0.01,
                   "bases": ["bspline_quadratic", "ugimp", "wls_bspline_quadratic"],
@@ -141,4 +149,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py path/to/Tesserae.jl")
+    main(sys.argv[1])

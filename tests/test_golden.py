@@ -207,3 +207,14 @@ def test_block_order_is_the_same_workload(tb, oracle):
         ref = getattr(a.particles, k)[..., order]
         got = getattr(b.particles, k)
         assert np.allclose(got, ref, rtol=0, atol=1e-12 * np.abs(ref).max()), k
+
+
+def test_grid_sampling_doctest(tb):
+    """generate_particles(ParticleProp, mesh; alg=GridSampling()) doctest
+    (src/particles.jl:79-89): 96 particles, the first at (0.125, 0.125)."""
+    for c in by_kind("grid_sampling"):
+        mesh = tb.CartesianMesh(c["h"], *[tuple(l) for l in c["lims"]])
+        P = tb.generate_particles(mesh, tb.GridSampling(c["spacing"]))
+        assert P.n == c["n"], c["source"]
+        assert list(P.x[:, 0]) == c["first"], c["source"]
+        assert np.all(P.v == 0) and np.all(P.F[[0, 3]] == 1) and np.all(P.F[[1, 2]] == 0)

@@ -56,6 +56,32 @@ def test_noalloc_matches_allocating_binning_twice(tb, ctx, dtype, precision):
         assert np.array_equal(da["particleindices"][:nass], db["particleindices"][:nass])
 
 
+def test_noalloc_allocates_nothing_after_warm_up(tb):
+    """After one warm-up call on the device (which may load the module and so
+    reserve the fixed array), further calls leave the device's free memory
+    unchanged: nothing is allocated, by the library or by the driver."""
+    rng = np.random.default_rng(7)
+    mesh = tb.CartesianMesh(1 / 64, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    n = 200_000
+    P = tb.Particles(n, 3, np.float32)
+    P.x[...] = rng.uniform(0.0, 1.0, size=(3, n)).astype(np.float32)
+    Pd = P.to("torch", device="cuda")
+    part = tb.Partition(mesh, n, backend="torch", device="cuda")
+    lib = tb._abi.load_library()
+    err = C.create_string_buffer(256)
+    stream = torch.cuda.current_stream().cuda_stream
+    args = (C.byref(mesh.struct()), C.byref(Pd.struct()), 1, C.byref(part.struct()), C.c_void_p(stream),
+            None, None, err, 256)
+    assert lib.tb_bin_particles_noalloc(*args) == tb._abi.TB_OK, err.value.decode()  # warm-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert lib.tb_bin_particles_noalloc(*args) == tb._abi.TB_OK, err.value.decode()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_oversized_input(tb):
     lib = tb._abi.load_library()
     mesh = tb.CartesianMesh(1 / 64, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
