@@ -214,6 +214,20 @@ def step_bytes(s: int, sx: int) -> tuple[int, int]:
     return per_p, per_n
 
 
+def config_bytes(s: int, sx: int, per_particle=(), apic: bool = False) -> tuple[int, int]:
+    """Algorithmic bytes of one whole step per particle and per active node for
+    a config: state scalars of `s` bytes, positions of `sx`, F FP64.
+    `per_particle` names the optional per-particle inputs (m and l read by P2G,
+    mu, lam and V0 by G2P). APIC reads B in P2G and writes it in G2P, and its
+    G2P reads neither the particle's old velocity nor the nodes' vn."""
+    p2g = 3 * sx + (3 + 1 + 6) * s + (9 * s if apic else 0) + s * sum(k in per_particle for k in ("m", "l"))
+    g2p_read = 3 * sx + (0 if apic else 3 * s) + 72 + s * sum(k in per_particle for k in ("mu", "lam", "V0", "l"))
+    g2p_write = 3 * sx + (3 + 9 + 6 + 1) * s + 72 + (9 * s if apic else 0)
+    per_p = (3 * sx + 8) + p2g + g2p_read + g2p_write
+    per_n = 7 * s + 7 * s + 6 * s + (3 * s if apic else 6 * s)
+    return per_p, per_n
+
+
 FORMS = {
     # name: (state dtype, FP64 positions, description)
     "x64": (np.float32, True, "mixed FP32 with FP64 positions (FP64 x, F, det F, log J; FP64-summed P2G partials)"),
@@ -430,6 +444,118 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
     }
 
 
+def _form_particles(tb, sc, name, device="cuda"):
+    """Device particles of scene `sc` in precision form `name` (x64 / f32 / f64)."""
+    dtype, x64, _ = FORMS[name]
+    if sc.meta.get("built_on_device"):
+        return tb.scenes.dambreak3d(scale=sc.meta["scale"], device=device, dtype=dtype).particles
+    return sc.particles.to("torch", device=device, dtype=dtype, x64=x64)
+
+
+def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: int, peak: float,
+               per_particle=(), apic=False) -> dict:
+    """One configuration: device time per step of each precision form (a fused
+    call of `steps` steps after `warmup`), its per-kernel split, the whole-step
+    and dominant-kernel roofline fractions, and the FP32 form's error against
+    the FP64 form after `acc_steps` steps from the same initial state."""
+    import torch
+    mesh, prm = sc.mesh, sc.params
+    out = {"n_particles": None, "steps": steps, "warmup": warmup, "forms": {}}
+    finals = {}
+    for name in forms:
+        P = _form_particles(tb, sc, name)
+        n = P.n
+        out["n_particles"] = n
+        dtype = FORMS[name][0]
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, P, part, mesh, prm, warmup, ctx=ctx)
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches
+        torch.cuda.synchronize()
+        e0.record()
+        runtime.step(G, P, part, mesh, prm, steps, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        launches = (ctx.launches - l0) / steps
+        nact = int((G.m != 0).sum())
+        ctx.profile(True)
+        runtime.step(G, P, part, mesh, prm, 3, ctx=ctx)
+        kt = ctx.profile_read()
+        ctx.profile(False)
+        s_b = np.dtype(dtype).itemsize
+        sx = 8 if FORMS[name][1] else s_b
+        bp, bn = config_bytes(s_b, sx, per_particle, apic)
+        alg = n * bp + nact * bn
+        kern = {k: v[1] / 3 for k, v in sorted(kt.items())}
+        dom = max(kern, key=kern.get)
+        out["forms"][name] = {
+            "form": FORMS[name][2], "ms_per_step": ms, "value": n / (ms * 1e-3), "launches_per_step": launches,
+            "active_nodes": nact, "bytes_per_particle": bp, "bytes_per_active_node": bn, "step_bytes": alg,
+            "step_roofline_frac": alg / (ms * 1e-3) / 1e9 / peak, "kernels_ms_per_step": kern,
+            "dominant_kernel": dom, "dominant_kernel_share": kern[dom] / sum(kern.values())}
+        del part, G, P
+        torch.cuda.empty_cache()
+        # accuracy run from the initial state
+        P = _form_particles(tb, sc, name)
+        part = tb.Partition(mesh, n, backend="torch", device="cuda")
+        G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+        x0 = P.x.double().clone()
+        runtime.step(G, P, part, mesh, prm, acc_steps, ctx=ctx)
+        ctx.synchronize()
+        finals[name] = {"x": P.x.double(), "v": P.v.double(), "x0": x0,
+                        "finite": bool(torch.isfinite(P.x).all() and torch.isfinite(P.v).all())}
+        del part, G, P
+        torch.cuda.empty_cache()
+    ref = finals.get("f64")
+    if ref is not None:
+        def rel(a, b):
+            return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        for name, f in finals.items():
+            if name == "f64":
+                continue
+            out["forms"][name]["accuracy"] = {
+                "steps": acc_steps, "rel_err_x": rel(f["x"], ref["x"]), "rel_err_v": rel(f["v"], ref["v"]),
+                "rel_err_displacement": rel(f["x"] - f["x0"], ref["x"] - ref["x0"]), "finite": f["finite"],
+                "against": "plain FP64 form on the device from the same initial state"}
+        fast = [k for k in forms if k != "f64"]
+        if fast:
+            out["fp32_over_fp64_speed"] = out["forms"]["f64"]["ms_per_step"] / out["forms"][fast[0]]["ms_per_step"]
+    del finals
+    torch.cuda.empty_cache()
+    return out
+
+
+def fullsize_oracle_check(tb, runtime, ctx, sc, nsteps: int = 3) -> dict:
+    """The plain FP64 device step against the FP64 oracle (the OpenMP
+    restatement of the reference's CPU step) on the full headline scene,
+    `nsteps` steps from the same state."""
+    om = load_oracle(tb)
+    orc = om.Oracle(tb._abi)
+    mesh, prm = sc.mesh, sc.params
+    P = sc.particles.to("torch", device="cuda", dtype=np.float64)
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    G = tb.generate_grid(mesh, np.float64, backend="torch", device="cuda")
+    runtime.step(G, P, part, mesh, prm, nsteps, ctx=ctx)
+    ctx.synchronize()
+    got = P.numpy()
+    del P, part, G
+    Pc = sc.particles.to("numpy")
+    Gc = tb.generate_grid(mesh)
+    t0 = time.perf_counter()
+    orc.step_parallel(mesh, Pc, Gc, prm, nsteps, om.cores())
+    cpu_s = time.perf_counter() - t0
+    out = {"steps": nsteps, "n_particles": Pc.n, "oracle_threads": om.cores(), "oracle_s": cpu_s,
+           "bound": 1e-9}
+    for k in ("x", "v", "F", "sigma", "V"):
+        ref = getattr(Pc, k)
+        out[f"rel_err_{k}"] = float(np.linalg.norm(got[k] - ref) / np.linalg.norm(ref))
+    out["pass"] = all(out[f"rel_err_{k}"] <= 1e-9 for k in ("x", "v", "F"))
+    return out
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
@@ -474,6 +600,11 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-rollout leg")
     ap.add_argument("--adj-scale", type=int, default=1, help="shrink the sphere scene of the adjoint leg")
     ap.add_argument("--no-taylor", action="store_true", help="skip the Taylor impact leg")
+    ap.add_argument("--configs", default="clusters3d,sphere3d,dambreak3d",
+                    help="comma list of the other configurations to measure (clusters3d, sphere3d, dambreak3d), "
+                         "or 'none'")
+    ap.add_argument("--config-scale", type=int, default=1, help="shrink the other configurations' scenes")
+    ap.add_argument("--no-oracle-check", action="store_true", help="skip the full-size FP64 oracle check")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed FP32 leg (for profiler captures); prints a reduced line")
     args = ap.parse_args()
@@ -627,7 +758,55 @@ def main():
            "note": "one bench step = one tb_rollout_host_f32x64 call on pinned host buffers (H2D, S steps, D2H)"}
     del hostp
 
-    adjoint = None if args.no_adjoint else adjoint_leg(tb, runtime, ctx, scale=args.adj_scale)
+    # One MPM step per call: every step pays the whole state's round trip.
+    hostp = host64.to("pinned", dtype=np.float32, x64=True)
+    runtime.rollout_host(hostp, mesh, prm, 1, ctx=ctx)
+    calls1 = 5
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(calls1):
+        runtime.rollout_host(hostp, mesh, prm, 1, ctx=ctx)
+    barrier()
+    e2e1_s = max_over_ranks_here(time.perf_counter() - t0)
+    e2e["one_step_per_call"] = {"value": job_throughput(world, n, calls1, 1e3 * e2e1_s), "unit": "particle-steps/s",
+                                "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes,
+                                "mpm_steps_per_call": 1, "calls": calls1}
+    del hostp
+
+    peak, peak_src = measured_peaks()
+    oracle_check = None
+    if world == 1 and not args.no_oracle_check and args.scale == 1:
+        oracle_check = fullsize_oracle_check(tb, runtime, ctx, sc)
+    configs = {}
+    # the other configurations and the oracle check run at N = 1 only
+    wanted = [c for c in args.configs.split(",") if c and c != "none"] if world == 1 else []
+    cs = args.config_scale
+    for cname in wanted:
+        if cname == "clusters3d":
+            csc = tb.scenes.clusters3d(scale=cs)
+            configs[cname] = config_leg(tb, runtime, ctx, csc, ("x64", "f64"), steps=10, warmup=3,
+                                        acc_steps=csc.nsteps, peak=peak, per_particle=("m",))
+            configs[cname]["workload"] = ("clusters3d: 512^3 cells, 64 Gaussian clusters (sigma 0.02), lognormal "
+                                          "masses, Neo-Hookean E=1e5 nu=0.35, dt=2.5e-5; block order")
+        elif cname == "sphere3d":
+            csc = tb.scenes.block_ordered(tb.scenes.sphere3d(scale=cs))
+            configs[cname] = config_leg(tb, runtime, ctx, csc, ("x64", "f64"), steps=20, warmup=3,
+                                        acc_steps=csc.nsteps, peak=peak, per_particle=("mu", "lam"))
+            configs[cname]["workload"] = ("sphere3d forward: 64^3 cells, sphere r=0.3, jittered 4^3 per cell, "
+                                          "per-particle E, dt=5e-4; block order")
+        elif cname == "dambreak3d":
+            csc = tb.scenes.dambreak3d(scale=cs, device="cuda", dtype=np.float32)
+            csc.particles = None  # each form builds its own state on the device
+            torch.cuda.empty_cache()
+            configs[cname] = config_leg(tb, runtime, ctx, csc, ("f32", "f64"), steps=5, warmup=3,
+                                        acc_steps=csc.nsteps, peak=peak, apic=True)
+            configs[cname]["workload"] = ("dambreak3d: 384^3 cells, column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell, "
+                                          "WLS(uGIMP) + APIC, fluid K=2e6, slip walls, dt=2.5e-5 (FP32 positions: "
+                                          "the FP64-position form takes B-spline/uGIMP FLIP only)")
+        else:
+            raise SystemExit(f"unknown config {cname}")
+
+    adjoint = None if (args.no_adjoint or world > 1) else adjoint_leg(tb, runtime, ctx, scale=args.adj_scale)
     taylor = None if (args.no_taylor or rank != 0) else taylor_leg(tb, runtime, ctx)
 
     if rank != 0:
@@ -643,7 +822,6 @@ def main():
     nact = active_nodes(mesh, host64.x)
     alg_bytes = n * per_p + nact * per_n
     achieved = alg_bytes / (ms_dom / launches_dom * 1e-3) / 1e9
-    peak, peak_src = measured_peaks()
     traffic = read_traffic(dom, n)
     sp, sn = step_bytes(4, 8)
     step_alg = n * sp + nact * sn
@@ -689,7 +867,8 @@ def main():
                                      "docs/src/parallel.md:47-57 sets up a GPU run (the reference arm and "
                                      "the CPU baseline time the same order; generation order under "
                                      "generation_order)"},
-        "accuracy": acc,
+        "accuracy": dict(acc, fullsize_oracle_check=oracle_check),
+        "configs": configs,
         "fp32_positions": {"value": job_throughput(world, n, args.steps, f32["ms"]), "ms_per_step": f32["ms"] / args.steps,
                            "form": FORMS["f32"][2], "accuracy": acc_f32},
         "fp64_plain": {"value": job_throughput(world, n, args.steps, f64["ms"]), "ms_per_step": f64["ms"] / args.steps},

@@ -24,7 +24,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from .state import CartesianMesh, GridSampling, Particles, generate_points, lame, step_params
+from .state import CartesianMesh, GridSampling, Particles, generate_points, lame, sampling_axes, step_params
 
 SEEDS = {"readme2d": 0, "cube3d": 20260001, "clusters3d": 20260002, "sphere3d": 20260003,
          "dambreak3d": 20260004, "taylor3d": 20260005}
@@ -102,6 +102,23 @@ def cube3d(scale: int = 1, seed: int | None = None) -> Scene:
     mu, lam = lame(E, nu)
     prm = step_params(5e-5, mass=rho0 * V0, V0=V0, mu=mu, lam=lam, gravity=(0.0, 0.0, -9.81))
     return Scene("cube3d", mesh, P, prm, 100, {"E": E, "nu": nu, "rho0": rho0, "cells": cells})
+
+
+def _lattice_on_device(mesh: CartesianMesh, box, device, dtype, optional=()) -> Particles:
+    """Particles on `device` (torch) at the GridSampling points of `mesh` inside
+    `box`, in the column-major order of `generate_points`, built from the axes
+    on the device without forming the points on the host."""
+    import torch
+    axes = sampling_axes(GridSampling(), mesh, box)
+    sizes = [len(a) for a in axes]
+    n = int(np.prod(sizes))
+    P = Particles(n, mesh.dim, dtype, backend="torch", device=device, optional=optional)
+    stride = 1
+    for d in range(mesh.dim):
+        a = torch.from_numpy(axes[d]).to(device=device, dtype=P.x.dtype)
+        P.x[d].copy_(a.repeat_interleave(stride).repeat(n // (stride * sizes[d])))
+        stride *= sizes[d]
+    return P
 
 
 def _sort_by_block(mesh: CartesianMesh, pts: np.ndarray) -> np.ndarray:
@@ -205,28 +222,36 @@ def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
     return Scene("sphere3d", mesh, P, prm, 200, {"nu": 0.3, "rho0": 1e3, "target": (0.5 * L, 0.5 * L, 0.8 * L)})
 
 
-def dambreak3d(scale: int = 1) -> Scene:
+def dambreak3d(scale: int = 1, device=None, dtype=np.float64) -> Scene:
     """384^3 cells (h = 1/384), column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell,
     weakly compressible fluid p = -K (J - 1) with K = 2e6, rho0 = 1e3, WLS(uGIMP)
     basis with l = h/2, APIC transfer, slip walls on every face, 100 steps at
     dt = 2.5e-5. dt: the configuration's 5e-5 puts the acoustic CFL number
     (sqrt(K / rho0) dt / h) at 0.86; the FP32 run diverges within 50 steps and
-    the FP64 run only survives unperturbed. Both are stable at 2.5e-5 (CFL 0.43)."""
+    the FP64 run only survives unperturbed. Both are stable at 2.5e-5 (CFL 0.43).
+    With `device`, the particles are built there directly in `dtype` (the full
+    scene has 145 M particles: 46 GB of FP64 host state otherwise); the state
+    is deterministic (a lattice at rest), so both builds are the same scene."""
     cells = 384 // scale
     h = 1.0 / 384
     L = cells * h
     mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
-    pts = generate_points(GridSampling(), mesh, box=[(0.0, 0.4 * L), None, (0.0, 0.8 * L)])
-    n = pts.shape[1]
-    P = Particles(n, 3, np.float64, optional=("B",))
-    P.x[...] = pts
+    box = [(0.0, 0.4 * L), None, (0.0, 0.8 * L)]
+    if device is None:
+        pts = generate_points(GridSampling(), mesh, box=box)
+        n = pts.shape[1]
+        P = Particles(n, 3, np.float64, optional=("B",))
+        P.x[...] = pts
+    else:
+        P = _lattice_on_device(mesh, box, device, dtype, optional=("B",))
     V0 = (h / 2) ** 3
     P.V[...] = V0
     K = 2e6
     prm = step_params(2.5e-5, mass=1e3 * V0, V0=V0, mu=0.0, lam=K, gravity=(0.0, 0.0, -9.81),
                       gimp_l=h / 2, basis=_abi.TB_WLS_UGIMP, transfer=_abi.TB_TRANSFER_APIC,
                       material=_abi.MATERIAL_FLUID, wall_mask=0b111111, wall_layers=2)
-    return Scene("dambreak3d", mesh, P, prm, 100, {"K": K, "rho0": 1e3})
+    return Scene("dambreak3d", mesh, P, prm, 100, {"K": K, "rho0": 1e3, "scale": scale,
+                                                   "built_on_device": device is not None})
 
 
 SCENES = {"readme2d": readme2d, "cube3d": cube3d, "clusters3d": clusters3d, "sphere3d": sphere3d,

@@ -371,14 +371,10 @@ class GridSampling:
     spacing: float = 0.5
 
 
-def generate_points(alg: GridSampling, mesh: CartesianMesh, box=None) -> np.ndarray:
-    """The sample points of `alg` over `mesh` (src/particles.jl:13-18), shape
-    (dim, n) in the reference's column-major order: per axis
-    `(xmin + l/2):l:xmax` with `l = spacing * h`. `box` (one (lo, hi) pair per
-    axis, or None) keeps the points with lo <= x <= hi on every axis: the same
-    points, in the same order, as filtering the whole lattice with that box,
-    without forming it (the lattice of a 256^3 mesh at 2 per cell per axis has
-    134 M points)."""
+def sampling_axes(alg: GridSampling, mesh: CartesianMesh, box=None) -> list[np.ndarray]:
+    """The per-axis coordinates of `alg`'s points over `mesh`: `(xmin + l/2):l:xmax`
+    with `l = spacing * h` (src/particles.jl:13-18), each kept inside
+    `box[d] = (lo, hi)` (lo <= x <= hi) when given."""
     if not isinstance(alg, GridSampling):
         raise TypeError("generate_points: only GridSampling is on the B200 path "
                         "(PoissonDiskSampling is the third-party PoissonDiskSampling.jl)")
@@ -394,7 +390,17 @@ def generate_points(alg: GridSampling, mesh: CartesianMesh, box=None) -> np.ndar
             lo, hi = box[d]
             ax = ax[(ax >= lo) & (ax <= hi)]
         axes.append(ax)
-    grids = np.meshgrid(*axes, indexing="ij")
+    return axes
+
+
+def generate_points(alg: GridSampling, mesh: CartesianMesh, box=None) -> np.ndarray:
+    """The sample points of `alg` over `mesh` (src/particles.jl:13-18), shape
+    (dim, n) in the reference's column-major order (first axis fastest). `box`
+    (one (lo, hi) pair per axis, or None) keeps the points with lo <= x <= hi on
+    every axis: the same points, in the same order, as filtering the whole
+    lattice with that box, without forming it (the lattice of a 256^3 mesh at 2
+    per cell per axis has 134 M points)."""
+    grids = np.meshgrid(*sampling_axes(alg, mesh, box), indexing="ij")
     return np.stack([g.reshape(-1, order="F") for g in grids])
 
 

@@ -47,3 +47,16 @@ def test_job_throughput(bench):
     assert bench.job_throughput(1, 1000, 10, 2.0) == pytest.approx(5e6)
     assert bench.job_throughput(4, 1000, 10, 2.0) == pytest.approx(2e7)
     assert bench.max_over_ranks(3.5) == 3.5  # one rank: its own time
+
+
+@pytest.mark.parametrize("s,sx", [(8, 8), (4, 4), (4, 8)])
+def test_config_bytes(bench, s, sx):
+    # the plain equation set is the headline's accounting
+    assert bench.config_bytes(s, sx) == bench.step_bytes(s, sx)
+    # per-particle mass (P2G) and Lame parameters (G2P) are one scalar read each
+    assert bench.config_bytes(s, sx, ("m",))[0] == bench.step_bytes(s, sx)[0] + s
+    assert bench.config_bytes(s, sx, ("mu", "lam"))[0] == bench.step_bytes(s, sx)[0] + 2 * s
+    # APIC: B read in P2G and written in G2P, the old velocity and vn not read
+    pp, pn = bench.config_bytes(s, sx, apic=True)
+    assert pp == bench.step_bytes(s, sx)[0] + 18 * s - 3 * s
+    assert pn == bench.step_bytes(s, sx)[1] - 3 * s
