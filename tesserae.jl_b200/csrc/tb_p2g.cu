@@ -1102,6 +1102,328 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     }
 }
 
+// ---------------------------------------------------------------------------
+// Plane kernel: the interior blocks of the 3D FP32 forms (quadratic B-spline,
+// KernelCorrection(BSpline) whose interior windows are the plain kernel), with
+// compact records in the packed FP32x2 layout (PairRec). The schedule of the
+// pencil kernel with a wider lane: a lane owns one z-slot k of a pencil's
+// window, i.e. the 3 x 3 (x, y) nodes of 3 window rows, and walks the pencil's
+// groups in x order keeping the 3 x-slots x 3 rows x 7 components (63 FP32
+// accumulators) in registers. Per record a lane loads the record once and
+// evaluates the x and y jets once for 9 nodes instead of 3, so the per-record
+// overhead (loads, jets, row factors) is paid 3 times per particle instead of
+// 9; the 25 pencils x 3 z-slots are 75 lanes of the 128-thread CTA. After each
+// group the x-node the window leaves for good is staged (3 rows, 7 components)
+// to the lane's own slots of the staging array; one thread per tile node then
+// sums the at most 9 staged partials in FP32 and adds the node to the grid
+// with one global atomic per non-zero value. Every other block of the block
+// list is appended to `bnd` for the full-record launch (MODE 2).
+constexpr int PLANE_THREADS = 128;
+constexpr int PLANE_NR = 512;
+
+// One record's contribution to a plane lane's 3 x 3 nodes.
+__device__ __forceinline__ void accumulate_plane(const PairRec& o, const SlotPoly& pz, float h_inv,
+                                                 PairAcc (&acc)[3][3]) {
+    const float tx = o.txy.x, ty = o.txy.y, tz = o.s5z.y;
+    const float2 t2 = make_float2(tx, tx);
+    // (wx_i, wx_i) and (dx_i, dx_i): the B-spline factors of the three x slots
+    const float2 wx0 = __ffma2_rn(t2, __ffma2_rn(t2, make_float2(0.5f, 0.5f), make_float2(-1.f, -1.f)),
+                                  make_float2(0.5f, 0.5f));
+    const float2 wx1 = __ffma2_rn(t2, __ffma2_rn(t2, make_float2(-1.f, -1.f), make_float2(1.f, 1.f)),
+                                  make_float2(0.5f, 0.5f));
+    const float2 wx2 = __fmul2_rn(t2, __fmul2_rn(t2, make_float2(0.5f, 0.5f)));
+    const float2 hh = make_float2(h_inv, h_inv);
+    const float2 dx0 = __fmul2_rn(__fadd2_rn(t2, make_float2(-1.f, -1.f)), hh);
+    const float2 dx1 = __fmul2_rn(__ffma2_rn(t2, make_float2(-2.f, -2.f), make_float2(1.f, 1.f)), hh);
+    const float2 dx2 = __fmul2_rn(t2, hh);
+    const float2 wxs[3] = {wx0, wx1, wx2}, dxs[3] = {dx0, dx1, dx2};
+    // y jets of the three window rows, z jet of this lane's slot
+    const float wy[3] = {0.5f + ty * (-1.0f + ty * 0.5f), 0.5f + ty * (1.0f + ty * -1.0f), ty * (ty * 0.5f)};
+    const float dy[3] = {(-1.0f + ty) * h_inv, (1.0f + ty * -2.0f) * h_inv, ty * h_inv};
+    const float wz = pz.a + tz * (pz.b + tz * pz.c);
+    const float dz = (pz.e + tz * pz.f) * h_inv;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float wyz = wy[j] * wz, dyz = dy[j] * wz, wdz = wy[j] * dz;
+        const float2 WYZ = make_float2(wyz, wyz);
+        const float2 fa01 = __fmul2_rn(o.sa, WYZ);
+        const float2 fb01 = __ffma2_rn(o.sc, make_float2(wdz, wdz), __fmul2_rn(o.sb, make_float2(dyz, dyz)));
+        const float fa2 = o.sc.x * wyz;
+        const float fb2 = __fmaf_rn(o.s5z.x, wdz, o.sc.y * dyz);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float2 w = __fmul2_rn(wxs[i], WYZ);
+            acc[i][j].a01 = __ffma2_rn(w, o.m0, acc[i][j].a01);
+            acc[i][j].a23 = __ffma2_rn(w, o.m1, acc[i][j].a23);
+            acc[i][j].f01 = __ffma2_rn(dxs[i], fa01, __ffma2_rn(wxs[i], fb01, acc[i][j].f01));
+            acc[i][j].f2 = __fmaf_rn(dxs[i].x, fa2, __fmaf_rn(wxs[i].x, fb2, acc[i][j].f2));
+        }
+    }
+}
+
+template <bool X64>
+__global__ void __launch_bounds__(PLANE_THREADS, 3)
+    p2g_plane_kernel(DMesh<3, float> M, PView<float> P, GView<float> G, Scalars<float> s,
+                     const int* __restrict__ totals, const int* __restrict__ blocklist,
+                     const int* __restrict__ offsets, const int* __restrict__ perm, int* err,
+                     int* __restrict__ bnd, unsigned long long* __restrict__ bnd_count) {
+    using SH = PencilShape<3, 4>;
+    constexpr int NT = PLANE_THREADS, NR = PLANE_NR, ITEMS = NR / NT;
+    constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
+    constexpr int NJK = SH::NJK, NPENCIL = SH::NPENCIL;
+    constexpr int CSTR = NPENCIL * NJK * TS;  // stride between components in the staging array
+    constexpr int SKW = 2;                    // record skew per pencil (words)
+    static_assert(NR % NT == 0, "whole items per thread");
+    static_assert(3 * NPENCIL <= NT, "one plane lane per (pencil, z slot)");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* rec = reinterpret_cast<float*>(smem_raw);
+    float* part = rec + NR * CRS + SKW * NPENCIL;
+    int* gcount = reinterpret_cast<int*>(part + NC * CSTR);
+    int* gstart = gcount + NG;
+    int* pslot = gstart + NG + 1;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nactive = totals[0];
+
+    for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+    __syncthreads();
+
+    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        const int b = blocklist[bi] - 1;
+        int org[3];
+        bool interior = true;
+        {
+            int r = b;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                org[d] = (r % M.nb[d]) * 4 - 1;
+                r /= M.nb[d];
+                interior = interior && org[d] >= 0 && org[d] + TS - 1 <= M.n[d] - 1;
+            }
+        }
+        if (!interior) {  // the full-record launch's block (uniform over the CTA)
+            if (tid == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
+            continue;
+        }
+        const int s0 = offsets[b], s1 = offsets[b + 1];
+        for (int b0 = s0; b0 < s1; b0 += NR) {
+            const int nbat = min(NR, s1 - b0);
+            // ---- 1a. every global load of the batch first, then group and rank;
+            //      the record's 14 values stay in registers until the slot is known
+            int pid[ITEMS], grp[ITEMS], rank[ITEMS];
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                const int ti = tid + u * NT;
+                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+            }
+            float pv[ITEMS][3], pV[ITEMS], pm[ITEMS], psg[ITEMS][6], pt[ITEMS][3];
+            double pxd[ITEMS][3];
+            float pxf[ITEMS][3];
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                const long long p = pid[u] >= 0 ? pid[u] : 0;
+                const bool on = pid[u] >= 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if constexpr (X64) pxd[u][d] = on ? P.x64[d][p] : 0.0;
+                    else pxf[u][d] = on ? P.x[d][p] : 0.0f;
+                    pv[u][d] = on ? P.v[d][p] : 0.0f;
+                }
+                pV[u] = on ? P.V[p] : 0.0f;
+                pm[u] = (on && P.m) ? P.m[p] : s.mass;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) psg[u][k] = on ? P.sig[k][p] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                grp[u] = -1;
+                rank[u] = 0;
+                if (pid[u] < 0) continue;
+                int gi = 0;
+                bool ok = true;
+#pragma unroll
+                for (int d = 2; d >= 0; --d) {
+                    // window start floor(xi - 1/2) and the fast path's t = fract(xi - 1/2)
+                    // (bspline.jl:28-40, 90-100)
+                    int lo;
+                    if constexpr (X64) {
+                        const double u64 = (pxd[u][d] - M.xmin64[d]) * M.h_inv64 - 0.5;
+                        const double fl = floor(u64);
+                        lo = int(fl);
+                        float t = float(u64 - fl);
+                        if (t >= 1.0f) t = 1.0f - 1.0f / float(1 << 24);
+                        pt[u][d] = t;
+                    } else {
+                        const float uu = (pxf[u][d] - M.xmin[d]) * M.h_inv - 0.5f;
+                        const float fl = floorf(uu);
+                        lo = int(fl);
+                        pt[u][d] = uu - fl;
+                    }
+                    const int q = lo - org[d];
+                    ok = ok && q >= 0 && q < G1;
+                    gi = gi * G1 + q;
+                }
+                if (!ok) {
+                    atomicOr(err, ERR_TILE_RANGE);
+                    continue;
+                }
+                grp[u] = gi;
+                rank[u] = atomicAdd(&gcount[gi], 1);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                int carry = 0;
+                for (int g0 = 0; g0 < NG; g0 += 32) {
+                    const int g = g0 + lane;
+                    const int c = g < NG ? gcount[g] : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    if (g < NG) gstart[g] = carry + incl - c;
+                    carry += __shfl_sync(0xffffffffu, incl, 31);
+                }
+                if (lane == 0) gstart[NG] = carry;
+            } else if (warp == 1) {
+                // pencil slots by size, largest first: the pencils of one warp
+                // then have similar lengths
+                const int myp = lane < NPENCIL ? lane : -1;
+                int mysize = 0;
+                if (myp >= 0) {
+                    const int gb = G1 * myp;
+#pragma unroll
+                    for (int gx = 0; gx < G1; ++gx) mysize += gcount[gb + gx];
+                }
+                int rk = 0;
+                for (int o = 0; o < NPENCIL; ++o) {
+                    const int os = __shfl_sync(0xffffffffu, mysize, o);
+                    rk += (os > mysize) || (os == mysize && o < lane);
+                }
+                if (myp >= 0) pslot[rk] = myp;
+            }
+            __syncthreads();
+            // ---- 1b. records at their group-sorted slots (PairRec layout)
+            for (int g = tid; g < NG; g += NT) gcount[g] = 0;  // ready for the next batch
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                if (grp[u] < 0) continue;
+                float* r = rec + (gstart[grp[u]] + rank[u]) * CRS + SKW * (grp[u] / G1);
+                const float mp = pm[u], nV = -pV[u];
+                st2(r + 0, mp, mp * pv[u][0]);
+                st2(r + 2, mp * pv[u][1], mp * pv[u][2]);
+                st2(r + 4, nV * psg[u][0], nV * psg[u][1]);
+                st2(r + 6, nV * psg[u][1], nV * psg[u][3]);
+                st2(r + 8, nV * psg[u][2], nV * psg[u][4]);
+                st2(r + 10, nV * psg[u][5], pt[u][2]);
+                st2(r + 12, pt[u][0], pt[u][1]);
+            }
+            __syncthreads();
+            // ---- 2. plane sweeps: lane (pencil slot, z slot k)
+            if (tid < 3 * NPENCIL) {
+                const int slot = tid / 3, k = tid - 3 * slot;
+                const int pc = pslot[slot];
+                const int gbase = G1 * pc;
+                const float* prec = rec + SKW * pc;
+                const SlotPoly pz = slot_poly(k);
+                PairAcc acc[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        acc[i][j].a01 = acc[i][j].a23 = acc[i][j].f01 = make_float2(0.f, 0.f);
+                        acc[i][j].f2 = 0.f;
+                    }
+                int qs = gstart[gbase];
+#pragma unroll
+                for (int gx = 0; gx < G1 + 2; ++gx) {
+                    if (gx < G1) {
+                        const int qe = gstart[gbase + gx + 1];
+#pragma unroll 2
+                        for (int q = qs; q < qe; ++q) {
+                            PairRec r0;
+                            load_pair_rec(prec + q * CRS, r0);
+                            accumulate_plane(r0, pz, M.h_inv, acc);
+                        }
+                        qs = qe;
+                    }
+                    // x-node gx of rows (j, k) is final: stage it, shift the rows
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        float* dst = part + ((j + 3 * k) * NPENCIL + pc) * TS + gx;
+                        dst[0 * CSTR] = acc[0][j].a01.x;
+                        dst[1 * CSTR] = acc[0][j].a01.y;
+                        dst[2 * CSTR] = acc[0][j].a23.x;
+                        dst[3 * CSTR] = acc[0][j].a23.y;
+                        dst[4 * CSTR] = acc[0][j].f01.x;
+                        dst[5 * CSTR] = acc[0][j].f01.y;
+                        dst[6 * CSTR] = acc[0][j].f2;
+                        acc[0][j] = acc[1][j];
+                        acc[1][j] = acc[2][j];
+                        acc[2][j].a01 = acc[2][j].a23 = acc[2][j].f01 = make_float2(0.f, 0.f);
+                        acc[2][j].f2 = 0.f;
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- 3. per tile node: FP32 sum of the staged partials, one global
+            //      atomic per non-zero value (gravity from the summed mass)
+            for (int t = tid; t < TN; t += NT) {
+                const int tx = t % TS, ty = (t / TS) % TS, tz = t / (TS * TS);
+                float val[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) val[c] = 0.0f;
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const int gy = ty - jj, gz = tz - kk;
+                        if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
+                        const int idx = ((jj + 3 * kk) * NPENCIL + gy + G1 * gz) * TS + tx;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
+                    }
+                const long long lin =
+                    (long long)(org[0] + tx) + (long long)M.n[0] * ((org[1] + ty) + (long long)M.n[1] * (org[2] + tz));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
+                if (val[0] != 0.0f) atomicAdd(G.m + lin, val[0]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (val[1 + d] != 0.0f) atomicAdd(G.mv[d] + lin, val[1 + d]);
+                    if (val[4 + d] != 0.0f) atomicAdd(G.f[d] + lin, val[4 + d]);
+                }
+            }
+        }
+    }
+}
+
+size_t plane_smem_bytes() {
+    using SH = PencilShape<3, 4>;
+    return sizeof(float) * (size_t(PLANE_NR) * CRS + 2 * SH::NPENCIL + SH::NPART) +
+           sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
+}
+
+template <bool X64>
+cudaError_t launch_plane(const DMesh<3, float>& M, const PView<float>& P, const GView<float>& G,
+                         const Scalars<float>& s, const BinBuffers& b, const LaunchCfg& cfg) {
+    auto kern = p2g_plane_kernel<X64>;
+    const size_t smem = plane_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PLANE_THREADS, smem);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    kern<<<grid, PLANE_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,
+                                                   b.cursors, b.partials);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
 template <int D, class T, int BW, int NR, int MODE>
 size_t pencil_smem_bytes() {
     using SH = PencilShape<D, BW>;
@@ -1144,7 +1466,8 @@ cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T
         if (s.basis == TB_BSPLINE_QUADRATIC || s.basis == TB_KC_BSPLINE_QUADRATIC) {
             cudaError_t e = cudaMemsetAsync(b.partials, 0, sizeof(unsigned long long), cfg.stream);
             if (e != cudaSuccess) return e;
-            e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
+            if constexpr (D == 3 && BW == 4) e = launch_plane<X64>(M, P, G, s, b, cfg);
+            else e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
             if (e != cudaSuccess) return e;
             return launch_pencil_mode<D, T, BW, X64, 2>(M, P, G, s, b, cfg);
         }
