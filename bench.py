@@ -444,12 +444,20 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
     }
 
 
-def _form_particles(tb, sc, name, device="cuda"):
-    """Device particles of scene `sc` in precision form `name` (x64 / f32 / f64)."""
+def _form_particles(tb, runtime, ctx, sc, name, device="cuda"):
+    """Device particles of scene `sc` in precision form `name` (x64 / f32 / f64),
+    stored in block order: binned once and put through reorder_particles!
+    (threshold 1: always), the set-up docs/src/parallel.md:47-57 gives a GPU run."""
     dtype, x64, _ = FORMS[name]
     if sc.meta.get("built_on_device"):
-        return tb.scenes.dambreak3d(scale=sc.meta["scale"], device=device, dtype=dtype).particles
-    return sc.particles.to("torch", device=device, dtype=dtype, x64=x64)
+        P = tb.scenes.dambreak3d(scale=sc.meta["scale"], device=device, dtype=dtype).particles
+    else:
+        P = sc.particles.to("torch", device=device, dtype=dtype, x64=x64)
+    part = tb.Partition(sc.mesh, P.n, backend="torch", device=device)
+    runtime.update(part, P, sc.mesh, ctx=ctx)
+    runtime.reorder_particles(P, part, 1.0, ctx=ctx)
+    del part
+    return P
 
 
 def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: int, peak: float,
@@ -463,7 +471,7 @@ def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: 
     out = {"n_particles": None, "steps": steps, "warmup": warmup, "forms": {}}
     finals = {}
     for name in forms:
-        P = _form_particles(tb, sc, name)
+        P = _form_particles(tb, runtime, ctx, sc, name)
         n = P.n
         out["n_particles"] = n
         dtype = FORMS[name][0]
@@ -499,7 +507,7 @@ def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: 
         del part, G, P
         torch.cuda.empty_cache()
         # accuracy run from the initial state
-        P = _form_particles(tb, sc, name)
+        P = _form_particles(tb, runtime, ctx, sc, name)
         part = tb.Partition(mesh, n, backend="torch", device="cuda")
         G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
         x0 = P.x.double().clone()
@@ -802,7 +810,7 @@ def main():
                                         acc_steps=csc.nsteps, peak=peak, apic=True)
             configs[cname]["workload"] = ("dambreak3d: 384^3 cells, column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell, "
                                           "WLS(uGIMP) + APIC, fluid K=2e6, slip walls, dt=2.5e-5 (FP32 positions: "
-                                          "the FP64-position form takes B-spline/uGIMP FLIP only)")
+                                          "the FP64-position form takes B-spline/uGIMP FLIP only); block order")
         else:
             raise SystemExit(f"unknown config {cname}")
 
