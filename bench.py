@@ -450,7 +450,7 @@ def _form_particles(tb, runtime, ctx, sc, name, device="cuda"):
     (threshold 1: always), the set-up docs/src/parallel.md:47-57 gives a GPU run."""
     dtype, x64, _ = FORMS[name]
     if sc.meta.get("built_on_device"):
-        P = tb.scenes.dambreak3d(scale=sc.meta["scale"], device=device, dtype=dtype).particles
+        P = tb.scenes.dambreak3d(scale=sc.meta["scale"], device=device, dtype=dtype, x64=x64).particles
     else:
         P = sc.particles.to("torch", device=device, dtype=dtype, x64=x64)
     part = tb.Partition(sc.mesh, P.n, backend="torch", device=device)
@@ -803,14 +803,11 @@ def main():
             configs[cname]["workload"] = ("sphere3d forward: 64^3 cells, sphere r=0.3, jittered 4^3 per cell, "
                                           "per-particle E, dt=5e-4; block order")
         elif cname == "dambreak3d":
-            csc = tb.scenes.dambreak3d(scale=cs, device="cuda", dtype=np.float32)
-            csc.particles = None  # each form builds its own state on the device
-            torch.cuda.empty_cache()
-            configs[cname] = config_leg(tb, runtime, ctx, csc, ("f32", "f64"), steps=5, warmup=3,
+            csc = tb.scenes.dambreak3d(scale=cs, particles=False)  # each form builds its own state on the device
+            configs[cname] = config_leg(tb, runtime, ctx, csc, ("x64", "f32", "f64"), steps=5, warmup=3,
                                         acc_steps=csc.nsteps, peak=peak, apic=True)
             configs[cname]["workload"] = ("dambreak3d: 384^3 cells, column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell, "
-                                          "WLS(uGIMP) + APIC, fluid K=2e6, slip walls, dt=2.5e-5 (FP32 positions: "
-                                          "the FP64-position form takes B-spline/uGIMP FLIP only); block order")
+                                          "WLS(uGIMP) + APIC, fluid K=2e6, slip walls, dt=2.5e-5; block order")
         else:
             raise SystemExit(f"unknown config {cname}")
 

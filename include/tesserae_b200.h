@@ -239,8 +239,9 @@ int32_t tb_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, t
  * and G2P adds the FP32 displacement to the FP64 position. A Float32 position
  * near 0.5 carries an ulp of 6e-8, larger than a step's displacement rounding
  * allows for 1e-5 accuracy over 100 steps; this form removes that error.
- * B-spline / uGIMP bases with the FLIP/PIC transfer only (TB_ERR_UNSUPPORTED
- * otherwise). The reference's counterpart is the same step under
+ * In 3D every basis and transfer of the step; in 2D the B-spline / uGIMP
+ * FLIP/PIC step only (TB_ERR_UNSUPPORTED otherwise). The reference's
+ * counterpart is the same step under
  * gpu_preserve (src/adapt.jl:15-17), which leaves chosen arrays in Float64. */
 int32_t tb_step_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                        tb_grid* grid, const tb_step_params* params, int32_t nsteps);

@@ -497,9 +497,9 @@ int dispatch_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* pa
     if ((rc = check_mesh(c, m)) != TB_OK) return rc;
     if ((rc = check_params(c, prm)) != TB_OK) return rc;
     if (nsteps < 0) return fail(c, TB_ERR_ARG, "nsteps must be >= 0");
-    if (x64 && (prm->transfer != TB_TRANSFER_FLIP || prm->basis == TB_WLS_BSPLINE_QUADRATIC ||
-                prm->basis == TB_WLS_UGIMP))
-        return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs the B-spline / uGIMP FLIP step only");
+    if (x64 && m->dim != 3 && (prm->transfer != TB_TRANSFER_FLIP || prm->basis == TB_WLS_BSPLINE_QUADRATIC ||
+                               prm->basis == TB_WLS_UGIMP))
+        return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs WLS and APIC in 3D only");
     if (!(reorder_threshold >= 0.0 && reorder_threshold <= 1.0))
         return fail(c, TB_ERR_ARG, "reorder threshold must be in [0, 1]");
     if (m->dim == 3) return run_step<3, T, 4>(c, m, p, part, g, prm, nsteps, b, p2g, gr, g2p, x64, reorder_threshold);

@@ -375,14 +375,21 @@ __device__ __forceinline__ void node_weight(const DMesh<D, T>& M, const Axis<T>*
 
 // WLS moment-matrix inverse (wls.jl:51-68); the closed form diag(1, 4/h^2) for a
 // full quadratic B-spline support (wls.jl:29-49). Returns false if singular.
+// `r[d][k]` = X_{lo+k} - x_p on axis d. The kernel weight is a product of axis
+// factors and P = (1, X - x_p) has one axis per component, so
+// M = sum_i w_i P_i P_i^T is built from the axis moments S0 = sum w, S1 = sum w r,
+// S2 = sum w r^2: M00 = prod S0, M0a = S1_a prod_{d!=a} S0_d,
+// Maa = S2_a prod_{d!=a} S0_d, Mab = S1_a S1_b prod_{d!=a,b} S0_d -- the
+// reference's sum over the window's nodes, regrouped (equal to rounding).
+// Slots beyond a truncated window have w = 0 and drop out.
 template <int D, class T>
-__device__ __forceinline__ bool wls_minv(const DMesh<D, T>& M, const Axis<T>* ax, const T* x, bool closed,
+__device__ __forceinline__ bool wls_minv(const DMesh<D, T>& M, const Axis<T>* ax, const T (&r)[3][3], bool closed,
                                          T (&Mi)[D + 1][D + 1]) {
     constexpr int N = D + 1;
 #pragma unroll
-    for (int r = 0; r < N; ++r)
+    for (int a = 0; a < N; ++a)
 #pragma unroll
-        for (int c = 0; c < N; ++c) Mi[r][c] = T(0);
+        for (int c = 0; c < N; ++c) Mi[a][c] = T(0);
     if (closed) {
         Mi[0][0] = T(1);
         T cval = T(4) / (M.h * M.h);
@@ -390,36 +397,40 @@ __device__ __forceinline__ bool wls_minv(const DMesh<D, T>& M, const Axis<T>* ax
         for (int d = 1; d < N; ++d) Mi[d][d] = cval;
         return true;
     }
+    T S0[3], S1[3], S2[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        S0[d] = S1[d] = S2[d] = T(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const T w = ax[d].val[k];
+            S0[d] += w;
+            S1[d] += w * r[d][k];
+            S2[d] += (w * r[d][k]) * r[d][k];
+        }
+    }
     T A[N][2 * N];
 #pragma unroll
-    for (int r = 0; r < N; ++r)
+    for (int a = 0; a < N; ++a)
 #pragma unroll
-        for (int c = 0; c < 2 * N; ++c) A[r][c] = (c - N == r) ? T(1) : T(0);
+        for (int c = 0; c < N; ++c) {
+            // factor of axis d in entry (a, c): S2 if both index d, S1 if one does, else S0
+            T v = T(1);
 #pragma unroll
-    for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                T w, dw[3];
-                node_weight<D, T>(M, ax, i, j, D == 3 ? k : 0, w, dw);
-                T P[N];
-                P[0] = T(1);
-                P[1] = node_coord(M, 0, ax[0].lo + i) - x[0];
-                P[2] = node_coord(M, 1, ax[1].lo + j) - x[1];
-                if constexpr (D == 3) P[3] = node_coord(M, 2, ax[2].lo + k) - x[2];
-#pragma unroll
-                for (int r = 0; r < N; ++r)
-#pragma unroll
-                    for (int c = 0; c < N; ++c) A[r][c] += w * P[r] * P[c];
+            for (int d = 0; d < D; ++d) {
+                const int hits = (a == d + 1) + (c == d + 1);
+                v *= hits == 2 ? S2[d] : (hits == 1 ? S1[d] : S0[d]);
             }
+            A[a][c] = v;
+            A[a][c + N] = (a == c) ? T(1) : T(0);
+        }
     // Gauss-Jordan with partial pivoting on [M | I].
 #pragma unroll
     for (int c = 0; c < N; ++c) {
         int p = c;
 #pragma unroll
-        for (int r = c + 1; r < N; ++r)
-            if (fabs(A[r][c]) > fabs(A[p][c])) p = r;
+        for (int q = c + 1; q < N; ++q)
+            if (fabs(A[q][c]) > fabs(A[p][c])) p = q;
         if (A[p][c] == T(0)) return false;
         if (p != c) {
 #pragma unroll
@@ -433,17 +444,17 @@ __device__ __forceinline__ bool wls_minv(const DMesh<D, T>& M, const Axis<T>* ax
 #pragma unroll
         for (int k = 0; k < 2 * N; ++k) A[c][k] *= inv;
 #pragma unroll
-        for (int r = 0; r < N; ++r)
-            if (r != c) {
-                T f = A[r][c];
+        for (int q = 0; q < N; ++q)
+            if (q != c) {
+                T f = A[q][c];
 #pragma unroll
-                for (int k = 0; k < 2 * N; ++k) A[r][k] -= f * A[c][k];
+                for (int k = 0; k < 2 * N; ++k) A[q][k] -= f * A[c][k];
             }
     }
 #pragma unroll
-    for (int r = 0; r < N; ++r)
+    for (int a = 0; a < N; ++a)
 #pragma unroll
-        for (int c = 0; c < N; ++c) Mi[r][c] = A[r][c + N];
+        for (int c = 0; c < N; ++c) Mi[a][c] = A[a][c + N];
     return true;
 }
 
@@ -483,7 +494,14 @@ __device__ __forceinline__ bool prepare_basis(const DMesh<D, T>& M, int basis, c
     B.wls = ALLOW_WLS && (basis == TB_WLS_BSPLINE_QUADRATIC || basis == TB_WLS_UGIMP);
     if constexpr (ALLOW_WLS) if (B.wls) {
         bool closed = (basis == TB_WLS_BSPLINE_QUADRATIC) && full;
-        if (!wls_minv<D, T>(M, B.ax, x, closed, B.Mi)) {
+        T r[3][3] = {};
+        if (!closed) {
+#pragma unroll
+            for (int d = 0; d < D; ++d)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) r[d][k] = node_coord(M, d, B.ax[d].lo + k) - x[d];
+        }
+        if (!wls_minv<D, T>(M, B.ax, r, closed, B.Mi)) {
             atomicOr(err, ERR_WLS_SINGULAR);
             return false;
         }
@@ -526,7 +544,7 @@ __device__ __forceinline__ bool axis_window_x64(const DMesh<D, T>& M, int basis,
     return true;
 }
 
-template <int D, class T>
+template <int D, class T, bool ALLOW_WLS = false>
 __device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basis, const double* x, T l_abs,
                                                   Basis<D, T>& B, int* err) {
     double lnorm = 0.0;
@@ -549,6 +567,13 @@ __device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basi
         B.ax[d].cnt = cnt[d];
         full = full && cnt[d] == 3;
     }
+    // X_{lo+k} - x_p in FP64, rounded once to T (KernelCorrection and WLS)
+    auto rel = [&](T (&r)[3][3]) {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r[d][k] = T(__dadd_rn(M.xmin64[d], __dmul_rn(double(lo[d] + k), M.h64)) - x[d]);
+    };
     if (!gimp && full) {
         // the fast path's t = fract(xi - 1/2) is xi - 1/2 - lo, in [0, 1); kept
         // below 1 after rounding so that the jets stay on the FP64 window
@@ -558,31 +583,40 @@ __device__ __forceinline__ bool prepare_basis_x64(const DMesh<D, T>& M, int basi
             if (t >= T(1)) t = T(1) - T(1) / T(1 << 24);
             bspline_quadratic_poly(t, B.ax[d].val, B.ax[d].der);
         }
-        return true;
-    }
-    const T ln = T(lnorm);
+    } else {
+        const T ln = T(lnorm);
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
+        for (int d = 0; d < D; ++d) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            B.ax[d].val[k] = T(0);
-            B.ax[d].der[k] = T(0);
-            if (k < cnt[d]) {
-                const T xn = T(xi[d] - double(lo[d] + k));
-                if (gimp) jet_ugimp(xn, ln, B.ax[d].val[k], B.ax[d].der[k]);
-                else jet_bspline_quadratic(xn, B.ax[d].val[k], B.ax[d].der[k]);
+            for (int k = 0; k < 3; ++k) {
+                B.ax[d].val[k] = T(0);
+                B.ax[d].der[k] = T(0);
+                if (k < cnt[d]) {
+                    const T xn = T(xi[d] - double(lo[d] + k));
+                    if (gimp) jet_ugimp(xn, ln, B.ax[d].val[k], B.ax[d].der[k]);
+                    else jet_bspline_quadratic(xn, B.ax[d].val[k], B.ax[d].der[k]);
+                }
+            }
+        }
+        if (basis_is_kc(basis) && !full) {
+            T r[3][3] = {};
+            rel(r);
+            if (!kc_correct<D, T>(M, basis == TB_KC_BSPLINE_QUADRATIC, r, B.ax)) {
+                atomicOr(err, ERR_WLS_SINGULAR);
+                return false;
             }
         }
     }
-    if (basis_is_kc(basis) && !full) {
-        T r[3][3] = {};
-#pragma unroll
-        for (int d = 0; d < D; ++d)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r[d][k] = T(__dadd_rn(M.xmin64[d], __dmul_rn(double(lo[d] + k), M.h64)) - x[d]);
-        if (!kc_correct<D, T>(M, basis == TB_KC_BSPLINE_QUADRATIC, r, B.ax)) {
-            atomicOr(err, ERR_WLS_SINGULAR);
-            return false;
+    if constexpr (ALLOW_WLS) {
+        B.wls = basis == TB_WLS_BSPLINE_QUADRATIC || basis == TB_WLS_UGIMP;
+        if (B.wls) {
+            const bool closed = basis == TB_WLS_BSPLINE_QUADRATIC && full;
+            T r[3][3] = {};
+            if (!closed) rel(r);
+            if (!wls_minv<D, T>(M, B.ax, r, closed, B.Mi)) {
+                atomicOr(err, ERR_WLS_SINGULAR);
+                return false;
+            }
         }
     }
     return true;

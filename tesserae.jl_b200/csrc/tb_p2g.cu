@@ -1424,6 +1424,388 @@ cudaError_t launch_plane(const DMesh<3, float>& M, const PView<float>& P, const 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// General plane kernel (3D): WLS weights (wls.jl:51-84) and/or the APIC affine
+// term mv_i += w_i m_p (v_p + B_p D^-1 (x_i - x_p)) (docs/src/transfer.md:
+// 176-178, D^-1 = 4/h^2 I), on the plane-lane schedule of p2g_plane_kernel.
+// Every quantity is a product of axis factors with an affine function of the
+// node offset r = X_i - x_p, so a lane evaluates it per window row from a few
+// per-row constants:
+//   WLS:  N_i = w_i (Mi[0] . P_i), grad N_i = w_i (Mi[1..3] . P_i), P = (1, r),
+//         w_i = wx wy wz the kernel (uGIMP or B-spline) values;
+//         per row j: A = Mi00 + Mi02 ry + Mi03 rz, C_d = Mi_d0 + Mi_d2 ry + Mi_d3 rz,
+//         per node:  N = w (A + Mi01 rx), G_d = w (C_d + Mi_d1 rx);
+//   plain kernel: N = w, G = the kernel jets' gradient;
+//   APIC: per row U = (m D^-1 B)[:,1] ry + (m D^-1 B)[:,2] rz, per node
+//         mv += N (m v_p + U + (m D^-1 B)[:,0] rx).
+// Records hold m_p, m_p v_p, -V_p sigma_p, the axis kernel values (and their
+// derivatives without WLS), r0 = X_lo - x_p per axis, the symmetric moment
+// inverse (WLS) and m_p D^-1 B_p (APIC). Any block (windows truncated at the
+// mesh boundary have zero values on their missing slots); staging and the
+// per-node gather as in p2g_plane_kernel, in T.
+template <bool WLSF, bool APICF>
+struct GenRec {
+    static constexpr int M = 0, MV = 1, S = 4, W = 10;  // W: kernel values x[3] y[3] z[3]
+    static constexpr int DW = 19;                       // without WLS: derivative jets x[3] y[3] z[3] (times h_inv)
+    static constexpr int R0 = WLSF ? 19 : 28;           // X_lo - x_p per axis
+    static constexpr int MI = R0 + 3;                   // WLS: Mi 00 01 02 03 11 12 13 22 23 33
+    static constexpr int DB = MI + (WLSF ? 10 : 0);     // APIC: m D^-1 B, column-major
+    static constexpr int END = DB + (APICF ? 9 : 0);
+    static constexpr int SIZE = (END + 1) & ~1;
+};
+
+constexpr int GEN_THREADS = 128;
+
+template <class T, bool X64, bool WLSF, bool APICF, int NR>
+__global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
+    p2g_gen_plane_kernel(DMesh<3, T> M, PView<T> P, GView<T> G, Scalars<T> s, const int* __restrict__ totals,
+                         const int* __restrict__ blocklist, const int* __restrict__ offsets,
+                         const int* __restrict__ perm, int* err) {
+    using SH = PencilShape<3, 4>;
+    using R = GenRec<WLSF, APICF>;
+    constexpr int NT = GEN_THREADS, ITEMS = NR / NT, RS = R::SIZE;
+    constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
+    constexpr int NJK = SH::NJK, NPENCIL = SH::NPENCIL;
+    constexpr int CSTR = NPENCIL * NJK * TS;
+    constexpr int SKW = 2;
+    static_assert(NR % NT == 0, "whole items per thread");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* rec = reinterpret_cast<T*>(smem_raw);
+    T* part = rec + NR * RS + SKW * NPENCIL;
+    int* gcount = reinterpret_cast<int*>(part + NC * CSTR);
+    int* gstart = gcount + NG;
+    int* pslot = gstart + NG + 1;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nactive = totals[0];
+    const T h = M.h;
+    const T dinv = T(4) / (M.h * M.h);
+
+    for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+    __syncthreads();
+
+    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        const int b = blocklist[bi] - 1;
+        int org[3];
+        {
+            int r = b;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                org[d] = (r % M.nb[d]) * 4 - 1;
+                r /= M.nb[d];
+            }
+        }
+        const int s0 = offsets[b], s1 = offsets[b + 1];
+        for (int b0 = s0; b0 < s1; b0 += NR) {
+            const int nbat = min(NR, s1 - b0);
+            // ---- 1a. window start -> group and rank
+            int pid[ITEMS], grp[ITEMS], rank[ITEMS];
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                const int ti = tid + u * NT;
+                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+                grp[u] = -1;
+                rank[u] = 0;
+            }
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                if (pid[u] < 0) continue;
+                const long long p = pid[u];
+                const T l = P.l ? P.l[p] : s.gimp_l;
+                int lo[3], cnt[3];
+                bool inside;
+                if constexpr (X64) {
+                    double x[3], xi[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) x[d] = P.x64[d][p];
+                    inside = axis_window_x64<3, T>(M, s.basis, x, double(l) / M.h64, xi, lo, cnt);
+                } else {
+                    T x[3], xi[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) x[d] = P.x[d][p];
+                    inside = axis_window<3, T>(M, s.basis, x, l / M.h, xi, lo, cnt);
+                }
+                if (!inside) continue;
+                int gi = 0;
+                bool ok = true;
+#pragma unroll
+                for (int d = 2; d >= 0; --d) {
+                    const int q = lo[d] - org[d];
+                    ok = ok && q >= 0 && q < G1;
+                    gi = gi * G1 + q;
+                }
+                if (!ok) {
+                    atomicOr(err, ERR_TILE_RANGE);
+                    continue;
+                }
+                grp[u] = gi;
+                rank[u] = atomicAdd(&gcount[gi], 1);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                int carry = 0;
+                for (int g0 = 0; g0 < NG; g0 += 32) {
+                    const int g = g0 + lane;
+                    const int c = g < NG ? gcount[g] : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    if (g < NG) gstart[g] = carry + incl - c;
+                    carry += __shfl_sync(0xffffffffu, incl, 31);
+                }
+                if (lane == 0) gstart[NG] = carry;
+            } else if (warp == 1) {
+                const int myp = lane < NPENCIL ? lane : -1;
+                int mysize = 0;
+                if (myp >= 0) {
+                    const int gb = G1 * myp;
+#pragma unroll
+                    for (int gx = 0; gx < G1; ++gx) mysize += gcount[gb + gx];
+                }
+                int rk = 0;
+                for (int o = 0; o < NPENCIL; ++o) {
+                    const int os = __shfl_sync(0xffffffffu, mysize, o);
+                    rk += (os > mysize) || (os == mysize && o < lane);
+                }
+                if (myp >= 0) pslot[rk] = myp;
+            }
+            __syncthreads();
+            // ---- 1b. basis (kernel jets, WLS moment inverse) and the record
+            for (int g = tid; g < NG; g += NT) gcount[g] = 0;
+#pragma unroll
+            for (int u = 0; u < ITEMS; ++u) {
+                if (grp[u] < 0) continue;
+                const long long p = pid[u];
+                const T l = P.l ? P.l[p] : s.gimp_l;
+                Basis<3, T> B;
+                T r0[3];
+                if constexpr (X64) {
+                    double x[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) x[d] = P.x64[d][p];
+                    prepare_basis_x64<3, T, WLSF>(M, s.basis, x, l, B, err);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        r0[d] = T(__dadd_rn(M.xmin64[d], __dmul_rn(double(B.ax[d].lo), M.h64)) - x[d]);
+                } else {
+                    T x[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) x[d] = P.x[d][p];
+                    prepare_basis<3, T, WLSF>(M, s.basis, x, l, B, err);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) r0[d] = node_coord(M, d, B.ax[d].lo) - x[d];
+                }
+                T* rr = rec + (gstart[grp[u]] + rank[u]) * RS + SKW * (grp[u] / G1);
+                const T mp = P.m ? P.m[p] : s.mass;
+                const T nV = -P.V[p];
+                rr[R::M] = mp;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) rr[R::MV + d] = mp * P.v[d][p];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) rr[R::S + k] = nV * P.sig[k][p];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        rr[R::W + 3 * d + k] = B.ax[d].val[k];
+                        if constexpr (!WLSF) rr[R::DW + 3 * d + k] = B.ax[d].der[k] * M.h_inv;
+                    }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) rr[R::R0 + d] = r0[d];
+                if constexpr (WLSF) {
+                    rr[R::MI + 0] = B.Mi[0][0];
+                    rr[R::MI + 1] = B.Mi[0][1];
+                    rr[R::MI + 2] = B.Mi[0][2];
+                    rr[R::MI + 3] = B.Mi[0][3];
+                    rr[R::MI + 4] = B.Mi[1][1];
+                    rr[R::MI + 5] = B.Mi[1][2];
+                    rr[R::MI + 6] = B.Mi[1][3];
+                    rr[R::MI + 7] = B.Mi[2][2];
+                    rr[R::MI + 8] = B.Mi[2][3];
+                    rr[R::MI + 9] = B.Mi[3][3];
+                }
+                if constexpr (APICF) {
+                    const T md = mp * dinv;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) rr[R::DB + k] = md * P.B[k][p];
+                }
+            }
+            __syncthreads();
+            // ---- 2. plane sweeps: lane (pencil slot, z slot k)
+            if (tid < 3 * NPENCIL) {
+                const int slot = tid / 3, k = tid - 3 * slot;
+                const int pc = pslot[slot];
+                const int gbase = G1 * pc;
+                const T* prec = rec + SKW * pc;
+                T acc[3][3][NC];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) acc[i][j][c] = T(0);
+                int qs = gstart[gbase];
+#pragma unroll
+                for (int gx = 0; gx < G1 + 2; ++gx) {
+                    if (gx < G1) {
+                        const int qe = gstart[gbase + gx + 1];
+                        for (int q = qs; q < qe; ++q) {
+                            const T* r = prec + q * RS;
+                            const T mp = r[R::M];
+                            const T mv[3] = {r[R::MV], r[R::MV + 1], r[R::MV + 2]};
+                            const T S[6] = {r[R::S], r[R::S + 1], r[R::S + 2], r[R::S + 3], r[R::S + 4], r[R::S + 5]};
+                            const T wz = r[R::W + 6 + k];
+                            const T rz = r[R::R0 + 2] + T(k) * h;
+                            T mi[10] = {}, db[9] = {}, dz = T(0);
+                            if constexpr (WLSF) {
+#pragma unroll
+                                for (int c = 0; c < 10; ++c) mi[c] = r[R::MI + c];
+                            } else {
+                                dz = r[R::DW + 6 + k];
+                            }
+                            if constexpr (APICF) {
+#pragma unroll
+                                for (int c = 0; c < 9; ++c) db[c] = r[R::DB + c];
+                            }
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) {
+                                const T ry = r[R::R0 + 1] + T(j) * h;
+                                const T wyz = r[R::W + 3 + j] * wz;
+                                // per-row constants
+                                T A = T(0), Cd[3] = {T(0), T(0), T(0)}, dyz = T(0), wdz = T(0);
+                                if constexpr (WLSF) {
+                                    A = mi[0] + mi[2] * ry + mi[3] * rz;
+                                    Cd[0] = mi[1] + mi[5] * ry + mi[6] * rz;  // row 1: Mi10 Mi11 Mi12 Mi13
+                                    Cd[1] = mi[2] + mi[7] * ry + mi[8] * rz;  // row 2: Mi20 Mi21 Mi22 Mi23
+                                    Cd[2] = mi[3] + mi[8] * ry + mi[9] * rz;  // row 3: Mi30 Mi31 Mi32 Mi33
+                                } else {
+                                    dyz = r[R::DW + 3 + j] * wz;
+                                    wdz = r[R::W + 3 + j] * dz;
+                                }
+                                T U[3] = {mv[0], mv[1], mv[2]};
+                                if constexpr (APICF) {
+#pragma unroll
+                                    for (int a = 0; a < 3; ++a) U[a] += db[a + 3] * ry + db[a + 6] * rz;
+                                }
+#pragma unroll
+                                for (int i = 0; i < 3; ++i) {
+                                    const T rx = r[R::R0] + T(i) * h;
+                                    const T wx = r[R::W + i];
+                                    const T w = wx * wyz;
+                                    T N, Gd[3];
+                                    if constexpr (WLSF) {
+                                        N = w * (A + mi[1] * rx);
+                                        Gd[0] = w * (Cd[0] + mi[4] * rx);
+                                        Gd[1] = w * (Cd[1] + mi[5] * rx);
+                                        Gd[2] = w * (Cd[2] + mi[6] * rx);
+                                    } else {
+                                        N = w;
+                                        Gd[0] = r[R::DW + i] * wyz;
+                                        Gd[1] = wx * dyz;
+                                        Gd[2] = wx * wdz;
+                                    }
+                                    acc[i][j][0] += N * mp;
+#pragma unroll
+                                    for (int a = 0; a < 3; ++a) {
+                                        T va = U[a];
+                                        if constexpr (APICF) va += db[a] * rx;
+                                        acc[i][j][1 + a] += N * va;
+                                    }
+                                    acc[i][j][4] += S[0] * Gd[0] + S[1] * Gd[1] + S[2] * Gd[2];
+                                    acc[i][j][5] += S[1] * Gd[0] + S[3] * Gd[1] + S[4] * Gd[2];
+                                    acc[i][j][6] += S[2] * Gd[0] + S[4] * Gd[1] + S[5] * Gd[2];
+                                }
+                            }
+                        }
+                        qs = qe;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        T* dst = part + ((j + 3 * k) * NPENCIL + pc) * TS + gx;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            dst[c * CSTR] = acc[0][j][c];
+                            acc[0][j][c] = acc[1][j][c];
+                            acc[1][j][c] = acc[2][j][c];
+                            acc[2][j][c] = T(0);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- 3. per tile node inside the mesh: sum of the staged partials
+            for (int t = tid; t < TN; t += NT) {
+                const int tx = t % TS, ty = (t / TS) % TS, tz = t / (TS * TS);
+                const int nx = org[0] + tx, ny = org[1] + ty, nz = org[2] + tz;
+                if (nx < 0 || ny < 0 || nz < 0 || nx >= M.n[0] || ny >= M.n[1] || nz >= M.n[2]) continue;
+                T val[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) val[c] = T(0);
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const int gy = ty - jj, gz = tz - kk;
+                        if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
+                        const int idx = ((jj + 3 * kk) * NPENCIL + gy + G1 * gz) * TS + tx;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
+                    }
+                const long long lin = (long long)nx + (long long)M.n[0] * (ny + (long long)M.n[1] * nz);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
+                if (val[0] != T(0)) atomicAdd(G.m + lin, val[0]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (val[1 + d] != T(0)) atomicAdd(G.mv[d] + lin, val[1 + d]);
+                    if (val[4 + d] != T(0)) atomicAdd(G.f[d] + lin, val[4 + d]);
+                }
+            }
+        }
+    }
+}
+
+template <class T, bool WLSF, bool APICF, int NR>
+size_t gen_smem_bytes() {
+    using SH = PencilShape<3, 4>;
+    return sizeof(T) * (size_t(NR) * GenRec<WLSF, APICF>::SIZE + 2 * SH::NPENCIL + SH::NPART) +
+           sizeof(int) * size_t(SH::NG + SH::NG + 1 + 32);
+}
+
+template <class T, bool X64, bool WLSF, bool APICF>
+cudaError_t launch_gen_plane_t(const DMesh<3, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                               const BinBuffers& b, const LaunchCfg& cfg) {
+    // Records per batch: 256 in FP32 (2 CTAs per SM), 128 in FP64.
+    constexpr int NR = sizeof(T) == 4 ? 256 : 128;
+    auto kern = p2g_gen_plane_kernel<T, X64, WLSF, APICF, NR>;
+    const size_t smem = gen_smem_bytes<T, WLSF, APICF, NR>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, GEN_THREADS, smem);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    KernelScope ks(cfg, "p2g");
+    kern<<<grid, GEN_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
+    ++*cfg.launches;
+    return cudaGetLastError();
+}
+
+template <class T, bool X64>
+cudaError_t launch_gen_plane(const DMesh<3, T>& M, const PView<T>& P, const GView<T>& G, const Scalars<T>& s,
+                             const BinBuffers& b, const LaunchCfg& cfg) {
+    const bool wls = s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
+    const bool apic = s.transfer == TB_TRANSFER_APIC;
+    if (wls && apic) return launch_gen_plane_t<T, X64, true, true>(M, P, G, s, b, cfg);
+    if (wls) return launch_gen_plane_t<T, X64, true, false>(M, P, G, s, b, cfg);
+    return launch_gen_plane_t<T, X64, false, true>(M, P, G, s, b, cfg);
+}
+
 template <int D, class T, int BW, int NR, int MODE>
 size_t pencil_smem_bytes() {
     using SH = PencilShape<D, BW>;
@@ -1513,13 +1895,18 @@ cudaError_t launch_p2g(const DMesh<D, T>& M, const PView<T>& P, const GView<T>& 
                        const BinBuffers& b, const LaunchCfg& cfg) {
     if (P.n == 0) return cudaSuccess;
     const bool gen = s.transfer == TB_TRANSFER_APIC || s.basis == TB_WLS_BSPLINE_QUADRATIC || s.basis == TB_WLS_UGIMP;
-    if (P.x64[0]) {  // FP64-position form: plain path, FP32 state only (checked by the caller)
+    if (P.x64[0]) {  // FP64-position form: FP32 state only (checked by the caller)
         if constexpr (sizeof(T) == 4) {
             if (!gen) return launch_pencil<D, T, BW, true>(M, P, G, s, b, cfg);
+            if constexpr (D == 3 && BW == 4) return launch_gen_plane<T, true>(M, P, G, s, b, cfg);
         }
         return cudaErrorInvalidValue;
     }
-    return gen ? launch_group<D, T, BW, true>(M, P, G, s, b, cfg) : launch_pencil<D, T, BW, false>(M, P, G, s, b, cfg);
+    if (gen) {
+        if constexpr (D == 3 && BW == 4) return launch_gen_plane<T, false>(M, P, G, s, b, cfg);
+        return launch_group<D, T, BW, true>(M, P, G, s, b, cfg);
+    }
+    return launch_pencil<D, T, BW, false>(M, P, G, s, b, cfg);
 }
 
 #define TB_INST_P2G(D, T, BW)                                                                        \

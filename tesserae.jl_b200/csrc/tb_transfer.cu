@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
             T gv[3][3] = {}, Bn[3][3] = {};
             Basis<D, T> B;
             bool in;
-            if constexpr (X64) in = prepare_basis_x64<D, T>(M, s.basis, xd, l, B, err);
+            if constexpr (X64) in = prepare_basis_x64<D, T, GEN>(M, s.basis, xd, l, B, err);
             else in = prepare_basis<D, T, GEN>(M, s.basis, x, l, B, err);
             if (in) {
                 int q0[3] = {0, 0, 0};
@@ -430,7 +430,13 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
                                                        : (q0[0] + i) + TS * (q0[1] + jj);
                                 T rel[3] = {T(0), T(0), T(0)};
 #pragma unroll
-                                for (int d = 0; d < D; ++d) rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
+                                for (int d = 0; d < D; ++d) {
+                                    if constexpr (X64)  // X_i - x_p in FP64, rounded once
+                                        rel[d] = T(__dadd_rn(M.xmin64[d], __dmul_rn(double(B.ax[d].lo + idx[d]), M.h64)) -
+                                                   xd[d]);
+                                    else
+                                        rel[d] = node_coord(M, d, B.ax[d].lo + idx[d]) - x[d];
+                                }
                                 T w, dw[3];
                                 eval_node<D, T>(M, B, i, jj, k, rel, w, dw);
                                 T vi[3], dvi[3];
@@ -667,12 +673,11 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
     if constexpr (D == 3) {
         if (vm) kern = gen ? g2p_tile_kernel<D, T, BW, true, false, true> : g2p_tile_kernel<D, T, BW, false, false, true>;
     }
-    if (P.x64[0]) {  // FP64-position form: plain path, FP32 state only (checked by the caller)
+    if (P.x64[0]) {  // FP64-position form: FP32 state only (checked by the caller)
         if constexpr (sizeof(T) == 4) {
-            if (gen) return cudaErrorInvalidValue;
-            kern = g2p_tile_kernel<D, T, BW, false, true>;
+            kern = gen ? g2p_tile_kernel<D, T, BW, true, true> : g2p_tile_kernel<D, T, BW, false, true>;
             if constexpr (D == 3) {
-                if (vm) kern = g2p_tile_kernel<D, T, BW, false, true, true>;
+                if (vm) kern = gen ? g2p_tile_kernel<D, T, BW, true, true, true> : g2p_tile_kernel<D, T, BW, false, true, true>;
             }
         } else {
             return cudaErrorInvalidValue;

@@ -104,7 +104,7 @@ def cube3d(scale: int = 1, seed: int | None = None) -> Scene:
     return Scene("cube3d", mesh, P, prm, 100, {"E": E, "nu": nu, "rho0": rho0, "cells": cells})
 
 
-def _lattice_on_device(mesh: CartesianMesh, box, device, dtype, optional=()) -> Particles:
+def _lattice_on_device(mesh: CartesianMesh, box, device, dtype, optional=(), x64=False) -> Particles:
     """Particles on `device` (torch) at the GridSampling points of `mesh` inside
     `box`, in the column-major order of `generate_points`, built from the axes
     on the device without forming the points on the host."""
@@ -112,7 +112,7 @@ def _lattice_on_device(mesh: CartesianMesh, box, device, dtype, optional=()) -> 
     axes = sampling_axes(GridSampling(), mesh, box)
     sizes = [len(a) for a in axes]
     n = int(np.prod(sizes))
-    P = Particles(n, mesh.dim, dtype, backend="torch", device=device, optional=optional)
+    P = Particles(n, mesh.dim, dtype, backend="torch", device=device, optional=optional, x64=x64)
     stride = 1
     for d in range(mesh.dim):
         a = torch.from_numpy(axes[d]).to(device=device, dtype=P.x.dtype)
@@ -222,14 +222,15 @@ def sphere3d(scale: int = 1, seed: int | None = None) -> Scene:
     return Scene("sphere3d", mesh, P, prm, 200, {"nu": 0.3, "rho0": 1e3, "target": (0.5 * L, 0.5 * L, 0.8 * L)})
 
 
-def dambreak3d(scale: int = 1, device=None, dtype=np.float64) -> Scene:
+def dambreak3d(scale: int = 1, device=None, dtype=np.float64, x64: bool = False, particles: bool = True) -> Scene:
     """384^3 cells (h = 1/384), column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell,
     weakly compressible fluid p = -K (J - 1) with K = 2e6, rho0 = 1e3, WLS(uGIMP)
     basis with l = h/2, APIC transfer, slip walls on every face, 100 steps at
     dt = 2.5e-5. dt: the configuration's 5e-5 puts the acoustic CFL number
     (sqrt(K / rho0) dt / h) at 0.86; the FP32 run diverges within 50 steps and
     the FP64 run only survives unperturbed. Both are stable at 2.5e-5 (CFL 0.43).
-    With `device`, the particles are built there directly in `dtype` (the full
+    With `device`, the particles are built there directly in `dtype` (FP64
+    positions with `x64`; the full
     scene has 145 M particles: 46 GB of FP64 host state otherwise); the state
     is deterministic (a lattice at rest), so both builds are the same scene."""
     cells = 384 // scale
@@ -237,21 +238,24 @@ def dambreak3d(scale: int = 1, device=None, dtype=np.float64) -> Scene:
     L = cells * h
     mesh = CartesianMesh(h, (0.0, L), (0.0, L), (0.0, L))
     box = [(0.0, 0.4 * L), None, (0.0, 0.8 * L)]
-    if device is None:
+    V0 = (h / 2) ** 3
+    if not particles:  # mesh and parameters only; the state is built per precision form
+        P = None
+    elif device is None:
         pts = generate_points(GridSampling(), mesh, box=box)
         n = pts.shape[1]
         P = Particles(n, 3, np.float64, optional=("B",))
         P.x[...] = pts
     else:
-        P = _lattice_on_device(mesh, box, device, dtype, optional=("B",))
-    V0 = (h / 2) ** 3
-    P.V[...] = V0
+        P = _lattice_on_device(mesh, box, device, dtype, optional=("B",), x64=x64)
+    if P is not None:
+        P.V[...] = V0
     K = 2e6
     prm = step_params(2.5e-5, mass=1e3 * V0, V0=V0, mu=0.0, lam=K, gravity=(0.0, 0.0, -9.81),
                       gimp_l=h / 2, basis=_abi.TB_WLS_UGIMP, transfer=_abi.TB_TRANSFER_APIC,
                       material=_abi.MATERIAL_FLUID, wall_mask=0b111111, wall_layers=2)
     return Scene("dambreak3d", mesh, P, prm, 100, {"K": K, "rho0": 1e3, "scale": scale,
-                                                   "built_on_device": device is not None})
+                                                   "built_on_device": device is not None or not particles})
 
 
 SCENES = {"readme2d": readme2d, "cube3d": cube3d, "clusters3d": clusters3d, "sphere3d": sphere3d,

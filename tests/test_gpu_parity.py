@@ -329,6 +329,38 @@ def test_step_x64_vs_fp64_oracle(tb, oracle, ctx):
         assert a * 10 <= b, res
 
 
+def test_step_x64_wls_apic_vs_fp64_oracle(tb, oracle, ctx):
+    """The FP64-position form on the WLS(uGIMP) + APIC fluid dam break (3D,
+    slip walls) after 40 steps against the FP64 oracle: relative L2 error <= 1e-6
+    on positions, <= 1e-5 on velocities and <= 1e-4 on displacements, and at
+    least 10x below the Float32-position form in displacement (the fluid moves
+    little in 40 steps, so a Float32 position's rounding is large against its
+    displacement)."""
+    from tesserae_b200 import runtime
+    sc = tb.scenes.dambreak3d(scale=8)
+    mesh, prm = sc.mesh, sc.params
+    P64 = sc.particles
+    x0 = P64.x.copy()
+    nsteps = 40
+    got = {}
+    for form, kw in (("f32", {}), ("x64", {"x64": True})):
+        Pd = P64.to("torch", device="cuda", dtype=np.float32, **kw)
+        part = tb.Partition(mesh, P64.n, backend="torch", device="cuda")
+        Gd = tb.generate_grid(mesh, np.float32, backend="torch", device="cuda")
+        runtime.step(Gd, Pd, part, mesh, prm, nsteps, ctx=ctx)
+        ctx.synchronize()
+        got[form] = Pd.numpy()
+    Po = P64.to("numpy")
+    oracle.step_parallel(mesh, Po, tb.generate_grid(mesh), prm, nsteps, 0)
+    res = {}
+    for form, g in got.items():
+        res[form] = (rel_l2(g["x"].astype(np.float64), Po.x), rel_l2(g["v"].astype(np.float64), Po.v),
+                     rel_l2(g["x"].astype(np.float64) - x0, Po.x - x0))
+    ex, ev, eu = res["x64"]
+    assert ex <= 1e-6 and ev <= 1e-5 and eu <= 1e-4, res
+    assert eu * 10 <= res["f32"][2], res
+
+
 def test_step_x64_binning_matches_fp64(tb, oracle, ctx):
     """Binning in the FP64-position form follows the Float64 findblock rule: the
     partition after one step equals the oracle's FP64 binning of the new
