@@ -403,10 +403,21 @@ def test_rollout_host_x64_matches_device_step(tb, ctx):
 
 
 def test_x64_rejects_other_forms(tb, ctx):
-    """The FP64-position form runs the B-spline / uGIMP FLIP step only: APIC is
-    refused with TB_ERR_UNSUPPORTED, and the per-kernel verbs refuse it in Python."""
+    """The FP64-position form runs every basis and transfer in 3D, the B-spline /
+    uGIMP FLIP step only in 2D: 2D APIC is refused with TB_ERR_UNSUPPORTED (3D
+    APIC without a B array is an argument error), and the per-kernel verbs
+    refuse the form in Python."""
     import ctypes
     from tesserae_b200 import runtime
+    sc2 = tb.scenes.readme2d()
+    P2 = sc2.particles.to("torch", device="cuda", dtype=np.float32, x64=True)
+    part2 = tb.Partition(sc2.mesh, P2.n, backend="torch", device="cuda")
+    G2 = tb.generate_grid(sc2.mesh, np.float32, backend="torch", device="cuda")
+    prm2 = type(sc2.params).from_buffer_copy(sc2.params)
+    prm2.transfer = tb._abi.TB_TRANSFER_APIC
+    rc = ctx.lib.tb_step_f32x64(ctx.ptr, ctypes.byref(sc2.mesh.struct()), ctypes.byref(P2.struct()),
+                                ctypes.byref(part2.struct()), ctypes.byref(G2.struct()), ctypes.byref(prm2), 1)
+    assert rc == tb._abi.TB_ERR_UNSUPPORTED
     sc, P = small_scene(tb, "cube", np.float32)
     mesh = sc.mesh
     Pd = P.to("torch", device="cuda", x64=True)
@@ -416,7 +427,7 @@ def test_x64_rejects_other_forms(tb, ctx):
     prm.transfer = tb._abi.TB_TRANSFER_APIC
     rc = ctx.lib.tb_step_f32x64(ctx.ptr, ctypes.byref(mesh.struct()), ctypes.byref(Pd.struct()),
                                 ctypes.byref(part.struct()), ctypes.byref(Gd.struct()), ctypes.byref(prm), 1)
-    assert rc == tb._abi.TB_ERR_UNSUPPORTED
+    assert rc == tb._abi.TB_ERR_ARG  # APIC needs particles.B
     with pytest.raises(TypeError):
         runtime.G2P(Gd, Pd, mesh, sc.params, ctx=ctx)
 
