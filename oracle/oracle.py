@@ -49,6 +49,7 @@ def lib(abi):
         "tbo_supportnodes": [C.c_int, P(abi.tb_mesh), C.c_int, P(dbl), dbl, P(i64)],
         "tbo_adjoint_step": [C.c_int, P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid),
                              P(abi.tb_step_params), P(abi.tb_adjoint)],
+        "tbo_step_dual": [P(abi.tb_mesh), P(abi.tb_particles), P(abi.tb_grid), P(abi.tb_step_params), C.c_int],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -127,6 +128,54 @@ class Oracle:
         _check(self.L.tbo_adjoint_step(_prec(particles.dtype), C.byref(mesh.struct()),
                                        C.byref(particles.struct()), C.byref(grid.struct()), C.byref(params),
                                        C.byref(adjoint.struct())), "adjoint_step")
+
+    def directional_derivative(self, mesh, particles, params, nsteps, seed: dict, outputs=("x", "v")):
+        """Forward-mode derivative of `nsteps` sequential FP64 steps: the state
+        of host FP64 `particles` is advanced in dual numbers whose derivative
+        parts start as `seed` (field name -> array shaped like the field, zero
+        for the fields not named); returns ({field: final value}, {field:
+        derivative of the final value}) for `outputs`. `particles` is left
+        unchanged."""
+        import numpy as np
+        from types import SimpleNamespace
+        abi = self.abi
+        fields = [k for k in particles.FIELDS if getattr(particles, k) is not None]
+        duals = {}
+        for k in fields:
+            a = np.asarray(getattr(particles, k), dtype=np.float64)
+            d = np.zeros(a.shape + (2,))
+            d[..., 0] = a
+            if k in seed:
+                d[..., 1] = np.asarray(seed[k], dtype=np.float64)
+            duals[k] = d
+
+        def rows(a, k):
+            return [a[i].ctypes.data for i in range(k)] if a.ndim == 3 else [a.ctypes.data]
+
+        s = abi.tb_particles()
+        D = particles.dim
+        s.n = particles.n
+        nsym = 6 if D == 3 else 3
+        for name, k, cnt in (("x", "x", D), ("v", "v", D), ("grad_v", "grad_v", D * D), ("sigma", "sigma", nsym),
+                             ("F", "F", D * D), ("B", "B", D * D), ("Cp_inv", "Cp_inv", nsym)):
+            if k in duals:
+                for i, ptr in enumerate(rows(duals[k], cnt)):
+                    getattr(s, name)[i] = ptr
+        for name, k in (("V", "V"), ("m", "m"), ("l", "l"), ("V0", "V0"), ("mu", "mu"), ("lambda_", "lam"),
+                        ("eps_p", "eps_p")):
+            if k in duals:
+                setattr(s, name, duals[k].ctypes.data)
+        nn = mesh.nnodes
+        gd = {k: np.zeros((D, nn, 2)) for k in ("mv", "f", "v", "vn")}
+        gm = np.zeros((nn, 2))
+        g = abi.tb_grid()
+        g.m = gm.ctypes.data
+        for k, arr in gd.items():
+            for i in range(D):
+                getattr(g, k)[i] = arr[i].ctypes.data
+        _check(self.L.tbo_step_dual(C.byref(mesh.struct()), C.byref(s), C.byref(g), C.byref(params), nsteps),
+               "step_dual")
+        return ({k: duals[k][..., 0].copy() for k in outputs}, {k: duals[k][..., 1].copy() for k in outputs})
 
     def supportnodes(self, mesh, basis, x, l=0.0):
         xs = (C.c_double * 3)(*list(x) + [0.0] * (3 - len(x)))

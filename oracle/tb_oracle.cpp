@@ -270,6 +270,16 @@ int tbo_adjoint_step(int prec, const tb_mesh* m, tb_particles* p, tb_grid* g, co
     TBO_DISPATCH(do_adjoint_step, m, p, g, prm, a);
 }
 
+// The sequential step in forward-mode dual numbers: every particle and grid
+// array (F included) holds (value, derivative) pairs of doubles.
+int tbo_step_dual(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm, int nsteps) {
+    if (m == nullptr) return TB_ERR_ARG;
+    if (prm->material == TB_MATERIAL_VONMISES) return TB_ERR_UNSUPPORTED;
+    if (m->dim == 3) return do_step<3, Dual>(m, p, g, prm, nsteps);
+    if (m->dim == 2) return do_step<2, Dual>(m, p, g, prm, nsteps);
+    return TB_ERR_UNSUPPORTED;
+}
+
 int tbo_max_threads(void) { return omp_get_max_threads(); }
 
 // 1-D jets for the known-answer tests of test/basis.jl:309-311.

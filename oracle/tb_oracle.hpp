@@ -29,10 +29,60 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <type_traits>
 
 #include "../include/tesserae_b200.h"
 
 namespace tbo {
+
+// ---------------------------------------------------------------------------
+// forward-mode dual numbers: a value and one directional derivative, carried
+// through the same templated step (T = Dual, with the FP64 kinematics in Dual
+// too) to give directional derivatives of a rollout: the gradient check of the
+// hand-written reverse step that stands in for differentiating the reference
+// with ForwardDiff (which cannot run here). Floors and comparisons act on the
+// value (piecewise constant), |x| and the kernels' branches follow the value,
+// as ForwardDiff's Dual numbers do.
+// ---------------------------------------------------------------------------
+
+struct Dual {
+    double v = 0.0, d = 0.0;
+    Dual() = default;
+    Dual(double a) : v(a), d(0.0) {}  // constants carry no derivative
+    Dual(double a, double b) : v(a), d(b) {}
+    explicit operator double() const { return v; }
+    explicit operator float() const { return float(v); }
+    explicit operator int64_t() const { return int64_t(v); }
+    Dual operator-() const { return Dual(-v, -d); }
+    Dual& operator+=(const Dual& o) { v += o.v; d += o.d; return *this; }
+    Dual& operator-=(const Dual& o) { v -= o.v; d -= o.d; return *this; }
+    Dual& operator*=(const Dual& o) { d = d * o.v + v * o.d; v *= o.v; return *this; }
+    Dual& operator/=(const Dual& o) { d = (d * o.v - v * o.d) / (o.v * o.v); v /= o.v; return *this; }
+};
+inline Dual operator+(Dual a, const Dual& b) { return a += b; }
+inline Dual operator-(Dual a, const Dual& b) { return a -= b; }
+inline Dual operator*(Dual a, const Dual& b) { return a *= b; }
+inline Dual operator/(Dual a, const Dual& b) { return a /= b; }
+inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+inline bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
+inline bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
+inline bool operator==(const Dual& a, const Dual& b) { return a.v == b.v; }
+inline bool operator!=(const Dual& a, const Dual& b) { return a.v != b.v; }
+
+template <class T> inline T floor_(T x) { return std::floor(x); }
+template <class T> inline T fabs_(T x) { return std::fabs(x); }
+template <class T> inline bool signbit_(T x) { return std::signbit(x); }
+template <class T> inline T log_(T x) { return std::log(x); }
+inline Dual floor_(Dual x) { return Dual(std::floor(x.v), 0.0); }
+inline Dual fabs_(Dual x) { return std::signbit(x.v) ? -x : x; }
+inline bool signbit_(Dual x) { return std::signbit(x.v); }
+inline Dual log_(Dual x) { return Dual(std::log(x.v), x.d / x.v); }
+
+// The type of the FP64 kinematics (F, det F, log J, the stress): double for the
+// float and double forms, Dual for the dual form.
+template <class T> struct Wide { using type = double; };
+template <> struct Wide<Dual> { using type = Dual; };
 
 // ---------------------------------------------------------------------------
 // mesh
@@ -96,7 +146,7 @@ template <int D, class T>
 inline int32_t findblock(const Mesh<D, T>& M, const T* x) {
     int64_t b[3] = {0, 0, 0};
     for (int d = 0; d < D; ++d) {
-        T c = std::floor((x[d] - M.xmin[d]) * M.h_inv);
+        T c = floor_((x[d] - M.xmin[d]) * M.h_inv);
         if (!(c >= T(0) && c <= T(M.n[d] - 2))) return 0;
         b[d] = int64_t(c) >> M.L;
     }
@@ -127,8 +177,8 @@ struct Weights {
 // forward-mode AD through abs()). Known answer: jet(0) = (0.75, 0.0) (test/basis.jl:311).
 template <class T>
 inline void jet_bspline_quadratic(T xi, T& val, T& der) {
-    T s = std::signbit(xi) ? T(-1) : T(1);
-    T a = std::fabs(xi);
+    T s = signbit_(xi) ? T(-1) : T(1);
+    T a = fabs_(xi);
     if (a < T(0.5)) {
         val = (T(3) - T(4) * (a * a)) / T(4);
         der = -(T(2) * a) * s;
@@ -145,8 +195,8 @@ inline void jet_bspline_quadratic(T xi, T& val, T& der) {
 // 1-D jet of uGIMP with l normalised by h (src/Basis/gimp.jl:28-33).
 template <class T>
 inline void jet_ugimp(T xi, T l, T& val, T& der) {
-    T s = std::signbit(xi) ? T(-1) : T(1);
-    T a = std::fabs(xi);
+    T s = signbit_(xi) ? T(-1) : T(1);
+    T a = fabs_(xi);
     if (a < l / T(2)) {
         val = T(1) - (T(4) * (a * a) + l * l) / (T(4) * l);
         der = -(T(2) * a / l) * s;
@@ -170,7 +220,7 @@ inline bool normalize_inside(const Mesh<D, T>& M, const T* x, T* xi) {
     bool inside = true;
     for (int d = 0; d < D; ++d) {
         xi[d] = (x[d] - M.xmin[d]) * M.h_inv;
-        T c = std::floor(xi[d]);
+        T c = floor_(xi[d]);
         inside = inside && (c >= T(0) && c <= T(M.n[d] - 2));
     }
     return inside;
@@ -182,7 +232,7 @@ template <int D, class T>
 inline void window_bspline_quadratic(const Mesh<D, T>& M, const T* xi, Weights<D, T>& W) {
     for (int d = 0; d < 3; ++d) { W.lo[d] = 0; W.cnt[d] = 1; }
     for (int d = 0; d < D; ++d) {
-        int64_t s = int64_t(std::floor(xi[d] - T(1) / T(2)));
+        int64_t s = int64_t(floor_(xi[d] - T(1) / T(2)));
         int64_t e = s + 2;
         int64_t lo = std::max<int64_t>(s, 0), hi = std::min<int64_t>(e, M.n[d] - 1);
         W.lo[d] = lo;
@@ -197,8 +247,8 @@ inline void window_ugimp(const Mesh<D, T>& M, const T* xi, T lnorm, Weights<D, T
     T r = T(1) + lnorm / T(2);
     for (int d = 0; d < 3; ++d) { W.lo[d] = 0; W.cnt[d] = 1; }
     for (int d = 0; d < D; ++d) {
-        int64_t s = int64_t(std::floor(xi[d] - r)) + 1;
-        int64_t e = int64_t(std::floor(xi[d] + r));
+        int64_t s = int64_t(floor_(xi[d] - r)) + 1;
+        int64_t e = int64_t(floor_(xi[d] + r));
         int64_t lo = std::max<int64_t>(s, 0), hi = std::min<int64_t>(e, M.n[d] - 1);
         W.lo[d] = lo;
         W.cnt[d] = hi - lo + 1;
@@ -245,7 +295,7 @@ inline void nodewise_values(const Mesh<D, T>& M, const T* x, Weights<D, T>& W, J
 template <class T>
 inline void bspline_quadratic_axis(T xi, T* v0, T* v1) {
     T u = xi - T(0.5);
-    T t = u - std::floor(u);
+    T t = u - floor_(u);
     const T half = T(1) / T(2);
     v0[0] = half + t * (T(-1) + t * half);
     v0[1] = half + t * (T(1) + t * T(-1));
@@ -284,7 +334,7 @@ inline bool invert(const T (&A)[N][N], T (&Ainv)[N][N]) {
     for (int c = 0; c < N; ++c) {
         int p = c;
         for (int r = c + 1; r < N; ++r)
-            if (std::fabs(a[r][c]) > std::fabs(a[p][c])) p = r;
+            if (fabs_(a[r][c]) > fabs_(a[p][c])) p = r;
         if (a[p][c] == T(0)) return false;
         if (p != c)
             for (int k = 0; k < 2 * N; ++k) std::swap(a[p][k], a[c][k]);
@@ -654,7 +704,7 @@ inline void sym_eigen3(const double (&A)[3][3], double (&e)[3], double (&V)[3][3
             if (a[p][q] == 0.0) continue;
             // the rotation (c, s) that zeroes a[p][q] (sym.schur2)
             const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
-            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs_(theta) + std::sqrt(theta * theta + 1.0));
             const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
             // a <- J^T a J, V <- V J with J = rotation in the (p, q) plane
             for (int k = 0; k < 3; ++k) {
@@ -815,21 +865,22 @@ inline void g2p_particle(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p,
         for (int c = 0; c < D; ++c) P<T>(p.grad_v[r + c * D])[i] = gv[r][c];
     for (int d = 0; d < D; ++d) P<T>(p.x[d])[i] = x[d] + dx[d];
 
-    // FP64 kinematics and constitutive update.
-    double F[3][3], Fn[3][3];
+    // FP64 kinematics and constitutive update (TD = double; Dual in the dual form).
+    using TD = typename Wide<T>::type;
+    TD F[3][3], Fn[3][3];
     for (int r = 0; r < D; ++r)
-        for (int c = 0; c < D; ++c) F[r][c] = CP<double>(p.F[r + c * D])[i];
+        for (int c = 0; c < D; ++c) F[r][c] = CP<TD>(p.F[r + c * D])[i];
     const double dtd = prm.dt;
     for (int r = 0; r < D; ++r)
         for (int c = 0; c < D; ++c) {
-            double a = 0.0;
+            TD a = 0.0;
             for (int k = 0; k < D; ++k) {
-                double Ark = (r == k ? 1.0 : 0.0) + double(gv[r][k]) * dtd;
+                TD Ark = TD(r == k ? 1.0 : 0.0) + TD(gv[r][k]) * TD(dtd);
                 a += Ark * F[k][c];
             }
             Fn[r][c] = a;
         }
-    double J;
+    TD J;
     if (D == 3)
         J = Fn[0][0] * (Fn[1][1] * Fn[2][2] - Fn[1][2] * Fn[2][1]) -
             Fn[0][1] * (Fn[1][0] * Fn[2][2] - Fn[1][2] * Fn[2][0]) +
@@ -837,13 +888,13 @@ inline void g2p_particle(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p,
     else
         J = Fn[0][0] * Fn[1][1] - Fn[0][1] * Fn[1][0];
     for (int r = 0; r < D; ++r)
-        for (int c = 0; c < D; ++c) P<double>(p.F[r + c * D])[i] = Fn[r][c];
-    const double mu = p.mu ? double(CP<T>(p.mu)[i]) : prm.mu;
-    const double lam = p.lambda ? double(CP<T>(p.lambda)[i]) : prm.lambda;
-    double sig[3][3] = {};
+        for (int c = 0; c < D; ++c) P<TD>(p.F[r + c * D])[i] = Fn[r][c];
+    const TD mu = p.mu ? TD(CP<T>(p.mu)[i]) : TD(prm.mu);
+    const TD lam = p.lambda ? TD(CP<T>(p.lambda)[i]) : TD(prm.lambda);
+    TD sig[3][3] = {};
     if (prm.material == TB_MATERIAL_VONMISES) {
         // docs/src/gpu.md:352-358: F = dF F, von Mises state update, V = det(dF) V
-        if constexpr (D == 3) {
+        if constexpr (D == 3 && std::is_same_v<TD, double>) {
             double Cp[3][3], Cpn[3][3], epn = double(CP<T>(p.eps_p)[i]), epo;
             for (int r = 0; r < 3; ++r)
                 for (int c = 0; c < 3; ++c) Cp[r][c] = double(CP<T>(p.Cp_inv[symidx<D>(r, c)])[i]);
@@ -865,19 +916,19 @@ inline void g2p_particle(const Mesh<D, T>& M, const tb_grid& g, tb_particles& p,
         return;
     }
     if (prm.material == 1) {
-        for (int d = 0; d < D; ++d) sig[d][d] = lam * (J - 1.0);
+        for (int d = 0; d < D; ++d) sig[d][d] = lam * (J - TD(1.0));
     } else {
-        const double lj = std::log(J);
+        const TD lj = log_(J);
         for (int r = 0; r < D; ++r)
             for (int c = 0; c < D; ++c) {
-                double b = 0.0;
+                TD b = 0.0;
                 for (int k = 0; k < D; ++k) b += Fn[r][k] * Fn[c][k];
-                sig[r][c] = (mu * (b - (r == c ? 1.0 : 0.0)) + (r == c ? lam * lj : 0.0)) / J;
+                sig[r][c] = (mu * (b - TD(r == c ? 1.0 : 0.0)) + (r == c ? lam * lj : TD(0.0))) / J;
             }
     }
     for (int r = 0; r < D; ++r)
         for (int c = 0; c <= r; ++c) P<T>(p.sigma[symidx<D>(r, c)])[i] = T(sig[r][c]);
-    const double V0 = p.V0 ? double(CP<T>(p.V0)[i]) : prm.V0;
+    const TD V0 = p.V0 ? TD(CP<T>(p.V0)[i]) : TD(prm.V0);
     P<T>(p.V)[i] = T(V0 * J);
 }
 
