@@ -334,6 +334,7 @@ typedef struct tb_adjoint {
     double* F[9];     /* d loss / d F_p, column-major like particles.F */
     double* mu;       /* d loss / d mu_p, accumulated (+=); NULL = not wanted */
     double* lambda;   /* d loss / d lambda_p (the bulk modulus K for fluids), accumulated; NULL = not wanted */
+    double* B[9];     /* d loss / d B_p, column-major like particles.B (TB_TRANSFER_APIC only; NULL otherwise) */
 } tb_adjoint;
 
 /* One step backwards. `particles` holds the state at the START of the step as

@@ -214,7 +214,9 @@ int do_step_parallel(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_ste
 template <int D, class T>
 int do_adjoint_step(const tb_mesh* m, tb_particles* p, tb_grid* g, const tb_step_params* prm, tb_adjoint* a) {
     auto M = make_mesh<D, T>(*m);
-    return adjoint_step<D, T>(M, *p, *g, *prm, *a);
+    if (adjoint_supported(*prm)) return adjoint_step<D, T>(M, *p, *g, *prm, *a);
+    // WLS and KernelCorrection bases, APIC: the general reverse step
+    return adjoint_step_general<D, T>(*m, M, *p, *g, *prm, *a);
 }
 
 #define TBO_DISPATCH(FN, ...)                                                   \

@@ -1081,6 +1081,249 @@ inline void constitutive_adjoint(const double (&F)[3][3], double mu, double lam,
         for (int c = 0; c < D; ++c) Fb[r][c] += Jb * C[r][c];
 }
 
+// ---- reverse step for every basis and the APIC transfer ---------------------
+// The weights' position derivatives come from the weights themselves evaluated
+// in dual numbers (one pass per axis of x_p), so WLS, KernelCorrection and the
+// truncated windows need no hand-derived derivative: dN[s][a] = dN_s/dx_p,a and
+// dG[s][c][a] = d(grad N_s)_c / dx_p,a.
+template <int D>
+struct GenAdjWeights {
+    double w[27], g[27][3], dN[27][3], dG[27][3][3];
+};
+
+template <int D, class T>
+inline void general_adjoint_weights(const tb_mesh& m, int basis, const T* x, T l_abs, const Weights<D, T>& W,
+                                    GenAdjWeights<D>& A) {
+    const Mesh<D, Dual> MD = make_mesh<D, Dual>(m);
+    for (int s = 0; s < 27; ++s) {
+        A.w[s] = double(W.w[s]);
+        for (int c = 0; c < 3; ++c) A.g[s][c] = double(W.dw[s][c]);
+    }
+    for (int a = 0; a < D; ++a) {
+        Dual xd[3];
+        for (int d = 0; d < 3; ++d) xd[d] = Dual(double(x[d]), d == a ? 1.0 : 0.0);
+        Weights<D, Dual> WD;
+        compute_weights(MD, basis, xd, Dual(double(l_abs)), WD);
+        for (int s = 0; s < 27; ++s) {
+            A.dN[s][a] = WD.w[s].d;
+            for (int c = 0; c < 3; ++c) A.dG[s][c][a] = WD.dw[s][c].d;
+        }
+    }
+}
+
+inline bool general_adjoint_supported(const tb_step_params& prm) {
+    return prm.basis >= TB_BSPLINE_QUADRATIC && prm.basis <= TB_KC_UGIMP &&
+           (prm.transfer == TB_TRANSFER_FLIP || prm.transfer == TB_TRANSFER_APIC) &&
+           prm.material != TB_MATERIAL_VONMISES;
+}
+
+// One step backwards for any supported basis with the FLIP/PIC or APIC transfer.
+// Forward (README.md:71-87, docs/src/transfer.md:166-186):
+//   m_i = sum N m_p,  mv_i = sum N m_p u_ip (u = v_p, APIC: v_p + B_p D^-1 r_ip, r = x_i - x_p),
+//   f_i = sum (-V_p sigma_p grad N + N m_p g);  grid half;  then per particle
+//   v_pic = sum N v_i, L = sum v_i (x) grad N, x' = x + dt v_pic, F' = (I + dt L) F,
+//   FLIP: v' = (1 - a) v_pic + a (v_p + sum N (v_i - vn_i));  APIC: v' = v_pic,
+//   B' = sum N v_i (x) r.   `a.B` (APIC) carries the sensitivity to B.
+template <int D, class T>
+inline int adjoint_step_general(const tb_mesh& mraw, const Mesh<D, T>& M, tb_particles& p, tb_grid& g,
+                                const tb_step_params& prm, tb_adjoint& a) {
+    if (!general_adjoint_supported(prm)) return TB_ERR_UNSUPPORTED;
+    const bool apic = prm.transfer == TB_TRANSFER_APIC;
+    if (apic)
+        for (int k = 0; k < D * D; ++k)
+            if (!a.B[k] || !p.B[k]) return TB_ERR_ARG;
+    p2g<D, T>(M, p, g, prm);
+    grid_update<D, T>(M, g, prm);
+    const int64_t nn = M.nnodes;
+    const size_t ndn = static_cast<size_t>(D) * static_cast<size_t>(nn);
+    std::vector<double> vb(ndn, 0.0), vnb(ndn, 0.0), pb(ndn, 0.0), fb(ndn, 0.0);
+    std::vector<double> mb(static_cast<size_t>(nn), 0.0);
+    const double dt = prm.dt, alpha = prm.flip_alpha;
+    const double dinv = 4.0 / (double(M.h) * double(M.h));
+    auto for_nodes = [&](const Weights<D, T>& W, auto&& fn) {
+        if (W.empty) return;
+        for (int k = 0; k < (D == 3 ? W.cnt[2] : 1); ++k)
+            for (int j = 0; j < W.cnt[1]; ++j)
+                for (int ii = 0; ii < W.cnt[0]; ++ii) {
+                    const int s = ii + 3 * j + (D == 3 ? 9 * k : 0);
+                    int64_t node[3] = {W.lo[0] + ii, W.lo[1] + j, W.lo[2] + k};
+                    fn(s, node_linear<D>(M.n, node), node);
+                }
+    };
+    // ---- G2P backwards
+    for (int64_t i = 0; i < p.n; ++i) {
+        T x[3] = {0, 0, 0};
+        for (int d = 0; d < D; ++d) x[d] = CP<T>(p.x[d])[i];
+        const T l = opt<T>(p.l, i, prm.gimp_l);
+        Weights<D, T> W;
+        compute_weights(M, prm.basis, x, l, W);
+        GenAdjWeights<D> A{};
+        if (!W.empty) general_adjoint_weights(mraw, prm.basis, x, l, W, A);
+        double L[3][3] = {};
+        for_nodes(W, [&](int s, int64_t I, const int64_t*) {
+            for (int r = 0; r < D; ++r)
+                for (int c = 0; c < D; ++c) L[r][c] += double(CP<T>(g.v[r])[I]) * A.g[s][c];
+        });
+        double F[3][3] = {}, Fb[3][3] = {};
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                F[r][c] = CP<double>(p.F[r + c * D])[i];
+                Fb[r][c] = a.F[r + c * D][i];
+            }
+        double Lb[3][3] = {}, Fbn[3][3] = {};
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                double s1 = 0.0, s2 = 0.0;
+                for (int k = 0; k < D; ++k) {
+                    s1 += ((r == k ? 1.0 : 0.0) + dt * L[k][r]) * Fb[k][c];
+                    s2 += Fb[r][k] * F[c][k];
+                }
+                Fbn[r][c] = s1;
+                Lb[r][c] = dt * s2;
+            }
+        double xb[3] = {}, vbp[3] = {}, vpicb[3] = {}, dvb[3] = {}, Bb[3][3] = {};
+        for (int d = 0; d < D; ++d) {
+            xb[d] = a.x[d][i];
+            vbp[d] = a.v[d][i];
+            if (apic) {
+                vpicb[d] = vbp[d] + dt * xb[d];
+            } else {
+                dvb[d] = alpha * vbp[d];
+                vpicb[d] = (1.0 - alpha) * vbp[d] + dt * xb[d];
+            }
+        }
+        if (apic)
+            for (int r = 0; r < D; ++r)
+                for (int c = 0; c < D; ++c) Bb[r][c] = a.B[r + c * D][i];
+        for_nodes(W, [&](int s, int64_t I, const int64_t* node) {
+            double vi[3] = {}, vni[3] = {}, rel[3] = {};
+            for (int d = 0; d < D; ++d) {
+                vi[d] = double(CP<T>(g.v[d])[I]);
+                vni[d] = double(CP<T>(g.vn[d])[I]);
+                rel[d] = double(node_coord(M, d, node[d])) - double(x[d]);
+            }
+            double Nb = 0.0, Gb[3] = {0, 0, 0};
+            for (int r = 0; r < D; ++r) {
+                double vb_r = A.w[s] * (vpicb[r] + dvb[r]);
+                for (int c = 0; c < D; ++c) vb_r += Lb[r][c] * A.g[s][c];
+                Nb += vpicb[r] * vi[r] + dvb[r] * (vi[r] - vni[r]);
+                for (int c = 0; c < D; ++c) Gb[c] += Lb[r][c] * vi[r];
+                if (apic) {
+                    double Br = 0.0;
+                    for (int c = 0; c < D; ++c) {
+                        Br += Bb[r][c] * rel[c];
+                        xb[c] -= A.w[s] * vi[r] * Bb[r][c];  // through r = x_i - x_p
+                    }
+                    vb_r += A.w[s] * Br;
+                    Nb += vi[r] * Br;
+                }
+                vb[size_t(r) * nn + I] += vb_r;
+                vnb[size_t(r) * nn + I] += -A.w[s] * dvb[r];
+            }
+            for (int b = 0; b < D; ++b) {
+                double h = 0.0;
+                for (int c = 0; c < D; ++c) h += Gb[c] * A.dG[s][c][b];
+                xb[b] += Nb * A.dN[s][b] + h;
+            }
+        });
+        for (int d = 0; d < D; ++d) {
+            a.x[d][i] = xb[d];
+            a.v[d][i] = apic ? 0.0 : alpha * vbp[d];
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                a.F[r + c * D][i] = Fbn[r][c];
+                if (apic) a.B[r + c * D][i] = 0.0;
+            }
+    }
+    // ---- grid update backwards (walled components were overwritten with 0)
+    for (int64_t I = 0; I < nn; ++I) {
+        const double m = double(CP<T>(g.m)[I]);
+        int64_t idx[3] = {0, 0, 0}, r = I;
+        for (int d = 0; d < D; ++d) { idx[d] = r % M.n[d]; r /= M.n[d]; }
+        double acc = 0.0;
+        for (int d = 0; d < D; ++d) {
+            double v_b = vb[size_t(d) * nn + I], vn_b = vnb[size_t(d) * nn + I];
+            const bool lo = (prm.wall_mask >> (2 * d)) & 1, hi = (prm.wall_mask >> (2 * d + 1)) & 1;
+            if ((lo && idx[d] < prm.wall_layers) || (hi && idx[d] >= M.n[d] - prm.wall_layers)) v_b = vn_b = 0.0;
+            if (m == 0.0) continue;
+            const double vt = vn_b + v_b;
+            fb[size_t(d) * nn + I] = dt * v_b / m;
+            pb[size_t(d) * nn + I] = vt / m;
+            acc += vt * double(CP<T>(g.mv[d])[I]) + dt * v_b * double(CP<T>(g.f[d])[I]);
+        }
+        mb[I] = (m == 0.0) ? 0.0 : -acc / (m * m);
+    }
+    // ---- P2G backwards
+    for (int64_t i = 0; i < p.n; ++i) {
+        ParticleIn<D, T> q;
+        load_particle<D, T>(p, prm, i, q);
+        Weights<D, T> W;
+        compute_weights(M, prm.basis, q.x, q.l, W);
+        double xb[3] = {}, vbs[3] = {}, sb[3][3] = {}, Vb = 0.0, Bbs[3][3] = {};
+        if (!W.empty) {
+            GenAdjWeights<D> A{};
+            general_adjoint_weights(mraw, prm.basis, q.x, q.l, W, A);
+            const double mp = double(q.m), Vp = double(q.V);
+            for_nodes(W, [&](int s, int64_t I, const int64_t* node) {
+                double rel[3] = {}, u[3] = {};
+                for (int d = 0; d < D; ++d) rel[d] = double(node_coord(M, d, node[d])) - double(q.x[d]);
+                for (int d = 0; d < D; ++d) {
+                    u[d] = double(q.v[d]);
+                    if (apic)
+                        for (int c = 0; c < D; ++c) u[d] += double(q.B[d][c]) * dinv * rel[c];
+                }
+                double Nb = mp * mb[I], Gb[3] = {0, 0, 0};
+                for (int d = 0; d < D; ++d) {
+                    const double p_b = pb[size_t(d) * nn + I], f_b = fb[size_t(d) * nn + I];
+                    Nb += mp * (u[d] * p_b + double(T(prm.gravity[d])) * f_b);
+                    const double ub = mp * A.w[s] * p_b;  // d loss / d u_d
+                    vbs[d] += ub;
+                    if (apic)
+                        for (int c = 0; c < D; ++c) {
+                            Bbs[d][c] += ub * dinv * rel[c];
+                            xb[c] -= ub * double(q.B[d][c]) * dinv;  // through r = x_i - x_p
+                        }
+                }
+                for (int r = 0; r < D; ++r) {
+                    const double f_b = fb[size_t(r) * nn + I];
+                    double sg = 0.0;
+                    for (int c = 0; c < D; ++c) {
+                        sg += double(q.sig[r][c]) * A.g[s][c];
+                        Gb[c] += -Vp * double(q.sig[r][c]) * f_b;
+                        sb[r][c] += -Vp * f_b * A.g[s][c];
+                    }
+                    Vb += -f_b * sg;
+                }
+                for (int b = 0; b < D; ++b) {
+                    double h = 0.0;
+                    for (int c = 0; c < D; ++c) h += Gb[c] * A.dG[s][c][b];
+                    xb[b] += Nb * A.dN[s][b] + h;
+                }
+            });
+        }
+        double F[3][3] = {}, Fb[3][3] = {}, mub = 0.0, lamb = 0.0;
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) F[r][c] = CP<double>(p.F[r + c * D])[i];
+        const double mu = p.mu ? double(CP<T>(p.mu)[i]) : prm.mu;
+        const double lam = p.lambda ? double(CP<T>(p.lambda)[i]) : prm.lambda;
+        const double V0 = p.V0 ? double(CP<T>(p.V0)[i]) : prm.V0;
+        constitutive_adjoint<D>(F, mu, lam, V0, prm.material, sb, Vb, Fb, mub, lamb);
+        for (int d = 0; d < D; ++d) {
+            a.x[d][i] += xb[d];
+            a.v[d][i] += vbs[d];
+        }
+        for (int r = 0; r < D; ++r)
+            for (int c = 0; c < D; ++c) {
+                a.F[r + c * D][i] += Fb[r][c];
+                if (apic) a.B[r + c * D][i] += Bbs[r][c];
+            }
+        if (a.mu) a.mu[i] += mub;
+        if (a.lambda) a.lambda[i] += lamb;
+    }
+    return TB_OK;
+}
+
 // One step backwards on the CPU. `p` is the state at the start of the step,
 // `g` receives the step's forward grid, `a` holds the sensitivities to the
 // end-of-step state on entry and to the start-of-step state on return.

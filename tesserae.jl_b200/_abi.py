@@ -106,7 +106,7 @@ class tb_step_params(C.Structure):
 
 
 class tb_adjoint(C.Structure):
-    _fields_ = [("x", VP * 3), ("v", VP * 3), ("F", VP * 9), ("mu", VP), ("lambda_", VP)]
+    _fields_ = [("x", VP * 3), ("v", VP * 3), ("F", VP * 9), ("mu", VP), ("lambda_", VP), ("B", VP * 9)]
 
 
 class tb_kernel_time(C.Structure):

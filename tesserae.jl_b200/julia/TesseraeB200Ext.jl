@@ -147,6 +147,7 @@ struct TbAdjoint
     F::NTuple{9,Ptr{Float64}}
     mu::Ptr{Float64}
     lambda::Ptr{Float64}
+    B::NTuple{9,Ptr{Float64}}
 end
 
 struct TbKernelTime
@@ -669,7 +670,7 @@ function ChainRulesCore.rrule(::typeof(b200_rollout), v0, particles, grid, parti
         adj = TbAdjoint(ntuple(d -> d <= dim ? row(gx, d) : Ptr{Float64}(0), 3),
                         ntuple(d -> d <= dim ? row(gv, d) : Ptr{Float64}(0), 3),
                         ntuple(k -> k <= dim * dim ? row(gF, k) : Ptr{Float64}(0), 9),
-                        Ptr{Float64}(0), Ptr{Float64}(0))
+                        Ptr{Float64}(0), Ptr{Float64}(0), ntuple(_ -> Ptr{Float64}(0), 9))
         pd, gd = tbparticles(particles), tbgrid(grid)
         GC.@preserve grid particles partition gx gv gF begin
             rc = ccall((sym(:tb_tape_backward, form(particles) === :f64 ? :f64 : :f32), libtb), Int32,

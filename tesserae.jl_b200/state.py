@@ -248,7 +248,7 @@ class Adjoint:
     per-particle Lame parameters, all float64 in both precision forms (the
     tb_adjoint descriptor). `mu` / `lam` accumulate across steps."""
 
-    def __init__(self, n, dim, backend="numpy", device=None, lame=True):
+    def __init__(self, n, dim, backend="numpy", device=None, lame=True, apic=False):
         self.n, self.dim, self.backend = int(n), int(dim), backend
         D = self.dim
         a = lambda shape: _alloc(backend, shape, np.float64, device, 0.0)  # noqa: E731
@@ -257,9 +257,10 @@ class Adjoint:
         self.F = a((D * D, self.n))
         self.mu = a((self.n,)) if lame else None
         self.lam = a((self.n,)) if lame else None
+        self.B = a((D * D, self.n)) if apic else None  # sensitivity to the APIC matrix
 
     def zero_(self):
-        for k in ("x", "v", "F", "mu", "lam"):
+        for k in ("x", "v", "F", "mu", "lam", "B"):
             arr = getattr(self, k)
             if arr is None:
                 continue
@@ -280,11 +281,13 @@ class Adjoint:
             s.F[k] = p
         s.mu = _ptr(self.mu)
         s.lambda_ = _ptr(self.lam)
+        for k, p in enumerate(_row_ptrs(self.B, D * D)):
+            s.B[k] = p
         return s
 
     def numpy(self) -> dict:
         out = {}
-        for k in ("x", "v", "F", "mu", "lam"):
+        for k in ("x", "v", "F", "mu", "lam", "B"):
             a = getattr(self, k)
             if a is not None:
                 out[k] = a if isinstance(a, np.ndarray) else a.detach().cpu().numpy()
