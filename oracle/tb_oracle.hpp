@@ -1007,7 +1007,8 @@ inline void adjoint_weights(const Mesh<D, T>& M, int basis, const T* x, T l_abs,
 }
 
 inline bool adjoint_supported(const tb_step_params& prm) {
-    return (prm.basis == TB_BSPLINE_QUADRATIC || prm.basis == TB_UGIMP) && prm.transfer == TB_TRANSFER_FLIP;
+    return (prm.basis == TB_BSPLINE_QUADRATIC || prm.basis == TB_UGIMP) && prm.transfer == TB_TRANSFER_FLIP &&
+           prm.material != TB_MATERIAL_VONMISES;
 }
 
 template <int D>

@@ -117,6 +117,7 @@ struct tb_ctx {
     bool tape_valid = false;
     long long tape_n = 0;
     int tape_dim = 0, tape_elem = 0;
+    bool tape_apic = false;
     int tape_nsteps = 0, tape_every = 1;
     // reorder_particles!: 8-byte-per-particle scratch, score accumulators,
     // decision words and the score
@@ -865,17 +866,19 @@ int dispatch_g2p2g(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* p
 int check_adjoint_params(tb_ctx* c, const tb_step_params* p) {
     int rc = check_params(c, p);
     if (rc != TB_OK) return rc;
-    if (p->basis != TB_BSPLINE_QUADRATIC && p->basis != TB_UGIMP)
-        return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the quadratic B-spline and uGIMP bases (basis %d)",
-                    p->basis);
-    if (p->transfer != TB_TRANSFER_FLIP)
-        return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the FLIP/PIC transfer only");
     if (p->material == TB_MATERIAL_VONMISES)
         return fail(c, TB_ERR_UNSUPPORTED, "the adjoint supports the Neo-Hookean and fluid materials only");
     return TB_OK;
 }
 
-int make_adjview(tb_ctx* c, const tb_adjoint* a, int dim, long long n, AdjView& A) {
+// The separable, block-scheduled adjoint kernels cover the quadratic B-spline
+// and uGIMP with FLIP/PIC; every other basis and APIC take the general
+// (particle-parallel, Dual3) reverse step.
+bool adjoint_is_general(const tb_step_params* p) {
+    return !(p->basis == TB_BSPLINE_QUADRATIC || p->basis == TB_UGIMP) || p->transfer == TB_TRANSFER_APIC;
+}
+
+int make_adjview(tb_ctx* c, const tb_adjoint* a, int dim, long long n, AdjView& A, bool apic = false) {
     if (!a) return fail(c, TB_ERR_ARG, "adjoint is NULL");
     std::memset(&A, 0, sizeof A);
     for (int d = 0; d < dim; ++d) {
@@ -889,6 +892,11 @@ int make_adjview(tb_ctx* c, const tb_adjoint* a, int dim, long long n, AdjView& 
     }
     A.mu = a->mu;
     A.lam = a->lambda;
+    if (apic)
+        for (int k = 0; k < dim * dim; ++k) {
+            A.B[k] = a->B[k];
+            if (n && !A.B[k]) return fail(c, TB_ERR_ARG, "adjoint.B component %d is NULL (APIC)", k);
+        }
     return TB_OK;
 }
 
@@ -927,9 +935,10 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     GView<T> G;
     AdjView A;
     GradGrid GB;
-    if ((rc = make_pview<T>(c, p, D, true, false, P)) != TB_OK) return rc;
+    const bool apic = prm->transfer == TB_TRANSFER_APIC;
+    if ((rc = make_pview<T>(c, p, D, true, apic, P)) != TB_OK) return rc;
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
-    if ((rc = make_adjview(c, adj, D, P.n, A)) != TB_OK) return rc;
+    if ((rc = make_adjview(c, adj, D, P.n, A, apic)) != TB_OK) return rc;
     if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
     if (cudaError_t ce = grow(c->adj_coef, c->adj_coef_cap, std::max<long long>(1, P.n) * (2 * D + D * D));
         ce != cudaSuccess)
@@ -938,7 +947,8 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     if (!part || !part->blocklist || !part->offsets || (P.n && (!part->particleindices || !part->blockids)))
         return fail(c, TB_ERR_ARG, "partition array is NULL");
     const AdjPartition AP{totals, part->blocklist, part->offsets, part->particleindices, part->blockids};
-    const cudaError_t e = launch_adjoint<D, T, BW>(M, G, P, S, A, GB, AP, cfg_of(c));
+    const cudaError_t e = adjoint_is_general(prm) ? launch_adjoint_general<D, T>(M, G, P, S, A, GB, AP, cfg_of(c))
+                                                  : launch_adjoint<D, T, BW>(M, G, P, S, A, GB, AP, cfg_of(c));
     return e == cudaSuccess ? TB_OK : cuda_fail(c, e, "adjoint launch");
 }
 
@@ -969,7 +979,7 @@ struct StateFields {
 };
 
 template <class T>
-StateFields state_fields(tb_particles* p, int D) {
+StateFields state_fields(tb_particles* p, int D, bool apic) {
     StateFields f;
     auto add = [&](void** s, size_t e) {
         f.slot[f.count] = s;
@@ -981,30 +991,32 @@ StateFields state_fields(tb_particles* p, int D) {
     for (int k = 0; k < D * D; ++k) add(&p->F[k], sizeof(double));
     for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&p->sigma[k], sizeof(T));
     add(&p->V, sizeof(T));
+    if (apic)
+        for (int k = 0; k < D * D; ++k) add(&p->B[k], sizeof(T));
     return f;
 }
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 template <class T>
-size_t state_bytes(int D, long long n) {
-    const int nf = 2 * D + (D == 3 ? 6 : 3) + 1;
+size_t state_bytes(int D, long long n, bool apic) {
+    const int nf = 2 * D + (D == 3 ? 6 : 3) + 1 + (apic ? D * D : 0);
     return size_t(nf) * align256(sizeof(T) * size_t(n)) + size_t(D * D) * align256(sizeof(double) * size_t(n));
 }
 
 // One step of a tape segment: the state before the step, the step's forward
 // grid and partition, and its device totals.
 template <class T>
-size_t slot_bytes(int D, long long n, long long nn, long long nb) {
-    return state_bytes<T>(D, n) + size_t(1 + 4 * D) * align256(sizeof(T) * size_t(nn)) +
+size_t slot_bytes(int D, long long n, long long nn, long long nb, bool apic) {
+    return state_bytes<T>(D, n, apic) + size_t(1 + 4 * D) * align256(sizeof(T) * size_t(nn)) +
            2 * align256(sizeof(int) * size_t(n)) + 2 * align256(sizeof(int) * size_t(nb)) +
            align256(sizeof(int) * size_t(nb + 1)) + 256;
 }
 
 template <class T>
-void slot_views(char* base, int D, long long n, long long nn, long long nb, tb_grid& g, tb_partition& part,
-                int*& totals) {
-    char* q = base + state_bytes<T>(D, n);
+void slot_views(char* base, int D, long long n, long long nn, long long nb, bool apic, tb_grid& g,
+                tb_partition& part, int*& totals) {
+    char* q = base + state_bytes<T>(D, n, apic);
     auto take = [&](size_t bytes) {
         char* r = q;
         q += align256(bytes);
@@ -1030,9 +1042,9 @@ void slot_views(char* base, int D, long long n, long long nn, long long nb, tb_g
 
 // Particles whose state fields point into the snapshot at `base`.
 template <class T>
-tb_particles snapshot_view(const tb_particles* p, int D, char* base) {
+tb_particles snapshot_view(const tb_particles* p, int D, char* base, bool apic) {
     tb_particles q = *p;
-    StateFields f = state_fields<T>(&q, D);
+    StateFields f = state_fields<T>(&q, D, apic);
     size_t off = 0;
     for (int i = 0; i < f.count; ++i) {
         *f.slot[i] = base + off;
@@ -1042,9 +1054,9 @@ tb_particles snapshot_view(const tb_particles* p, int D, char* base) {
 }
 
 template <class T>
-int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int D) {
-    StateFields fd = state_fields<T>(const_cast<tb_particles*>(dst), D);
-    StateFields fs = state_fields<T>(const_cast<tb_particles*>(src), D);
+int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int D, bool apic) {
+    StateFields fd = state_fields<T>(const_cast<tb_particles*>(dst), D, apic);
+    StateFields fs = state_fields<T>(const_cast<tb_particles*>(src), D, apic);
     for (int i = 0; i < fd.count; ++i) {
         if (!*fs.slot[i] || !*fd.slot[i]) return fail(c, TB_ERR_ARG, "particle state field %d is NULL", i);
         const cudaError_t e = cudaMemcpyAsync(*fd.slot[i], *fs.slot[i], fd.elem[i] * size_t(src->n),
@@ -1064,15 +1076,16 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
     const int D = m->dim;
     PView<T> P;
-    if ((rc = make_pview<T>(c, p, D, true, false, P)) != TB_OK) return rc;
+    const bool apic = prm->transfer == TB_TRANSFER_APIC;
+    if ((rc = make_pview<T>(c, p, D, true, apic, P)) != TB_OK) return rc;
     c->tape_valid = false;
     const long long ncp = nsteps > 0 ? (nsteps + every - 1) / every : 1;
-    const size_t sb = state_bytes<T>(D, p->n);
+    const size_t sb = state_bytes<T>(D, p->n, apic);
     cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(ncp * sb));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc checkpoints");
     for (long long k = 0; k < ncp; ++k) {
-        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb);
-        if ((rc = copy_state<T>(c, &cp, p, D)) != TB_OK) return rc;
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic);
+        if ((rc = copy_state<T>(c, &cp, p, D, apic)) != TB_OK) return rc;
         const int steps = std::min<long long>(every, nsteps - k * every);
         if (steps > 0 && (rc = dispatch_step<T>(c, m, p, part, g, prm, steps, true, true, true, true)) != TB_OK)
             return rc;
@@ -1081,6 +1094,7 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     c->tape_n = p->n;
     c->tape_dim = D;
     c->tape_elem = int(sizeof(T));
+    c->tape_apic = apic;
     c->tape_nsteps = nsteps;
     c->tape_every = every;
     return TB_OK;
@@ -1094,7 +1108,9 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
         return rc;
     if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
     const int D = m->dim;
-    if (!c->tape_valid || c->tape_n != p->n || c->tape_dim != D || c->tape_elem != int(sizeof(T)))
+    const bool apic = prm->transfer == TB_TRANSFER_APIC;
+    if (!c->tape_valid || c->tape_n != p->n || c->tape_dim != D || c->tape_elem != int(sizeof(T)) ||
+        c->tape_apic != apic)
         return fail(c, TB_ERR_ARG, "no forward tape for these particles on this context (run tb_tape_forward first)");
     (void)part;
     (void)g;
@@ -1102,39 +1118,39 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
     long long nn = 1;
     for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
     const long long nb = mesh_nblocks(m);
-    const size_t sb = state_bytes<T>(D, p->n), slot = slot_bytes<T>(D, p->n, nn, nb);
+    const size_t sb = state_bytes<T>(D, p->n, apic), slot = slot_bytes<T>(D, p->n, nn, nb, apic);
     cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * slot));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape segment");
     const long long ncp = nsteps > 0 ? (nsteps + K - 1) / K : 1;
     for (long long k = ncp - 1; k >= 0 && nsteps > 0; --k) {
         const int len = int(std::min<long long>(K, nsteps - k * K));
-        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb);
-        if ((rc = copy_state<T>(c, p, &cp, D)) != TB_OK) return rc;
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic);
+        if ((rc = copy_state<T>(c, p, &cp, D, apic)) != TB_OK) return rc;
         // re-run the segment, keeping each step's input state, grid and partition
         for (int j = 0; j < len; ++j) {
             char* base = c->tape_seg + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, gj, pj, tj);
-            if ((rc = copy_state<T>(c, &sj, p, D)) != TB_OK) return rc;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
+            if ((rc = copy_state<T>(c, &sj, p, D, apic)) != TB_OK) return rc;
             if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, j + 1 < len)) != TB_OK) return rc;
             e = cudaMemcpyAsync(tj, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
             if (e != cudaSuccess) return cuda_fail(c, e, "tape totals copy");
         }
         for (int j = len - 1; j >= 0; --j) {
             char* base = c->tape_seg + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, gj, pj, tj);
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
             if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj)) != TB_OK) return rc;
         }
     }
-    tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp);
-    return copy_state<T>(c, p, &cp0, D);
+    tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp, apic);
+    return copy_state<T>(c, p, &cp0, D, apic);
 }
 
 }  // namespace

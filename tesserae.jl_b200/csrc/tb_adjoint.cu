@@ -854,6 +854,317 @@ __global__ void __launch_bounds__(256) adj_material_kernel(PView<T> P, Scalars<T
     }
 }
 
+// ---------------------------------------------------------------------------
+// General reverse step (WLS and KernelCorrection bases, the APIC transfer): the
+// oracle's general reverse step on the device, one thread per particle. The
+// weights N_i, grad N_i and their derivatives with respect to x_p come from the
+// basis evaluated in Dual3 (value plus the three x_p derivatives), so no
+// second derivative of a WLS or corrected kernel is written out by hand. The
+// v / vn sensitivities of G2P backwards are scattered with FP64 global atomics
+// (27 nodes x 2D per particle); P2G backwards gathers m_bar, mv_bar, f_bar over
+// the window and leaves sigma_bar, V_bar for adj_material_kernel.
+template <int D, class T>
+__device__ __forceinline__ DMesh<D, Dual3> dual_mesh(const DMesh<D, T>& M) {
+    DMesh<D, Dual3> R;
+    for (int d = 0; d < 3; ++d) {
+        R.n[d] = M.n[d];
+        R.nb[d] = M.nb[d];
+        R.xmin[d] = Dual3(double(M.xmin[d]));
+        R.xmin64[d] = M.xmin64[d];
+    }
+    R.L = M.L;
+    R.nblocks = M.nblocks;
+    R.nnodes = M.nnodes;
+    R.h = Dual3(double(M.h));
+    R.h_inv = Dual3(double(M.h_inv));
+    R.h64 = M.h64;
+    R.h_inv64 = M.h_inv64;
+    return R;
+}
+
+// Basis of particle x in Dual3: dual seeds e_0 .. e_{D-1} on the position.
+template <int D, class T>
+__device__ __forceinline__ bool dual_basis(const DMesh<D, Dual3>& MD, const Scalars<T>& s, const T* x, T l,
+                                           Basis<D, Dual3>& B, int* err) {
+    Dual3 xd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        xd[d] = Dual3(d < D ? double(x[d]) : 0.0);
+        if (d < D) xd[d].d[d] = 1.0;
+    }
+    return prepare_basis<D, Dual3, true>(MD, s.basis, xd, Dual3(double(l)), B, err);
+}
+
+// N, grad N (values and x_p derivatives) at window slot (i, j, k), r = X - x_p.
+template <int D>
+__device__ __forceinline__ void dual_node(const DMesh<D, Dual3>& MD, const Basis<D, Dual3>& B, int i, int j, int k,
+                                          const Dual3* rel, Dual3& N, Dual3* G) {
+    eval_node<D, Dual3>(MD, B, i, j, k, rel, N, G);
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
+                                                          AdjView A, GradGrid GB, const int* __restrict__ blockids,
+                                                          int* err) {
+    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M);
+    const bool apic = s.transfer == TB_TRANSFER_APIC;
+    const double dt = s.dt64, alpha = double(s.alpha);
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n;
+         p += (long long)gridDim.x * blockDim.x) {
+        T x[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+        const T l = P.l ? P.l[p] : s.gimp_l;
+        Basis<D, Dual3> B;
+        const bool in = blockids[p] != 0 && dual_basis<D, T>(MD, s, x, l, B, err);
+        double F[3][3] = {}, Fb[3][3] = {}, L[3][3] = {};
+        load_F<D, T>(P, p, F);
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) Fb[r][c] = A.F[r + c * D][p];
+        auto node_of = [&](int i, int j, int k, long long& I, Dual3 (&rel)[3], bool& valid) {
+            const int idx[3] = {i, j, k};
+            I = 0;
+            valid = true;
+#pragma unroll
+            for (int d = D - 1; d >= 0; --d) {
+                valid = valid && idx[d] < B.ax[d].cnt;
+                I = I * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(double(x[d]));
+                rel[d].d[d] = -1.0;
+            }
+        };
+        if (in) {
+            for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+                for (int j = 0; j < 3; ++j)
+                    for (int i = 0; i < 3; ++i) {
+                        long long I;
+                        Dual3 rel[3];
+                        bool valid;
+                        node_of(i, j, k, I, rel, valid);
+                        if (!valid) continue;
+                        Dual3 N, Gn[3];
+                        dual_node<D>(MD, B, i, j, k, rel, N, Gn);
+#pragma unroll
+                        for (int r = 0; r < D; ++r)
+#pragma unroll
+                            for (int c = 0; c < D; ++c) L[r][c] += double(G.v[r][I]) * Gn[c].v;
+                    }
+        }
+        double Lb[3][3] = {}, Fbn[3][3] = {};
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < D; ++q) {
+                    s1 += ((r == q ? 1.0 : 0.0) + dt * L[q][r]) * Fb[q][c];
+                    s2 += Fb[r][q] * F[c][q];
+                }
+                Fbn[r][c] = s1;
+                Lb[r][c] = dt * s2;
+            }
+        double xb[3] = {}, vbp[3] = {}, vpicb[3] = {}, dvb[3] = {}, Bb[3][3] = {};
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            xb[d] = A.x[d][p];
+            vbp[d] = A.v[d][p];
+            if (apic) {
+                vpicb[d] = vbp[d] + dt * xb[d];
+            } else {
+                dvb[d] = alpha * vbp[d];
+                vpicb[d] = (1.0 - alpha) * vbp[d] + dt * xb[d];
+            }
+        }
+        if (apic) {
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) Bb[r][c] = A.B[r + c * D][p];
+        }
+        if (in) {
+            for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+                for (int j = 0; j < 3; ++j)
+                    for (int i = 0; i < 3; ++i) {
+                        long long I;
+                        Dual3 rel[3];
+                        bool valid;
+                        node_of(i, j, k, I, rel, valid);
+                        if (!valid) continue;
+                        Dual3 N, Gn[3];
+                        dual_node<D>(MD, B, i, j, k, rel, N, Gn);
+                        double vi[3] = {}, vni[3] = {};
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            vi[d] = double(G.v[d][I]);
+                            vni[d] = double(G.vn[d][I]);
+                        }
+                        double Nb = 0.0, Gb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                        for (int r = 0; r < D; ++r) {
+                            double vb_r = N.v * (vpicb[r] + dvb[r]);
+#pragma unroll
+                            for (int c = 0; c < D; ++c) vb_r += Lb[r][c] * Gn[c].v;
+                            Nb += vpicb[r] * vi[r] + dvb[r] * (vi[r] - vni[r]);
+#pragma unroll
+                            for (int c = 0; c < D; ++c) Gb[c] += Lb[r][c] * vi[r];
+                            if (apic) {
+                                double Br = 0.0;
+#pragma unroll
+                                for (int c = 0; c < D; ++c) {
+                                    Br += Bb[r][c] * rel[c].v;
+                                    xb[c] -= N.v * vi[r] * Bb[r][c];
+                                }
+                                vb_r += N.v * Br;
+                                Nb += vi[r] * Br;
+                            }
+                            atomicAdd(GB.vb[r] + I, vb_r);
+                            if (!apic) atomicAdd(GB.vnb[r] + I, -N.v * dvb[r]);
+                        }
+#pragma unroll
+                        for (int b = 0; b < D; ++b) {
+                            double h = 0.0;
+#pragma unroll
+                            for (int c = 0; c < D; ++c) h += Gb[c] * Gn[c].d[b];
+                            xb[b] += Nb * N.d[b] + h;
+                        }
+                    }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            A.x[d][p] = xb[d];
+            A.v[d][p] = apic ? 0.0 : alpha * vbp[d];
+        }
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                A.F[r + c * D][p] = Fbn[r][c];
+                if (apic) A.B[r + c * D][p] = 0.0;
+            }
+    }
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s, AdjView A,
+                                                          GradGrid GB, double* __restrict__ sbar,
+                                                          const int* __restrict__ blockids, int* err) {
+    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M);
+    const bool apic = s.transfer == TB_TRANSFER_APIC;
+    const double dinv = 4.0 / (double(M.h) * double(M.h));
+    const long long n = P.n;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        if (blockids[p] == 0) continue;
+        T x[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+        const T l = P.l ? P.l[p] : s.gimp_l;
+        Basis<D, Dual3> B;
+        if (!dual_basis<D, T>(MD, s, x, l, B, err)) continue;
+        const double mp = P.m ? double(P.m[p]) : double(s.mass);
+        const double Vp = double(P.V[p]);
+        double vp[3] = {}, Bp[3][3] = {}, sg[3][3] = {};
+#pragma unroll
+        for (int d = 0; d < D; ++d) vp[d] = double(P.v[d][p]);
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                sg[r][c] = double(P.sig[symidx<D>(r, c)][p]);
+                if (apic) Bp[r][c] = double(P.B[r + c * D][p]);
+            }
+        double xb[3] = {}, vbs[3] = {}, sb[3][3] = {}, Vb = 0.0, Bbs[3][3] = {};
+        for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
+            for (int j = 0; j < 3; ++j)
+                for (int i = 0; i < 3; ++i) {
+                    const int idx[3] = {i, j, k};
+                    long long I = 0;
+                    bool valid = true;
+#pragma unroll
+                    for (int d = D - 1; d >= 0; --d) {
+                        valid = valid && idx[d] < B.ax[d].cnt;
+                        I = I * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
+                    }
+                    if (!valid) continue;
+                    Dual3 rel[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(double(x[d]));
+                        rel[d].d[d] = -1.0;
+                    }
+                    Dual3 N, Gn[3];
+                    dual_node<D>(MD, B, i, j, k, rel, N, Gn);
+                    double u[3] = {};
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        u[d] = vp[d];
+                        if (apic)
+#pragma unroll
+                            for (int c = 0; c < D; ++c) u[d] += Bp[d][c] * dinv * rel[c].v;
+                    }
+                    double Nb = mp * GB.mb[I], Gb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        const double p_b = GB.pb[d][I], f_b = GB.fb[d][I];
+                        Nb += mp * (u[d] * p_b + double(s.g[d]) * f_b);
+                        const double ub = mp * N.v * p_b;
+                        vbs[d] += ub;
+                        if (apic)
+#pragma unroll
+                            for (int c = 0; c < D; ++c) {
+                                Bbs[d][c] += ub * dinv * rel[c].v;
+                                xb[c] -= ub * Bp[d][c] * dinv;
+                            }
+                    }
+#pragma unroll
+                    for (int r = 0; r < D; ++r) {
+                        const double f_b = GB.fb[r][I];
+                        double sgg = 0.0;
+#pragma unroll
+                        for (int c = 0; c < D; ++c) {
+                            sgg += sg[r][c] * Gn[c].v;
+                            Gb[c] += -Vp * sg[r][c] * f_b;
+                            sb[r][c] += -Vp * f_b * Gn[c].v;
+                        }
+                        Vb += -f_b * sgg;
+                    }
+#pragma unroll
+                    for (int b = 0; b < D; ++b) {
+                        double h = 0.0;
+#pragma unroll
+                        for (int c = 0; c < D; ++c) h += Gb[c] * Gn[c].d[b];
+                        xb[b] += Nb * N.d[b] + h;
+                    }
+                }
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            A.x[d][p] += xb[d];
+            A.v[d][p] += vbs[d];
+        }
+        if (apic) {
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) A.B[r + c * D][p] += Bbs[r][c];
+        }
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) sbar[(r * D + c) * n + p] = sb[r][c];
+        sbar[D * D * n + p] = Vb;
+    }
+}
+
 }  // namespace
 
 template <int D, class T, int BW>
@@ -926,10 +1237,61 @@ cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<
     return e;
 }
 
+template <int D, class T>
+cudaError_t launch_adjoint_general(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                                   const AdjView& A, const GradGrid& GB, const AdjPartition& part, const LaunchCfg& cfg) {
+    cudaError_t e = cudaSuccess;
+    for (int d = 0; d < D && e == cudaSuccess; ++d) {
+        e = cudaMemsetAsync(GB.vb[d], 0, sizeof(double) * size_t(M.nnodes), cfg.stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(GB.vnb[d], 0, sizeof(double) * size_t(M.nnodes), cfg.stream);
+    }
+    if (e != cudaSuccess) return e;
+    const int pgrid = int(std::max<long long>(1, std::min<long long>((P.n + 127) / 128, (long long)cfg.num_sms * 16)));
+    const int ngrid = int(std::max<long long>(1, std::min<long long>((M.nnodes + 255) / 256, (long long)cfg.num_sms * 8)));
+    if (P.n > 0) {
+        KernelScope ks(cfg, "adj_g2p");
+        adj_g2p_gen_kernel<D, T><<<pgrid, 128, 0, cfg.stream>>>(M, G, P, s, A, GB, part.blockids, cfg.err);
+        ++*cfg.launches;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    {
+        KernelScope ks(cfg, "adj_grid");
+        adj_grid_kernel<D, T><<<ngrid, 256, 0, cfg.stream>>>(M, G, s, GB);
+        ++*cfg.launches;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (P.n > 0) {
+        {
+            KernelScope ks(cfg, "adj_p2g");
+            adj_p2g_gen_kernel<D, T><<<pgrid, 128, 0, cfg.stream>>>(M, P, s, A, GB, GB.coef, part.blockids, cfg.err);
+            ++*cfg.launches;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        const int mgrid = int(std::max<long long>(1, std::min<long long>((P.n + 255) / 256, (long long)cfg.num_sms * 8)));
+        KernelScope ks(cfg, "adj_material");
+        adj_material_kernel<D, T><<<mgrid, 256, 0, cfg.stream>>>(P, s, A, GB.coef, part.blockids);
+        ++*cfg.launches;
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
 #define TB_INST_ADJ(D, T, BW)                                                                                 \
     template cudaError_t launch_adjoint<D, T, BW>(const DMesh<D, T>&, const GView<T>&, const PView<T>&,       \
                                                   const Scalars<T>&, const AdjView&, const GradGrid&,         \
                                                   const AdjPartition&, const LaunchCfg&);
+template cudaError_t launch_adjoint_general<3, double>(const DMesh<3, double>&, const GView<double>&,
+                                                      const PView<double>&, const Scalars<double>&, const AdjView&,
+                                                      const GradGrid&, const AdjPartition&, const LaunchCfg&);
+template cudaError_t launch_adjoint_general<3, float>(const DMesh<3, float>&, const GView<float>&,
+                                                     const PView<float>&, const Scalars<float>&, const AdjView&,
+                                                     const GradGrid&, const AdjPartition&, const LaunchCfg&);
+template cudaError_t launch_adjoint_general<2, double>(const DMesh<2, double>&, const GView<double>&,
+                                                      const PView<double>&, const Scalars<double>&, const AdjView&,
+                                                      const GradGrid&, const AdjPartition&, const LaunchCfg&);
+template cudaError_t launch_adjoint_general<2, float>(const DMesh<2, float>&, const GView<float>&,
+                                                     const PView<float>&, const Scalars<float>&, const AdjView&,
+                                                     const GradGrid&, const AdjPartition&, const LaunchCfg&);
 TB_INST_ADJ(3, double, 4)
 TB_INST_ADJ(3, float, 4)
 TB_INST_ADJ(2, double, 8)

@@ -65,6 +65,66 @@ __device__ __forceinline__ void group_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// Forward-mode dual number with the three derivatives with respect to a
+// particle's position: the weights evaluated in Dual3 give dN/dx_p and
+// d(grad N)/dx_p for the reverse step of every basis (WLS, KernelCorrection,
+// truncated windows) without hand-derived second derivatives. Floors and
+// comparisons act on the value, |x| follows the value's sign. In a namespace of
+// its own, so that floor, fabs and signbit of plain numbers inside tb still
+// resolve to the CUDA functions (the Dual3 overloads are found by argument-
+// dependent lookup).
+namespace ad {
+struct Dual3 {
+    double v, d[3];
+    __host__ __device__ Dual3() : v(0.0), d{0.0, 0.0, 0.0} {}
+    __host__ __device__ Dual3(double a) : v(a), d{0.0, 0.0, 0.0} {}
+    __host__ __device__ explicit operator double() const { return v; }
+    __host__ __device__ explicit operator float() const { return float(v); }
+    __host__ __device__ explicit operator int() const { return int(v); }
+    __host__ __device__ Dual3 operator-() const {
+        Dual3 r;
+        r.v = -v;
+        for (int k = 0; k < 3; ++k) r.d[k] = -d[k];
+        return r;
+    }
+    __host__ __device__ Dual3& operator+=(const Dual3& o) {
+        v += o.v;
+        for (int k = 0; k < 3; ++k) d[k] += o.d[k];
+        return *this;
+    }
+    __host__ __device__ Dual3& operator-=(const Dual3& o) {
+        v -= o.v;
+        for (int k = 0; k < 3; ++k) d[k] -= o.d[k];
+        return *this;
+    }
+    __host__ __device__ Dual3& operator*=(const Dual3& o) {
+        for (int k = 0; k < 3; ++k) d[k] = d[k] * o.v + v * o.d[k];
+        v *= o.v;
+        return *this;
+    }
+    __host__ __device__ Dual3& operator/=(const Dual3& o) {
+        const double iv = 1.0 / o.v;
+        for (int k = 0; k < 3; ++k) d[k] = (d[k] - v * iv * o.d[k]) * iv;
+        v *= iv;
+        return *this;
+    }
+};
+__host__ __device__ inline Dual3 operator+(Dual3 a, const Dual3& b) { return a += b; }
+__host__ __device__ inline Dual3 operator-(Dual3 a, const Dual3& b) { return a -= b; }
+__host__ __device__ inline Dual3 operator*(Dual3 a, const Dual3& b) { return a *= b; }
+__host__ __device__ inline Dual3 operator/(Dual3 a, const Dual3& b) { return a /= b; }
+__host__ __device__ inline bool operator<(const Dual3& a, const Dual3& b) { return a.v < b.v; }
+__host__ __device__ inline bool operator>(const Dual3& a, const Dual3& b) { return a.v > b.v; }
+__host__ __device__ inline bool operator<=(const Dual3& a, const Dual3& b) { return a.v <= b.v; }
+__host__ __device__ inline bool operator>=(const Dual3& a, const Dual3& b) { return a.v >= b.v; }
+__host__ __device__ inline bool operator==(const Dual3& a, const Dual3& b) { return a.v == b.v; }
+__host__ __device__ inline bool operator!=(const Dual3& a, const Dual3& b) { return a.v != b.v; }
+__device__ inline Dual3 floor(const Dual3& a) { return Dual3(::floor(a.v)); }
+__device__ inline Dual3 fabs(const Dual3& a) { return ::signbit(a.v) ? -a : a; }
+__device__ inline bool signbit(const Dual3& a) { return ::signbit(a.v); }
+}  // namespace ad
+using ad::Dual3;
+
 template <int D, class T>
 struct DMesh {
     int n[3];      // nodes per axis

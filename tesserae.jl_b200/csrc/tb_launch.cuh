@@ -113,6 +113,7 @@ struct AdjView {
     double* F[9];
     double* mu;
     double* lam;
+    double* B[9];  // APIC only
 };
 struct GradGrid {
     double* vb[3];   // d loss / d v_i (scattered by G2P backwards)
@@ -138,6 +139,11 @@ struct AdjPartition {
 template <int D, class T, int BW>
 cudaError_t launch_adjoint(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
                            const AdjView& A, const GradGrid& GB, const AdjPartition& part, const LaunchCfg& cfg);
+// The same for WLS / KernelCorrection bases and the APIC transfer (particle-parallel,
+// weight derivatives in Dual3).
+template <int D, class T>
+cudaError_t launch_adjoint_general(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& P, const Scalars<T>& s,
+                                   const AdjView& A, const GradGrid& GB, const AdjPartition& part, const LaunchCfg& cfg);
 
 template <int D, class T>
 cudaError_t launch_update_weights(const DMesh<D, T>& M, const PView<T>& P, const Scalars<T>& s, T* w, T* grad_w,

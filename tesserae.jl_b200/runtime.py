@@ -291,7 +291,8 @@ def rollout_grad(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     tape_forward(grid, particles, part, mesh, params, nsteps, checkpoint_every, ctx=ctx)
     loss, gx, gv = loss_grad(particles)
     lame = particles.mu is not None and particles.lam is not None
-    adj = Adjoint(n, D, backend="torch", device=particles.device or "cuda", lame=lame)
+    apic = params.transfer == _abi.TB_TRANSFER_APIC
+    adj = Adjoint(n, D, backend="torch", device=particles.device or "cuda", lame=lame, apic=apic)
     adj.x.copy_(gx)
     adj.v.copy_(gv)
     tape_backward(grid, particles, part, mesh, params, adj, ctx=ctx)
@@ -326,7 +327,8 @@ class RolloutFunction:
             @staticmethod
             def backward(fctx, gx):
                 c = ctx or _default()
-                adj = Adjoint(particles.n, particles.dim, backend="torch", device=gx.device, lame=False)
+                adj = Adjoint(particles.n, particles.dim, backend="torch", device=gx.device, lame=False,
+                              apic=params.transfer == _abi.TB_TRANSFER_APIC)
                 adj.x.copy_(gx.double())
                 tape_backward(fctx.grid, particles, fctx.part, mesh, params, adj, ctx=c)
                 return adj.v.to(v0.dtype)

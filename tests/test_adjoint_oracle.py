@@ -51,8 +51,13 @@ def test_oracle_adjoint_matches_finite_differences(tb, oracle, case):
 
 
 def test_adjoint_rejects_unsupported(tb, oracle):
+    """APIC needs the B sensitivity array; the von Mises model has no adjoint."""
     mesh, P, prm = box_scene(tb, dim=3)
     prm.transfer = tb._abi.TB_TRANSFER_APIC
     adj = tb.Adjoint(P.n, 3)
+    with pytest.raises(RuntimeError):
+        oracle.adjoint_step(mesh, P, tb.generate_grid(mesh, np.float64), prm, adj)
+    prm.transfer = tb._abi.TB_TRANSFER_FLIP
+    prm.material = tb._abi.MATERIAL_VONMISES
     with pytest.raises(RuntimeError):
         oracle.adjoint_step(mesh, P, tb.generate_grid(mesh, np.float64), prm, adj)
