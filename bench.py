@@ -536,6 +536,109 @@ def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: 
     return out
 
 
+def dambreak_adjoint_leg(tb, runtime, ctx, scale: int = 2, fd_scale: int = 4, forward: int = 80, last: int = 20,
+                         every: int = 5, fd_directions: int = 2) -> dict:
+    """The dam break's differentiable leg: `forward` steps, then the gradient of
+    L = sum c . x at the end of `last` more steps with respect to the velocity
+    field at their start (the checkpointed tape over the last steps; WLS(uGIMP)
+    + APIC + fluid take the general reverse step), mixed FP32 form, at 1/scale
+    of the resolution (the tape holds last/every states plus `every` steps of
+    state, grid and partition: 224 GB for the full 145 M-particle scene at the
+    best interval). Device times per step of the plain forward, the taped
+    forward and the backward pass; the FP64 tape's directional derivatives
+    against central differences of the FP64 device rollout at 1/fd_scale."""
+    import torch
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def setup(sc_scale, dtype):
+        sc = tb.scenes.dambreak3d(scale=sc_scale, particles=False)
+        P = _form_particles(tb, runtime, ctx, tb.scenes.dambreak3d(scale=sc_scale, particles=False), "f64"
+                            if dtype == np.float64 else "f32")
+        part = tb.Partition(sc.mesh, P.n, backend="torch", device="cuda")
+        G = tb.generate_grid(sc.mesh, dtype, backend="torch", device="cuda")
+        runtime.step(G, P, part, sc.mesh, sc.params, forward, ctx=ctx)
+        ctx.synchronize()
+        return sc, P, part, G
+
+    sc, P, part, G = setup(scale, np.float32)
+    mesh, prm, n = sc.mesh, sc.params, P.n
+    start = {k: getattr(P, k).clone() for k in P.FIELDS if getattr(P, k) is not None}
+
+    def restore():
+        for k, v in start.items():
+            getattr(P, k).copy_(v)
+
+    fwd_ms = timed(lambda: runtime.step(G, P, part, mesh, prm, last, ctx=ctx))
+    restore()
+    tape_ms = timed(lambda: runtime.tape_forward(G, P, part, mesh, prm, last, every, ctx=ctx))
+    rng = np.random.default_rng(31)
+    cw = torch.from_numpy(rng.normal(size=(3, n))).cuda()
+    adj = tb.Adjoint(n, 3, backend="torch", device="cuda", lame=False, apic=True)
+    adj.x.copy_(cw)
+    bwd_ms = timed(lambda: runtime.tape_backward(G, P, part, mesh, prm, adj, ctx=ctx))
+    ctx.profile(True)
+    restore()
+    runtime.tape_forward(G, P, part, mesh, prm, every, every, ctx=ctx)
+    ctx.profile_read()
+    a2 = tb.Adjoint(n, 3, backend="torch", device="cuda", lame=False, apic=True)
+    a2.x.copy_(cw)
+    runtime.tape_backward(G, P, part, mesh, prm, a2, ctx=ctx)
+    kt = ctx.profile_read()
+    ctx.profile(False)
+    gnorm = float(adj.v.norm())
+    del P, part, G, start, adj, a2
+    torch.cuda.empty_cache()
+
+    # FP64 tape against central differences of the FP64 rollout, at 1/fd_scale
+    sc, P, part, G = setup(fd_scale, np.float64)
+    n2 = P.n
+    start = {k: getattr(P, k).clone() for k in P.FIELDS if getattr(P, k) is not None}
+    cw2 = torch.from_numpy(rng.normal(size=(3, n2))).cuda()
+
+    def restore2():
+        for k, v in start.items():
+            getattr(P, k).copy_(v)
+
+    runtime.tape_forward(G, P, part, sc.mesh, sc.params, last, every, ctx=ctx)
+    adj = tb.Adjoint(n2, 3, backend="torch", device="cuda", lame=False, apic=True)
+    adj.x.copy_(cw2)
+    runtime.tape_backward(G, P, part, sc.mesh, sc.params, adj, ctx=ctx)
+    gv = adj.v.clone()
+    checks = []
+    for _ in range(fd_directions):
+        d = torch.from_numpy(rng.normal(size=(3, n2))).cuda()
+        eps = 1e-6
+        Ls = []
+        for sgn in (1.0, -1.0):
+            restore2()
+            P.v.add_(sgn * eps * d)
+            runtime.step(G, P, part, sc.mesh, sc.params, last, ctx=ctx)
+            ctx.synchronize()
+            Ls.append(float((cw2 * P.x).sum()))
+        fd = (Ls[0] - Ls[1]) / (2 * eps)
+        ad = float((gv * d).sum())
+        checks.append({"fd": fd, "adjoint": ad, "rel_err": abs(ad - fd) / max(abs(fd), 1e-30)})
+    del P, part, G, start, adj
+    torch.cuda.empty_cache()
+    return {"workload": f"dambreak3d at 1/{scale} resolution ({n} particles): {forward} steps, then the gradient of "
+                        f"sum c . x after {last} more steps w.r.t. the velocities at their start; tape every {every}",
+            "n_particles": n, "forward_ms_per_step": fwd_ms / last, "tape_forward_ms_per_step": tape_ms / last,
+            "backward_ms_per_step": bwd_ms / last, "backward_over_forward": bwd_ms / fwd_ms,
+            "value": (tape_ms + bwd_ms) / fwd_ms, "grad_v_norm": gnorm,
+            "backward_kernels_ms_per_step": {k: v[1] / every for k, v in sorted(kt.items())},
+            "fd_check": {"scale": fd_scale, "n_particles": n2, "against": "central differences (eps 1e-6) of the "
+                         "FP64 device rollout, FP64 tape", "max_rel_err": max(c["rel_err"] for c in checks),
+                         "directions": checks}}
+
+
 def fullsize_oracle_check(tb, runtime, ctx, sc, nsteps: int = 3) -> dict:
     """The plain FP64 device step against the FP64 oracle (the OpenMP
     restatement of the reference's CPU step) on the full headline scene,
@@ -808,6 +911,8 @@ def main():
                                         acc_steps=csc.nsteps, peak=peak, apic=True)
             configs[cname]["workload"] = ("dambreak3d: 384^3 cells, column [0,0.4]x[0,1]x[0,0.8] at 2^3 per cell, "
                                           "WLS(uGIMP) + APIC, fluid K=2e6, slip walls, dt=2.5e-5; block order")
+            if not args.no_adjoint:
+                configs[cname]["adjoint_last_20"] = dambreak_adjoint_leg(tb, runtime, ctx)
         else:
             raise SystemExit(f"unknown config {cname}")
 
