@@ -1447,7 +1447,9 @@ __global__ void __launch_bounds__(WS_THREADS, 2)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* recbuf = reinterpret_cast<float*>(smem_raw);  // [2][RECW]
     float* part = recbuf + 2 * RECW;
-    WsShared& sh = *reinterpret_cast<WsShared*>(part + NC * CSTR);
+    // the mbarriers (8-byte words) start on a 16-byte boundary
+    constexpr size_t SH_OFF = ((sizeof(float) * size_t(2 * RECW + NC * CSTR) + 15) / 16) * 16;
+    WsShared& sh = *reinterpret_cast<WsShared*>(smem_raw + SH_OFF);
 
     const int tid = threadIdx.x;
     const bool producer = tid < NP;
@@ -1727,7 +1729,8 @@ __global__ void __launch_bounds__(WS_THREADS, 2)
 
 size_t ws_smem_bytes() {
     using SH = PencilShape<3, 4>;
-    return sizeof(float) * (2 * (size_t(PLANE_NR) * CRS + 2 * SH::NPENCIL) + SH::NPART) + sizeof(WsShared);
+    const size_t words = sizeof(float) * (2 * (size_t(PLANE_NR) * CRS + 2 * SH::NPENCIL) + SH::NPART);
+    return ((words + 15) / 16) * 16 + sizeof(WsShared);
 }
 
 template <bool X64>
