@@ -2199,7 +2199,7 @@ cudaError_t launch_pencil(const DMesh<D, T>& M, const PView<T>& P, const GView<T
         if (s.basis == TB_BSPLINE_QUADRATIC || s.basis == TB_KC_BSPLINE_QUADRATIC) {
             cudaError_t e = cudaMemsetAsync(b.partials, 0, sizeof(unsigned long long), cfg.stream);
             if (e != cudaSuccess) return e;
-            if constexpr (D == 3 && BW == 4) e = launch_ws<X64>(M, P, G, s, b, cfg);
+            if constexpr (D == 3 && BW == 4) e = launch_plane<X64>(M, P, G, s, b, cfg);
             else e = launch_pencil_mode<D, T, BW, X64, 1>(M, P, G, s, b, cfg);
             if (e != cudaSuccess) return e;
             return launch_pencil_mode<D, T, BW, X64, 2>(M, P, G, s, b, cfg);
