@@ -326,13 +326,16 @@ def taylor_leg(tb, runtime, ctx, steps: int = 200, warmup: int = 5, cpu_steps: i
     return out
 
 
-def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions: int = 2) -> dict:
+def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions: int = 32) -> dict:
     """Differentiable rollout on the sphere scene (64^3 cells, ~1.9M particles,
-    200 steps, checkpoint every 20), mixed FP32 form with FP32 positions (the
-    form the tape runs): device time of the plain forward rollout, the taped
-    forward and the backward pass for the centre-of-mass loss, plus directional
-    derivatives of a linear loss on the final positions, from the FP64 tape and
-    from the FP32 tape, against central differences of the FP64 device rollout."""
+    200 steps), mixed FP32 form with FP32 positions (the form the tape runs):
+    device time of the plain forward rollout, the taped forward and the backward
+    pass for the centre-of-mass loss, with the whole tape held in HBM (every
+    step's state, grid and partition: the backward pass runs the adjoint kernels
+    only) and with checkpoints every `every` steps (the backward pass re-runs
+    each segment); plus directional derivatives of a linear loss on the final
+    positions along `fd_directions` random directions per field, from the FP64
+    and the FP32 tape, against central differences of the FP64 device rollout."""
     import torch
     sc = tb.scenes.sphere3d(scale=scale)
     mesh, prm, host = sc.mesh, sc.params, sc.particles
@@ -351,35 +354,49 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
 
     P = host.to("torch", device="cuda", dtype=np.float32)
     runtime.step(G32, P, part, mesh, prm, 3, ctx=ctx)  # warm-up
-    # warm-up of the tape: its checkpoint and segment buffers are allocated once
-    # per context (grow-only) on the first call, outside the timed region
-    P = host.to("torch", device="cuda", dtype=np.float32)
-    runtime.tape_forward(G32, P, part, mesh, prm, 2 * every, every, ctx=ctx)
-    adj_w = tb.Adjoint(n, 3, backend="torch", device="cuda")
-    runtime.tape_backward(G32, P, part, mesh, prm, adj_w, ctx=ctx)
-    del adj_w
     P = host.to("torch", device="cuda", dtype=np.float32)
     fwd_ms = timed(lambda: runtime.step(G32, P, part, mesh, prm, nsteps, ctx=ctx))
-    P = host.to("torch", device="cuda", dtype=np.float32)
-    tape_ms = timed(lambda: runtime.tape_forward(G32, P, part, mesh, prm, nsteps, every, ctx=ctx))
     c = torch.tensor(sc.meta["target"], dtype=torch.float64, device="cuda")[:, None]
-    r = P.x.double().mean(dim=1, keepdim=True) - c
-    loss = float((r ** 2).sum())
-    adj = tb.Adjoint(n, 3, backend="torch", device="cuda")
-    adj.x.copy_((2 * r / n).expand(-1, n))
-    bwd_ms = timed(lambda: runtime.tape_backward(G32, P, part, mesh, prm, adj, ctx=ctx))
+
+    def tape_run(k):
+        # warm-up of the tape: its buffers are allocated once per context
+        # (grow-only) on the first call, outside the timed region
+        Q = host.to("torch", device="cuda", dtype=np.float32)
+        runtime.tape_forward(G32, Q, part, mesh, prm, nsteps, k, ctx=ctx)
+        adj_w = tb.Adjoint(n, 3, backend="torch", device="cuda")
+        runtime.tape_backward(G32, Q, part, mesh, prm, adj_w, ctx=ctx)
+        del adj_w, Q
+        Q = host.to("torch", device="cuda", dtype=np.float32)
+        tape_ms = timed(lambda: runtime.tape_forward(G32, Q, part, mesh, prm, nsteps, k, ctx=ctx))
+        r = Q.x.double().mean(dim=1, keepdim=True) - c
+        loss = float((r ** 2).sum())
+        adj = tb.Adjoint(n, 3, backend="torch", device="cuda")
+        adj.x.copy_((2 * r / n).expand(-1, n))
+        bwd_ms = timed(lambda: runtime.tape_backward(G32, Q, part, mesh, prm, adj, ctx=ctx))
+        return Q, adj, loss, tape_ms, bwd_ms
+
+    # the whole tape first (timed), then the checkpointed one, whose backward is
+    # also split per kernel
+    P, adj, loss, tape_ms, bwd_ms = tape_run(1)
     glogE = adj.mu * P.mu.double() + adj.lam * P.lam.double()
     gnorm_v, gnorm_logE = float(adj.v.norm()), float(glogE.norm())
-    # per-kernel split of one backward segment
+    ctx.profile(True)
+    runtime.tape_backward(G32, P, part, mesh, prm, adj, ctx=ctx)
+    kt_full = ctx.profile_read()
+    ctx.profile(False)
+    ctx.release_tape()
+    del adj
+    P, adj, _, tape_ck_ms, bwd_ck_ms = tape_run(every)
     ctx.profile(True)
     runtime.tape_forward(G32, P, part, mesh, prm, every, every, ctx=ctx)
     ctx.profile_read()
     runtime.tape_backward(G32, P, part, mesh, prm, adj, ctx=ctx)
     kt = ctx.profile_read()
     ctx.profile(False)
+    del adj
 
     # finite-difference check: L = sum c . x_T with random c, gradients from the
-    # FP64 tape (the check of the adjoint itself) and from the FP32 tape timed above
+    # FP64 tape (the check of the adjoint itself) and from the FP32 tape
     rng = np.random.default_rng(17)
     cw = rng.normal(size=(3, n))
     G64 = tb.generate_grid(mesh, np.float64, backend="torch", device="cuda")
@@ -393,6 +410,7 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
         return adj_c.numpy()
 
     gs = {"f64": grads(np.float64, G64), "f32": grads(np.float32, G32)}
+    ctx.release_tape()
 
     def loss64(Q):
         Qd = Q.to("torch", device="cuda")
@@ -421,24 +439,31 @@ def adjoint_leg(tb, runtime, ctx, scale: int = 1, every: int = 20, fd_directions
                            "rel_err_f32": abs(ad["f32"] - fd) / max(abs(fd), 1e-30)})
     del G64, P
     torch.cuda.empty_cache()
+    adj_ms = sum(v[1] for k, v in kt.items() if k.startswith("adj_")) / every
     return {
         "value": (tape_ms + bwd_ms) / fwd_ms,
         "backward_over_forward": bwd_ms / fwd_ms,
-        "workload": f"sphere3d: 64^3 cells, sphere r=0.3, {n} particles, {nsteps} steps, checkpoint every "
-                    f"{every}, mixed FP32 form; loss = |x_com - (0.5, 0.5, 0.8)|^2",
-        "n_particles": n, "steps": nsteps, "checkpoint_every": every, "loss": loss,
+        "workload": f"sphere3d: 64^3 cells, sphere r=0.3, {n} particles, {nsteps} steps, whole tape in HBM "
+                    f"(checkpointed every {every} beside it), mixed FP32 form; loss = |x_com - (0.5, 0.5, 0.8)|^2",
+        "n_particles": n, "steps": nsteps, "loss": loss,
         "forward_ms_per_step": fwd_ms / nsteps, "tape_forward_ms_per_step": tape_ms / nsteps,
         "backward_ms_per_step": bwd_ms / nsteps,
+        "tape_bytes_per_step": runtime.tape_slot_bytes(mesh, n, np.float32),
         "grad_v0_norm": gnorm_v, "grad_logE_norm": gnorm_logE,
-        "backward_kernels_ms_per_step": {k: v[1] / every for k, v in sorted(kt.items())},
-        # the backward step's two parts: the forward recomputed from the last
-        # checkpoint (binning, P2G, grid, G2P kernels) and the adjoint kernels
-        "backward_split": {
-            "recompute_ms_per_step": sum(v[1] for k, v in kt.items() if not k.startswith("adj_")) / every,
-            "adjoint_kernels_ms_per_step": sum(v[1] for k, v in kt.items() if k.startswith("adj_")) / every,
-            "adjoint_kernels_over_forward": sum(v[1] for k, v in kt.items() if k.startswith("adj_")) / every
-                                            / (fwd_ms / nsteps)},
+        "backward_kernels_ms_per_step": {k: v[1] / nsteps for k, v in sorted(kt_full.items())},
+        "checkpointed": {
+            "checkpoint_every": every,
+            "value": (tape_ck_ms + bwd_ck_ms) / fwd_ms,
+            "backward_over_forward": bwd_ck_ms / fwd_ms,
+            "tape_forward_ms_per_step": tape_ck_ms / nsteps, "backward_ms_per_step": bwd_ck_ms / nsteps,
+            # the backward step's two parts: the forward recomputed from the last
+            # checkpoint (binning, P2G, grid, G2P kernels) and the adjoint kernels
+            "backward_split": {
+                "recompute_ms_per_step": sum(v[1] for k, v in kt.items() if not k.startswith("adj_")) / every,
+                "adjoint_kernels_ms_per_step": adj_ms,
+                "adjoint_kernels_over_forward": adj_ms / (fwd_ms / nsteps)}},
         "fd_check": {"against": "central differences of the FP64 device rollout, L = sum c . x_T, random c",
+                     "directions_per_field": fd_directions,
                      "max_rel_err": max(ch["rel_err_f64"] for ch in checks),
                      "max_rel_err_fp32_tape": max(ch["rel_err_f32"] for ch in checks), "directions": checks},
     }

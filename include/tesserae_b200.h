@@ -355,7 +355,9 @@ int32_t tb_adjoint_step_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* part
  * steps); for each segment of K steps it restores the checkpoint, re-runs the
  * segment keeping every step's input state, grid and partition, and steps
  * backwards through it, so the device memory held is nsteps/K particle states
- * plus K (state + grid + partition) slots. `particles` is the working state
+ * plus K (state + grid + partition) slots. With K = 1 the forward pass keeps
+ * every step's (state + grid + partition) slot instead (nsteps slots) and the
+ * backward pass runs no forward step at all. `particles` is the working state
  * and holds the step-0 state again on return; the backward pass uses its own
  * grids and partitions (`partition` and `grid` are not touched). It must
  * follow the forward pass on the same context with the same particle count,
@@ -368,6 +370,17 @@ int32_t tb_tape_backward_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* par
                              tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
 int32_t tb_tape_backward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                              tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+/* Device bytes a tape of `nsteps` steps over `n` particles holds (forward and
+ * backward pass together) for element size `elem` (4 or 8; F is FP64 in both),
+ * with the APIC matrix B when `apic` != 0, checkpointed every
+ * `checkpoint_every` steps (1: the whole tape). Pure arithmetic, no device call:
+ * lets a caller pick the interval against its free device memory. Returns -1 on
+ * invalid arguments. */
+int64_t tb_tape_bytes(const tb_mesh* mesh, int64_t n, int32_t elem, int32_t apic, int32_t nsteps,
+                      int32_t checkpoint_every);
+/* Frees the context's tape buffers (the next tb_tape_forward_* allocates them
+ * again); the tape is invalid afterwards. Synchronises the context's stream. */
+int32_t tb_tape_release(tb_ctx* ctx);
 
 /* ---- binning without allocation ---------------------------------------
  * No counterpart in the reference: Tesserae.jl always allocates its partition

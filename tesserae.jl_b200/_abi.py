@@ -129,6 +129,8 @@ SIGNATURES = [
     ("tb_profile_read", I32, [VP, P(tb_kernel_time), I32, P(I32)]),
     ("tb_bin_particles_noalloc", I32, [P(tb_mesh), P(tb_particles), I32, P(tb_partition), VP, P(I64), P(I64),
                                        C.c_char_p, I32]),
+    ("tb_tape_bytes", I64, [P(tb_mesh), I64, I32, I32, I32, I32]),
+    ("tb_tape_release", I32, [VP]),
 ]
 for _p in ("f64", "f32"):
     SIGNATURES += [

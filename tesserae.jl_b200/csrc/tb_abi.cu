@@ -1079,6 +1079,31 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     const bool apic = prm->transfer == TB_TRANSFER_APIC;
     if ((rc = make_pview<T>(c, p, D, true, apic, P)) != TB_OK) return rc;
     c->tape_valid = false;
+    if (every == 1) {
+        // every step kept whole: its input state, grid and partition (the slots
+        // the backward pass of a checkpointed tape rebuilds per segment), so the
+        // backward pass runs the adjoint kernels only
+        long long nn = 1;
+        for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
+        const long long nb = mesh_nblocks(m);
+        const size_t slot = slot_bytes<T>(D, p->n, nn, nb, apic);
+        const long long nslot = std::max(nsteps, 1);
+        cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(nslot * slot));
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape");
+        for (long long j = 0; j < nslot; ++j) {
+            char* base = c->tape_cp + j * slot;
+            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_grid gj;
+            tb_partition pj;
+            int* tj;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
+            if ((rc = copy_state<T>(c, &sj, p, D, apic)) != TB_OK) return rc;
+            if (j >= nsteps) continue;
+            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, true)) != TB_OK) return rc;
+            e = cudaMemcpyAsync(tj, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
+            if (e != cudaSuccess) return cuda_fail(c, e, "tape totals copy");
+        }
+    } else {
     const long long ncp = nsteps > 0 ? (nsteps + every - 1) / every : 1;
     const size_t sb = state_bytes<T>(D, p->n, apic);
     cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(ncp * sb));
@@ -1089,6 +1114,7 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
         const int steps = std::min<long long>(every, nsteps - k * every);
         if (steps > 0 && (rc = dispatch_step<T>(c, m, p, part, g, prm, steps, true, true, true, true)) != TB_OK)
             return rc;
+    }
     }
     c->tape_valid = true;
     c->tape_n = p->n;
@@ -1119,6 +1145,19 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
     for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
     const long long nb = mesh_nblocks(m);
     const size_t sb = state_bytes<T>(D, p->n, apic), slot = slot_bytes<T>(D, p->n, nn, nb, apic);
+    if (K == 1) {  // the whole tape: the adjoint steps read the slots the forward kept
+        for (long long j = nsteps - 1; j >= 0; --j) {
+            char* base = c->tape_cp + j * slot;
+            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_grid gj;
+            tb_partition pj;
+            int* tj;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
+            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj)) != TB_OK) return rc;
+        }
+        tb_particles s0 = snapshot_view<T>(p, D, c->tape_cp, apic);
+        return copy_state<T>(c, p, &s0, D, apic);
+    }
     cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * slot));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape segment");
     const long long ncp = nsteps > 0 ? (nsteps + K - 1) / K : 1;
@@ -1418,6 +1457,39 @@ int32_t tb_tape_backward_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_pa
 int32_t tb_tape_backward_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
                              const tb_step_params* prm, tb_adjoint* adj) {
     return do_tape_backward<float>(c, m, p, part, g, prm, adj);
+}
+
+int64_t tb_tape_bytes(const tb_mesh* m, int64_t n, int32_t elem, int32_t apic, int32_t nsteps,
+                      int32_t checkpoint_every) {
+    if (!m || (m->dim != 2 && m->dim != 3) || n < 0 || (elem != 4 && elem != 8) || nsteps < 0 ||
+        checkpoint_every < 1)
+        return -1;
+    const int D = m->dim;
+    long long nn = 1;
+    for (int d = 0; d < D; ++d) {
+        if (m->n_nodes[d] < 1) return -1;
+        nn *= m->n_nodes[d];
+    }
+    const long long nb = mesh_nblocks(m);
+    const bool ap = apic != 0;
+    const size_t sb = elem == 4 ? state_bytes<float>(D, n, ap) : state_bytes<double>(D, n, ap);
+    const size_t slot = elem == 4 ? slot_bytes<float>(D, n, nn, nb, ap) : slot_bytes<double>(D, n, nn, nb, ap);
+    if (checkpoint_every == 1) return (int64_t)(std::max(nsteps, 1) * slot);
+    const long long ncp = nsteps > 0 ? (nsteps + checkpoint_every - 1) / checkpoint_every : 1;
+    return (int64_t)(ncp * sb + (long long)checkpoint_every * slot);
+}
+
+int32_t tb_tape_release(tb_ctx* c) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamSynchronize");
+    cudaFree(c->tape_cp);
+    cudaFree(c->tape_seg);
+    c->tape_cp = c->tape_seg = nullptr;
+    c->tape_cp_cap = c->tape_seg_cap = 0;
+    c->tape_valid = false;
+    return TB_OK;
 }
 
 }  // extern "C"

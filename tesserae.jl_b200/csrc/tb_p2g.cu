@@ -1341,7 +1341,7 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
                 for (int gx = 0; gx < G1 + 2; ++gx) {
                     if (gx < G1) {
                         const int qe = gstart[gbase + gx + 1];
-#pragma unroll 2
+#pragma unroll 1
                         for (int q = qs; q < qe; ++q) {
                             PairRec r0;
                             load_pair_rec(prec + q * CRS, r0);

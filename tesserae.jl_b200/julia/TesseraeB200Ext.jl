@@ -625,16 +625,27 @@ function b200_step!(grid, particles, partition, prm::TbParams, nsteps::Integer)
 end
 
 """
-    xT = b200_rollout(v0, particles, grid, partition, params, nsteps; checkpoint_every=20)
+    xT = b200_rollout(v0, particles, grid, partition, params, nsteps; checkpoint_every=nothing)
 
 Final positions (a dim x n Float64 matrix) of a rollout from the initial
 velocities `v0` (dim x n). Differentiable: the `rrule` below runs the
 checkpointed tape (`tb_tape_forward_*`) forward and `tb_tape_backward_*` in the
 pullback, giving d loss / d v0 (the Julia counterpart of the torch
-autograd.Function of the Python host mirror).
+autograd.Function of the Python host mirror). `checkpoint_every = nothing`
+keeps the whole tape (interval 1: the pullback runs no forward step) when
+`tb_tape_bytes` says it takes at most 60% of the device's free memory, else
+checkpoints every 20 steps.
 """
 function b200_rollout(v0::CuMatrix, particles, grid, partition, prm::TbParams, nsteps::Integer;
-                      checkpoint_every::Integer=20)
+                      checkpoint_every::Union{Integer,Nothing}=nothing)
+    if checkpoint_every === nothing
+        elem = form(particles) === :f64 ? 8 : 4
+        bytes = GC.@preserve grid ccall((:tb_tape_bytes, libtb), Int64,
+                                        (Ref{TbMesh}, Int64, Int32, Int32, Int32, Int32),
+                                        tbmesh(grid.x), length(particles), Int32(elem),
+                                        Int32(prm.transfer == TB_TRANSFER_APIC), Int32(nsteps), Int32(1))
+        checkpoint_every = 0 <= bytes <= 0.6 * CUDA.available_memory() ? 1 : 20
+    end
     setv!(particles, v0)
     pd, gd = tbparticles(particles), tbgrid(grid)
     GC.@preserve grid particles partition begin
@@ -659,7 +670,7 @@ function setv!(particles, v0)
 end
 
 function ChainRulesCore.rrule(::typeof(b200_rollout), v0, particles, grid, partition, prm, nsteps;
-                              checkpoint_every=20)
+                              checkpoint_every=nothing)
     xT = b200_rollout(v0, particles, grid, partition, prm, nsteps; checkpoint_every)
     function pullback(x̄)
         dim, n = size(xT)

@@ -86,6 +86,10 @@ class Context:
         self.check(self.lib.tb_profile_read(self.ptr, buf, cap, C.byref(cnt)), "tb_profile_read")
         return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].ms)) for i in range(min(cnt.value, cap))}
 
+    def release_tape(self):
+        """Free this context's tape buffers (the next tape_forward allocates again)."""
+        self.check(self.lib.tb_tape_release(self.ptr), "tb_tape_release")
+
     def fn(self, name: str, dtype):
         return getattr(self.lib, f"{name}_{_suffix(dtype)}")
 
@@ -251,9 +255,37 @@ def adjoint_step(grid: Grid, particles: Particles, partition: Partition, mesh: C
     ctx.check(rc, "adjoint_step")
 
 
+def tape_bytes(mesh: CartesianMesh, n: int, dtype, nsteps: int, checkpoint_every: int, apic: bool = False) -> int:
+    """Device bytes a tape holds (forward and backward pass) for `n` particles of
+    element type `dtype` over `nsteps` steps, checkpointed every
+    `checkpoint_every` steps (1: the whole tape, no recompute in the backward)."""
+    lib = _abi.load_library()
+    b = int(lib.tb_tape_bytes(C.byref(mesh.struct()), int(n), int(np.dtype(dtype).itemsize), int(bool(apic)),
+                              int(nsteps), int(checkpoint_every)))
+    if b < 0:
+        raise ValueError("tape_bytes: invalid arguments")
+    return b
+
+
+def tape_slot_bytes(mesh: CartesianMesh, n: int, dtype, apic: bool = False) -> int:
+    """Device bytes one step of the whole tape holds (state, grid, partition)."""
+    return tape_bytes(mesh, n, dtype, 1, 1, apic)
+
+
+def choose_checkpoint_every(mesh: CartesianMesh, n: int, dtype, nsteps: int, apic: bool = False,
+                            device=None, budget: float = 0.6, fallback: int = 20) -> int:
+    """1 (the whole tape in device memory) when it takes at most `budget` of the
+    device's free memory, else `fallback`."""
+    import torch
+    free, _ = torch.cuda.mem_get_info(device)
+    return 1 if tape_bytes(mesh, n, dtype, nsteps, 1, apic) <= budget * free else fallback
+
+
 def tape_forward(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
                  nsteps: int, checkpoint_every: int = 20, ctx: Context | None = None):
-    """Advance `nsteps` steps (as `step`) keeping checkpoints every `checkpoint_every` steps."""
+    """Advance `nsteps` steps (as `step`) keeping checkpoints every
+    `checkpoint_every` steps; 1 keeps every step's state, grid and partition (the
+    whole tape), so tape_backward runs no forward step."""
     ctx = ctx or _default()
     rc = ctx.pfn("tb_tape_forward", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
@@ -273,7 +305,7 @@ def tape_backward(grid: Grid, particles: Particles, partition: Partition, mesh: 
 
 
 def rollout_grad(particles: Particles, mesh: CartesianMesh, params, nsteps: int, loss_grad,
-                 checkpoint_every: int = 20, nu: float | None = None, ctx: Context | None = None):
+                 checkpoint_every: int | None = None, nu: float | None = None, ctx: Context | None = None):
     """Gradients of a rollout loss with respect to the initial velocities and the
     per-particle log Young's modulus.
 
@@ -282,10 +314,14 @@ def rollout_grad(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     shape (dim, n)). With per-particle Lame arrays (particles.mu / particles.lam)
     and E entering both as mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)),
     dL/dlogE = mu dL/dmu + lambda dL/dlambda. `particles` is left in its initial
-    state. Returns (loss, dL/dv0, dL/dlogE or None)."""
+    state. `checkpoint_every` None: the whole tape when it fits in device memory
+    (choose_checkpoint_every). Returns (loss, dL/dv0, dL/dlogE or None)."""
     import torch
     ctx = ctx or _default()
     D, n = particles.dim, particles.n
+    if checkpoint_every is None:
+        checkpoint_every = choose_checkpoint_every(mesh, n, particles.dtype, nsteps,
+                                                   params.transfer == _abi.TB_TRANSFER_APIC, particles.device)
     part = Partition(mesh, n, backend="torch", device=particles.device or "cuda")
     grid = Grid(mesh, particles.dtype, backend="torch", device=particles.device or "cuda")
     tape_forward(grid, particles, part, mesh, params, nsteps, checkpoint_every, ctx=ctx)
@@ -309,9 +345,12 @@ class RolloutFunction:
     adjoint tape. The counterpart of a ChainRulesCore rrule on the Julia side."""
 
     @staticmethod
-    def apply(v0, particles: Particles, mesh: CartesianMesh, params, nsteps: int, checkpoint_every: int = 20,
+    def apply(v0, particles: Particles, mesh: CartesianMesh, params, nsteps: int, checkpoint_every: int | None = None,
               ctx: Context | None = None):
         import torch
+        if checkpoint_every is None:
+            checkpoint_every = choose_checkpoint_every(mesh, particles.n, particles.dtype, nsteps,
+                                                       params.transfer == _abi.TB_TRANSFER_APIC, v0.device)
 
         class _F(torch.autograd.Function):
             @staticmethod

@@ -5,6 +5,8 @@ import pathlib
 import re
 import subprocess
 
+import pytest
+
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 
@@ -57,3 +59,22 @@ def test_struct_sizes_match_header(tb):
     a = tb._abi
     assert sizes == [ctypes.sizeof(s) for s in (a.tb_mesh, a.tb_particles, a.tb_grid, a.tb_partition,
                                                 a.tb_weights, a.tb_step_params)]
+
+
+def test_tape_bytes_arithmetic():
+    """tb_tape_bytes (no device call): the whole tape is nsteps slots; a
+    checkpointed tape is its checkpoints plus one segment of slots."""
+    import numpy as np
+    import tesserae_b200 as tb
+    from tesserae_b200 import runtime
+    mesh = tb.CartesianMesh(1 / 16, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    n = 1000
+    slot = runtime.tape_slot_bytes(mesh, n, np.float32)
+    assert slot > n * (13 * 4 + 9 * 8)
+    assert runtime.tape_bytes(mesh, n, np.float32, 50, 1) == 50 * slot
+    ck = runtime.tape_bytes(mesh, n, np.float32, 50, 10)
+    assert slot * 10 < ck < 50 * slot
+    assert runtime.tape_bytes(mesh, n, np.float64, 50, 1) > 50 * slot
+    assert runtime.tape_bytes(mesh, n, np.float32, 50, 1, apic=True) > 50 * slot
+    with pytest.raises(ValueError):
+        runtime.tape_bytes(mesh, n, np.float32, 50, 0)

@@ -99,10 +99,11 @@ def tape_grad(tb, ctx, mesh, P, prm, nsteps, every, seeds):
     return adj.numpy(), final, restored
 
 
+@pytest.mark.parametrize("every", [3, 1])  # 1: the whole tape, no recompute in the backward pass
 @pytest.mark.parametrize("case", ["bspline3d", "ugimp", "walls", "bspline2d"])
-def test_tape_matches_oracle_rollout_grad(tb, oracle, ctx, case):
+def test_tape_matches_oracle_rollout_grad(tb, oracle, ctx, case, every):
     mesh, P, prm = box_scene(tb, **CASES[case])
-    nsteps, every = 7, 3
+    nsteps = 7
     seeds = random_seeds(P, np.random.default_rng(5))
     got, final, restored = tape_grad(tb, ctx, mesh, P, prm, nsteps, every, seeds)
     ref, final_o = oracle_rollout_grad(tb, oracle, mesh, P, prm, nsteps, seeds)

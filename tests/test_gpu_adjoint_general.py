@@ -43,8 +43,9 @@ def test_general_adjoint_step_matches_oracle(tb, oracle, ctx, case, dtype, tol):
         assert err <= tol, (case, k, err)
 
 
+@pytest.mark.parametrize("every", [2, 1])  # 1: the whole tape
 @pytest.mark.parametrize("case", ["dambreak_set", "apic_bspline", "wls_bspline"])
-def test_general_tape_matches_oracle_rollout(tb, oracle, ctx, case):
+def test_general_tape_matches_oracle_rollout(tb, oracle, ctx, case, every):
     from tesserae_b200 import runtime
     mesh, P, prm = scene(tb, **CASES[case])
     apic = prm.transfer == 1
@@ -54,7 +55,7 @@ def test_general_tape_matches_oracle_rollout(tb, oracle, ctx, case):
     Pd = P.to("torch", device="cuda")
     part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
     G = tb.generate_grid(mesh, np.float64, backend="torch", device="cuda")
-    runtime.tape_forward(G, Pd, part, mesh, prm, nsteps, 2, ctx=ctx)
+    runtime.tape_forward(G, Pd, part, mesh, prm, nsteps, every, ctx=ctx)
     ctx.synchronize()
     assert rel_l2(Pd.x.cpu().numpy(), final.x) <= 1e-12
     adj_d = tb.Adjoint(P.n, P.dim, backend="torch", device="cuda", apic=apic)
