@@ -16,8 +16,9 @@
  *   _f32  "mixed": every array is float EXCEPT the deformation gradient F,
  *         which stays double; weights, P2G and G2P run in FP32 (each P2G lane
  *         sums its particles' contributions to a node in plain FP32 registers;
- *         the few partial sums that reach a node are added in FP64 before the
- *         one global atomic per node), and F update, det F and log J run in
+ *         the at most 9 partial sums that reach a node are added, in FP32 on
+ *         the 3D paths and in FP64 on the 2D and boundary-block ones, before
+ *         the one global atomic per node), and F update, det F and log J run in
  *         FP64. Drop-in for `gpu` (Float32-cast) data plus an FP64 F array.
  *
  * Index conventions follow the reference (Julia, column-major, 1-based):

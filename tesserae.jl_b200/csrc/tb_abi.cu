@@ -304,7 +304,6 @@ int check_device_status(tb_ctx* c) {
         if (h & ERR_TILE_RANGE) why += " support window outside its block tile;";
         if (h & ERR_GIMP_LENGTH) why += " uGIMP requires 0 <= l <= spacing(mesh);";
         if (h & ERR_WLS_SINGULAR) why += " singular WLS moment matrix;";
-        if (h & ERR_WAIT_LIMIT) why += " a bounded wait inside a kernel gave up (results incomplete);";
         if (h & ERR_REORDER_OUTSIDE)
             why += " reorder_particles!: some particles are outside the mesh and were not assigned to any block;";
         return fail(c, TB_ERR_DEVICE, "kernel reported:%s", why.c_str());

@@ -23,46 +23,22 @@ enum : int {
     ERR_TILE_RANGE = 1,   // a support window left its block tile
     ERR_GIMP_LENGTH = 2,  // uGIMP requires 0 <= l <= h (gimp.jl:22)
     ERR_WLS_SINGULAR = 4,  // WLS moment matrix not invertible
-    ERR_REORDER_OUTSIDE = 8,  // a reorder was due but particles lie outside the mesh
-    ERR_WAIT_LIMIT = 16       // a bounded wait on an mbarrier gave up (the kernel stopped early)
+    ERR_REORDER_OUTSIDE = 8   // a reorder was due but particles lie outside the mesh
 };
 
-// ---- mbarriers with bounded waits (shared memory, CTA scope) ---------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-// arrive with release semantics: this thread's shared-memory writes before it are
-// visible to a thread that observes the phase completion
-__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Wait for the phase with the given parity to complete, at most `limit` tries
-// (each try may suspend the thread for a hardware-chosen time); on giving up
-// sets ERR_WAIT_LIMIT and returns false so the caller can stop.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* err,
-                                          int limit = 1 << 22) {
-    for (int i = 0; i < limit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    atomicOr(err, ERR_WAIT_LIMIT);
-    return false;
-}
-// Barrier of the `count` threads of a warp group (named hardware barrier `id`, 1..15).
-__device__ __forceinline__ void group_sync(int id, int count) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+// CTAs that share one block of the block list: the average particle count of
+// the non-empty blocks (totals = {nactive, nassigned}) over `per_cta`, the
+// particles one CTA takes per pass, between 1 and 8. A crowded scene (4^3
+// particles per cell: 4096 per 4^3-cell block) has fewer blocks than the GPU
+// has CTA slots; splitting each block's passes over several CTAs (CTA `sub` of
+// `split` takes passes sub, sub + split, ...) restores the parallelism. The
+// transfers add each pass's tile to the grid with global atomics anyway, so
+// the split costs no extra work.
+__device__ __forceinline__ int block_split(const int* totals, int per_cta) {
+    const long long nact = totals[0], nass = totals[1];
+    if (nact <= 0) return 1;
+    const long long s = (nass / nact + per_cta / 2) / per_cta;
+    return int(s < 1 ? 1 : (s > 8 ? 8 : s));
 }
 
 // Forward-mode dual number with the three derivatives with respect to a

@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
         }
         return in;
     };
-    auto process_block = [&](const int b) {
+    auto process_block = [&](const int b, const int piece, const int pieces) {
         int org[3] = {0, 0, 0};
         {
             int r = b;
@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
             }
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0; b0 < s1; b0 += NR) {
+        for (int b0 = s0 + piece * NR; b0 < s1; b0 += pieces * NR) {
             const int nbat = min(NR, s1 - b0);
             // ---- 1a. every global load of the batch first (the ids, then all of
             //      the particles' fields at once: two dependent round trips per
@@ -1087,17 +1087,19 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
 
     if constexpr (MODE == 2) {
         const int nlist = int(*bnd_count);
-        for (int q = blockIdx.x; q < nlist; q += gridDim.x) process_block(bnd[q]);
+        for (int q = blockIdx.x; q < nlist; q += gridDim.x) process_block(bnd[q], 0, 1);
     } else {
-        for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+        const int split = block_split(totals, NR);
+        for (int vi = blockIdx.x; vi < nactive * split; vi += gridDim.x) {
+            const int bi = split == 1 ? vi : vi / split, piece = vi - bi * split;
             const int b = blocklist[bi] - 1;
             if constexpr (MODE == 1) {
                 if (!interior_block(b)) {  // the boundary launch's block (uniform over the CTA)
-                    if (tid == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
+                    if (tid == 0 && piece == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
                     continue;
                 }
             }
-            process_block(b);
+            process_block(b, piece, split);
         }
     }
 }
@@ -1189,7 +1191,9 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
     for (int g = tid; g < NG; g += NT) gcount[g] = 0;
     __syncthreads();
 
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+    const int split = block_split(totals, NR);
+    for (int vi = blockIdx.x; vi < nactive * split; vi += gridDim.x) {
+        const int bi = split == 1 ? vi : vi / split, piece = vi - bi * split;
         const int b = blocklist[bi] - 1;
         int org[3];
         bool interior = true;
@@ -1203,11 +1207,11 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
             }
         }
         if (!interior) {  // the full-record launch's block (uniform over the CTA)
-            if (tid == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
+            if (tid == 0 && piece == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
             continue;
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0; b0 < s1; b0 += NR) {
+        for (int b0 = s0 + piece * NR; b0 < s1; b0 += split * NR) {
             const int nbat = min(NR, s1 - b0);
             // ---- 1a. every global load of the batch first, then group and rank;
             //      the record's 14 values stay in registers until the slot is known
@@ -1400,357 +1404,6 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
     }
 }
 
-// ---------------------------------------------------------------------------
-// Warp-specialized plane kernel: the plane kernel's phases pipelined across the
-// blocks a CTA processes. Warps 0-3 (producers) build the records of the next
-// batch into one of two record buffers (loads, window start, group rank,
-// group scan, pencil order) and, once the sweep of the previous batch has
-// staged its partials, sum them and add them to the grid; warps 4-7
-// (consumers) sweep the current batch's records into the staging array (lane =
-// pencil slot x z slot, as p2g_plane_kernel). So a batch's global loads and
-// record building overlap the previous batch's sweep. Hand-offs are mbarriers:
-//   full[b]   records of buffer b ready      (producers arrive, consumers wait)
-//   empty[b]  records of buffer b consumed   (consumers arrive, producers wait)
-//   staged    the sweep's partials staged    (consumers arrive, producers wait)
-//   gathered  the staged partials consumed   (producers arrive, consumers wait)
-// Every wait is bounded (mbar_wait): a wait that gives up sets ERR_WAIT_LIMIT
-// and its warp group stops, and so does the other group at its next wait;
-// nothing spins unbounded. Both groups walk the same (block, batch) sequence
-// (boundary blocks are skipped by both, the producers list them for MODE 2).
-constexpr int WS_THREADS = 256;
-
-struct WsShared {
-    unsigned long long full[2], empty[2], staged, gathered;
-    int gstart[2][128];  // NG + 1 = 126 used
-    int pslot[2][32];
-    int org[2][3];
-    int gcount[128];     // NG = 125 used (producers only)
-    int stop;            // set when a group gave up a wait
-};
-
-template <bool X64>
-__global__ void __launch_bounds__(WS_THREADS, 2)
-    p2g_ws_kernel(DMesh<3, float> M, PView<float> P, GView<float> G, Scalars<float> s,
-                  const int* __restrict__ totals, const int* __restrict__ blocklist,
-                  const int* __restrict__ offsets, const int* __restrict__ perm, int* err,
-                  int* __restrict__ bnd, unsigned long long* __restrict__ bnd_count) {
-    using SH = PencilShape<3, 4>;
-    constexpr int NP = 128;  // producer threads
-    constexpr int NR = PLANE_NR, ITEMS = NR / NP;
-    constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
-    constexpr int NJK = SH::NJK, NPENCIL = SH::NPENCIL;
-    constexpr int CSTR = NPENCIL * NJK * TS;
-    constexpr int SKW = 2;
-    constexpr int RECW = NR * CRS + SKW * NPENCIL;  // words of one record buffer
-    static_assert(NR % NP == 0 && 3 * NPENCIL <= NP, "layout");
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float* recbuf = reinterpret_cast<float*>(smem_raw);  // [2][RECW]
-    float* part = recbuf + 2 * RECW;
-    // the mbarriers (8-byte words) start on a 16-byte boundary
-    constexpr size_t SH_OFF = ((sizeof(float) * size_t(2 * RECW + NC * CSTR) + 15) / 16) * 16;
-    WsShared& sh = *reinterpret_cast<WsShared*>(smem_raw + SH_OFF);
-
-    const int tid = threadIdx.x;
-    const bool producer = tid < NP;
-    const int gt = producer ? tid : tid - NP;  // thread index within the group
-    const int lane = tid & 31, gwarp = gt >> 5;
-    const int nactive = totals[0];
-
-    if (tid == 0) {
-        mbar_init(&sh.full[0], NP);
-        mbar_init(&sh.full[1], NP);
-        mbar_init(&sh.empty[0], NP);
-        mbar_init(&sh.empty[1], NP);
-        mbar_init(&sh.staged, NP);
-        mbar_init(&sh.gathered, NP);
-        sh.stop = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int g = tid; g < 128; g += WS_THREADS) sh.gcount[g] = 0;
-    __syncthreads();
-
-    // interior block: its halo tile lies inside the mesh (uniform over the CTA)
-    auto interior = [&](int b, int* org) {
-        bool in = true;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            org[d] = (b % M.nb[d]) * 4 - 1;
-            b /= M.nb[d];
-            in = in && org[d] >= 0 && org[d] + TS - 1 <= M.n[d] - 1;
-        }
-        return in;
-    };
-
-    if (producer) {
-        int it = 0;
-        int prev_buf = -1;
-        // sum the staged partials of the batch in buffer pb and add them to the
-        // grid; a wait that gives up raises sh.stop, which every producer reads
-        // after the next group barrier, so the group leaves its loop together
-        auto gather = [&](int pb) {
-            if (!mbar_wait(&sh.staged, unsigned((it - 1) & 1), err)) {
-                sh.stop = 1;
-                return;
-            }
-            const int* org = sh.org[pb];
-            for (int t = gt; t < TN; t += NP) {
-                const int tx = t % TS, ty = (t / TS) % TS, tz = t / (TS * TS);
-                float val[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c) val[c] = 0.0f;
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk)
-#pragma unroll
-                    for (int jj = 0; jj < 3; ++jj) {
-                        const int gy = ty - jj, gz = tz - kk;
-                        if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
-                        const int idx = ((jj + 3 * kk) * NPENCIL + gy + G1 * gz) * TS + tx;
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
-                    }
-                const long long lin = (long long)(org[0] + tx) +
-                                      (long long)M.n[0] * ((org[1] + ty) + (long long)M.n[1] * (org[2] + tz));
-#pragma unroll
-                for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
-                if (val[0] != 0.0f) atomicAdd(G.m + lin, val[0]);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    if (val[1 + d] != 0.0f) atomicAdd(G.mv[d] + lin, val[1 + d]);
-                    if (val[4 + d] != 0.0f) atomicAdd(G.f[d] + lin, val[4 + d]);
-                }
-            }
-            mbar_arrive(&sh.gathered);
-        };
-        bool ok = true;
-        for (int bi = blockIdx.x; bi < nactive && ok; bi += gridDim.x) {
-            const int b = blocklist[bi] - 1;
-            int org[3];
-            if (!interior(b, org)) {
-                if (gt == 0) bnd[atomicAdd(bnd_count, 1ull)] = b;
-                continue;
-            }
-            const int s0 = offsets[b], s1 = offsets[b + 1];
-            for (int b0 = s0; b0 < s1; b0 += NR, ++it) {
-                const int buf = it & 1;
-                float* rec = recbuf + buf * RECW;
-                if (it >= 2 && !mbar_wait(&sh.empty[buf], unsigned(((it >> 1) - 1) & 1), err)) sh.stop = 1;
-                // every producer has zeroed the group counters and left the last
-                // gather; a raised stop is seen by all of them here
-                group_sync(1, NP);
-                if (sh.stop) {
-                    ok = false;
-                    break;
-                }
-                const int nbat = min(NR, s1 - b0);
-                // ---- loads, window start, group and rank (as p2g_plane_kernel)
-                int pid[ITEMS], grp[ITEMS], rank[ITEMS];
-#pragma unroll
-                for (int u = 0; u < ITEMS; ++u) {
-                    const int ti = gt + u * NP;
-                    pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
-                }
-                float pv[ITEMS][3], pV[ITEMS], pm[ITEMS], psg[ITEMS][6], pt[ITEMS][3];
-                double pxd[ITEMS][3];
-                float pxf[ITEMS][3];
-#pragma unroll
-                for (int u = 0; u < ITEMS; ++u) {
-                    const long long p = pid[u] >= 0 ? pid[u] : 0;
-                    const bool on = pid[u] >= 0;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        if constexpr (X64) pxd[u][d] = on ? P.x64[d][p] : 0.0;
-                        else pxf[u][d] = on ? P.x[d][p] : 0.0f;
-                        pv[u][d] = on ? P.v[d][p] : 0.0f;
-                    }
-                    pV[u] = on ? P.V[p] : 0.0f;
-                    pm[u] = (on && P.m) ? P.m[p] : s.mass;
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) psg[u][k] = on ? P.sig[k][p] : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < ITEMS; ++u) {
-                    grp[u] = -1;
-                    rank[u] = 0;
-                    if (pid[u] < 0) continue;
-                    int gi = 0;
-                    bool okq = true;
-#pragma unroll
-                    for (int d = 2; d >= 0; --d) {
-                        int lo;
-                        if constexpr (X64) {
-                            const double u64 = (pxd[u][d] - M.xmin64[d]) * M.h_inv64 - 0.5;
-                            const double fl = floor(u64);
-                            lo = int(fl);
-                            float t = float(u64 - fl);
-                            if (t >= 1.0f) t = 1.0f - 1.0f / float(1 << 24);
-                            pt[u][d] = t;
-                        } else {
-                            const float uu = (pxf[u][d] - M.xmin[d]) * M.h_inv - 0.5f;
-                            const float fl = floorf(uu);
-                            lo = int(fl);
-                            pt[u][d] = uu - fl;
-                        }
-                        const int q = lo - org[d];
-                        okq = okq && q >= 0 && q < G1;
-                        gi = gi * G1 + q;
-                    }
-                    if (!okq) {
-                        atomicOr(err, ERR_TILE_RANGE);
-                        continue;
-                    }
-                    grp[u] = gi;
-                    rank[u] = atomicAdd(&sh.gcount[gi], 1);
-                }
-                group_sync(1, NP);
-                if (gwarp == 0) {
-                    int carry = 0;
-                    for (int g0 = 0; g0 < NG; g0 += 32) {
-                        const int g = g0 + lane;
-                        const int c = g < NG ? sh.gcount[g] : 0;
-                        int incl = c;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                            if (lane >= o) incl += t;
-                        }
-                        if (g < NG) sh.gstart[buf][g] = carry + incl - c;
-                        carry += __shfl_sync(0xffffffffu, incl, 31);
-                    }
-                    if (lane == 0) sh.gstart[buf][NG] = carry;
-                } else if (gwarp == 1) {
-                    const int myp = lane < NPENCIL ? lane : -1;
-                    int mysize = 0;
-                    if (myp >= 0) {
-                        const int gb = G1 * myp;
-#pragma unroll
-                        for (int gx = 0; gx < G1; ++gx) mysize += sh.gcount[gb + gx];
-                    }
-                    int rk = 0;
-                    for (int o = 0; o < NPENCIL; ++o) {
-                        const int os = __shfl_sync(0xffffffffu, mysize, o);
-                        rk += (os > mysize) || (os == mysize && o < lane);
-                    }
-                    if (myp >= 0) sh.pslot[buf][rk] = myp;
-                } else if (gt == 64) {
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) sh.org[buf][d] = org[d];
-                }
-                group_sync(1, NP);
-                for (int g = gt; g < NG; g += NP) sh.gcount[g] = 0;
-#pragma unroll
-                for (int u = 0; u < ITEMS; ++u) {
-                    if (grp[u] < 0) continue;
-                    float* r = rec + (sh.gstart[buf][grp[u]] + rank[u]) * CRS + SKW * (grp[u] / G1);
-                    const float mp = pm[u], nV = -pV[u];
-                    st2(r + 0, mp, mp * pv[u][0]);
-                    st2(r + 2, mp * pv[u][1], mp * pv[u][2]);
-                    st2(r + 4, nV * psg[u][0], nV * psg[u][1]);
-                    st2(r + 6, nV * psg[u][1], nV * psg[u][3]);
-                    st2(r + 8, nV * psg[u][2], nV * psg[u][4]);
-                    st2(r + 10, nV * psg[u][5], pt[u][2]);
-                    st2(r + 12, pt[u][0], pt[u][1]);
-                }
-                mbar_arrive(&sh.full[buf]);  // release: records, gstart, pslot, org of this batch
-                // ---- the previous batch's partials into the grid
-                if (prev_buf >= 0) gather(prev_buf);
-                prev_buf = buf;
-            }
-        }
-        group_sync(1, NP);
-        // `it` counts the batches, so the last one's staging completes phase it - 1
-        if (ok && !sh.stop && prev_buf >= 0) gather(prev_buf);
-    } else {
-        int it = 0;
-        bool ok = true;
-        for (int bi = blockIdx.x; bi < nactive && ok; bi += gridDim.x) {
-            const int b = blocklist[bi] - 1;
-            int org[3];
-            if (!interior(b, org)) continue;
-            const int s0 = offsets[b], s1 = offsets[b + 1];
-            for (int b0 = s0; b0 < s1; b0 += NR, ++it) {
-                const int buf = it & 1;
-                const float* rec = recbuf + buf * RECW;
-                if (!mbar_wait(&sh.full[buf], unsigned((it >> 1) & 1), err) ||
-                    (it >= 1 && !mbar_wait(&sh.gathered, unsigned((it - 1) & 1), err))) {
-                    ok = false;
-                    break;
-                }
-                if (gt < 3 * NPENCIL) {
-                    const int slot = gt / 3, k = gt - 3 * slot;
-                    const int pc = sh.pslot[buf][slot];
-                    const int gbase = G1 * pc;
-                    const float* prec = rec + SKW * pc;
-                    const SlotPoly pz = slot_poly(k);
-                    PairAcc acc[3][3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) {
-                            acc[i][j].a01 = acc[i][j].a23 = acc[i][j].f01 = make_float2(0.f, 0.f);
-                            acc[i][j].f2 = 0.f;
-                        }
-                    int qs = sh.gstart[buf][gbase];
-#pragma unroll
-                    for (int gx = 0; gx < G1 + 2; ++gx) {
-                        if (gx < G1) {
-                            const int qe = sh.gstart[buf][gbase + gx + 1];
-#pragma unroll 2
-                            for (int q = qs; q < qe; ++q) {
-                                PairRec r0;
-                                load_pair_rec(prec + q * CRS, r0);
-                                accumulate_plane(r0, pz, M.h_inv, acc);
-                            }
-                            qs = qe;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) {
-                            float* dst = part + ((j + 3 * k) * NPENCIL + pc) * TS + gx;
-                            dst[0 * CSTR] = acc[0][j].a01.x;
-                            dst[1 * CSTR] = acc[0][j].a01.y;
-                            dst[2 * CSTR] = acc[0][j].a23.x;
-                            dst[3 * CSTR] = acc[0][j].a23.y;
-                            dst[4 * CSTR] = acc[0][j].f01.x;
-                            dst[5 * CSTR] = acc[0][j].f01.y;
-                            dst[6 * CSTR] = acc[0][j].f2;
-                            acc[0][j] = acc[1][j];
-                            acc[1][j] = acc[2][j];
-                            acc[2][j].a01 = acc[2][j].a23 = acc[2][j].f01 = make_float2(0.f, 0.f);
-                            acc[2][j].f2 = 0.f;
-                        }
-                    }
-                }
-                mbar_arrive(&sh.empty[buf]);  // the records of this buffer are consumed
-                mbar_arrive(&sh.staged);      // release: the staged partials
-            }
-        }
-    }
-}
-
-size_t ws_smem_bytes() {
-    using SH = PencilShape<3, 4>;
-    const size_t words = sizeof(float) * (2 * (size_t(PLANE_NR) * CRS + 2 * SH::NPENCIL) + SH::NPART);
-    return ((words + 15) / 16) * 16 + sizeof(WsShared);
-}
-
-template <bool X64>
-cudaError_t launch_ws(const DMesh<3, float>& M, const PView<float>& P, const GView<float>& G, const Scalars<float>& s,
-                      const BinBuffers& b, const LaunchCfg& cfg) {
-    auto kern = p2g_ws_kernel<X64>;
-    const size_t smem = ws_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WS_THREADS, smem);
-    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
-    kern<<<grid, WS_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,
-                                                b.cursors, b.partials);
-    ++*cfg.launches;
-    return cudaGetLastError();
-}
-
 size_t plane_smem_bytes() {
     using SH = PencilShape<3, 4>;
     return sizeof(float) * (size_t(PLANE_NR) * CRS + 2 * SH::NPENCIL + SH::NPART) +
@@ -1768,7 +1421,7 @@ cudaError_t launch_plane(const DMesh<3, float>& M, const PView<float>& P, const 
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PLANE_THREADS, smem);
-    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), 8 * M.nblocks);  // blocks may be split (block_split)
     kern<<<grid, PLANE_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,
                                                    b.cursors, b.partials);
     ++*cfg.launches;
@@ -1836,7 +1489,9 @@ __global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
     for (int g = tid; g < NG; g += NT) gcount[g] = 0;
     __syncthreads();
 
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+    const int split = block_split(totals, NR);
+    for (int vi = blockIdx.x; vi < nactive * split; vi += gridDim.x) {
+        const int bi = split == 1 ? vi : vi / split, piece = vi - bi * split;
         const int b = blocklist[bi] - 1;
         int org[3];
         {
@@ -1848,7 +1503,7 @@ __global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
             }
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0; b0 < s1; b0 += NR) {
+        for (int b0 = s0 + piece * NR; b0 < s1; b0 += split * NR) {
             const int nbat = min(NR, s1 - b0);
             // ---- 1a. window start -> group and rank
             int pid[ITEMS], grp[ITEMS], rank[ITEMS];
@@ -2140,7 +1795,7 @@ cudaError_t launch_gen_plane_t(const DMesh<3, T>& M, const PView<T>& P, const GV
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, GEN_THREADS, smem);
-    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), 8 * M.nblocks);  // blocks may be split (block_split)
     KernelScope ks(cfg, "p2g");
     kern<<<grid, GEN_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err);
     ++*cfg.launches;
@@ -2179,7 +1834,7 @@ cudaError_t launch_pencil_mode(const DMesh<D, T>& M, const PView<T>& P, const GV
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2G_THREADS, smem);
-    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), M.nblocks);
+    const int grid = std::min(cfg.num_sms * std::max(per_sm, 1), 8 * M.nblocks);  // blocks may be split (block_split)
     // the boundary-block list lives in binning scratch that is free until the
     // next binning: cursors (one int per block) and the first scan partial
     kern<<<grid, P2G_THREADS, smem, cfg.stream>>>(M, P, G, s, b.totals, b.blocklist, b.offsets, b.perm, cfg.err,

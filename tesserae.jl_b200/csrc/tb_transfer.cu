@@ -240,7 +240,12 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
     const int nactive = totals[0];
     const int tid = threadIdx.x, nth = blockDim.x;
     const bool apic = s.transfer == TB_TRANSFER_APIC;
-    for (int bi = blockIdx.x; bi < nactive; bi += gridDim.x) {
+    // CTA `piece` of `split` sharing a block takes its particles piece nth + tid,
+    // (piece + split) nth + tid, ... (block_split: 4 particles per thread)
+    const int split = block_split(totals, 4 * nth);
+    const int stride = split * nth;
+    for (int vi = blockIdx.x; vi < nactive * split; vi += gridDim.x) {
+        const int bi = split == 1 ? vi : vi / split, piece = vi - bi * split;
         int b = blocklist[bi] - 1;
         int org[3] = {0, 0, 0};
 #pragma unroll
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
         b = blocklist[bi] - 1;
         // the block's particle range and this thread's first particle id are
         // loaded before the tile, so their round trips overlap the tile's
-        const int s0 = offsets[b], s1 = offsets[b + 1];
+        const int s0 = offsets[b] + piece * nth, s1 = offsets[b + 1];
         int pnext = (s0 + tid < s1) ? perm[s0 + tid] : 1;
         for (int t = tid; t < TN; t += nth) {
             int node[3], rem = t;
@@ -284,9 +289,9 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
             }
         }
         __syncthreads();
-        for (int j = s0 + tid; j < s1; j += nth) {
+        for (int j = s0 + tid; j < s1; j += stride) {
             const long long p = pnext - 1;
-            pnext = (j + nth < s1) ? perm[j + nth] : 1;  // next id in flight during this particle
+            pnext = (j + stride < s1) ? perm[j + stride] : 1;  // next id in flight during this particle
             T x[3] = {T(0), T(0), T(0)}, vp[3];
             double xd[3] = {0.0, 0.0, 0.0};
             if constexpr (X64) {
@@ -683,7 +688,7 @@ cudaError_t launch_g2p(const DMesh<D, T>& M, const GView<T>& G, const PView<T>& 
             return cudaErrorInvalidValue;
         }
     }
-    const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), M.nblocks);
+    const int grid = std::min(occupancy_grid(kern, 128, cfg.num_sms), 8 * M.nblocks);  // blocks may be split
     {
         // first: it reads this step's block ids, which the tiled pass below
         // replaces with the next step's when it counts
