@@ -371,13 +371,24 @@ int32_t tb_tape_backward_f64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* par
                              tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
 int32_t tb_tape_backward_f32(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
                              tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+/* The FP64-position form (particles.x double, the rest as _f32; the cases of
+ * tb_step_f32x64): the forward steps, the windows and the in-window offsets of
+ * the reverse step come from the FP64 positions. */
+int32_t tb_adjoint_step_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                               tb_grid* grid, const tb_step_params* params, tb_adjoint* adj);
+int32_t tb_tape_forward_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles, tb_partition* partition,
+                               tb_grid* grid, const tb_step_params* params, int32_t nsteps, int32_t checkpoint_every);
+int32_t tb_tape_backward_f32x64(tb_ctx* ctx, const tb_mesh* mesh, tb_particles* particles,
+                                tb_partition* partition, tb_grid* grid, const tb_step_params* params,
+                                tb_adjoint* adj);
 /* Device bytes a tape of `nsteps` steps over `n` particles holds (forward and
  * backward pass together) for element size `elem` (4 or 8; F is FP64 in both),
- * with the APIC matrix B when `apic` != 0, checkpointed every
+ * with the APIC matrix B when `apic` != 0, FP64 positions when `x64` != 0
+ * (elem 4 only), checkpointed every
  * `checkpoint_every` steps (1: the whole tape). Pure arithmetic, no device call:
  * lets a caller pick the interval against its free device memory. Returns -1 on
  * invalid arguments. */
-int64_t tb_tape_bytes(const tb_mesh* mesh, int64_t n, int32_t elem, int32_t apic, int32_t nsteps,
+int64_t tb_tape_bytes(const tb_mesh* mesh, int64_t n, int32_t elem, int32_t apic, int32_t x64, int32_t nsteps,
                       int32_t checkpoint_every);
 /* Frees the context's tape buffers (the next tb_tape_forward_* allocates them
  * again); the tape is invalid afterwards. Synchronises the context's stream. */

@@ -129,7 +129,7 @@ SIGNATURES = [
     ("tb_profile_read", I32, [VP, P(tb_kernel_time), I32, P(I32)]),
     ("tb_bin_particles_noalloc", I32, [P(tb_mesh), P(tb_particles), I32, P(tb_partition), VP, P(I64), P(I64),
                                        C.c_char_p, I32]),
-    ("tb_tape_bytes", I64, [P(tb_mesh), I64, I32, I32, I32, I32]),
+    ("tb_tape_bytes", I64, [P(tb_mesh), I64, I32, I32, I32, I32, I32]),
     ("tb_tape_release", I32, [VP]),
 ]
 for _p in ("f64", "f32"):
@@ -151,6 +151,12 @@ for _p in ("f64", "f32"):
 
 SIGNATURES += [
     ("tb_step_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(tb_step_params), I32]),
+    ("tb_adjoint_step_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                     P(tb_step_params), P(tb_adjoint)]),
+    ("tb_tape_forward_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                     P(tb_step_params), I32, I32]),
+    ("tb_tape_backward_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid),
+                                      P(tb_step_params), P(tb_adjoint)]),
     ("tb_rollout_host_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_step_params), I32]),
     ("tb_particle_contiguity", I32, [VP, P(tb_partition), I64, P(C.c_double)]),
     ("tb_max_wave_speed_f64", I32, [VP, I32, P(tb_particles), P(tb_step_params), P(C.c_double)]),

@@ -117,7 +117,7 @@ struct tb_ctx {
     bool tape_valid = false;
     long long tape_n = 0;
     int tape_dim = 0, tape_elem = 0;
-    bool tape_apic = false;
+    bool tape_apic = false, tape_x64 = false;
     int tape_nsteps = 0, tape_every = 1;
     // reorder_particles!: 8-byte-per-particle scratch, score accumulators,
     // decision words and the score
@@ -922,10 +922,10 @@ int grad_grid(tb_ctx* c, int dim, long long nn, GradGrid& GB) {
 // otherwise `part`, `g` and `totals` (device nactive, nassigned) already hold them.
 template <int D, class T, int BW>
 int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                 const tb_step_params* prm, const tb_adjoint* adj, bool recompute, const int* totals) {
+                 const tb_step_params* prm, const tb_adjoint* adj, bool recompute, const int* totals, bool x64) {
     int rc;
     if (recompute) {
-        if ((rc = run_step<D, T, BW>(c, m, p, part, g, prm, 1, true, true, true, false)) != TB_OK) return rc;
+        if ((rc = run_step<D, T, BW>(c, m, p, part, g, prm, 1, true, true, true, false, x64)) != TB_OK) return rc;
         totals = c->d_totals;
     }
     const auto M = make_dmesh<D, T>(*m);
@@ -935,7 +935,7 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     AdjView A;
     GradGrid GB;
     const bool apic = prm->transfer == TB_TRANSFER_APIC;
-    if ((rc = make_pview<T>(c, p, D, true, apic, P)) != TB_OK) return rc;
+    if ((rc = make_pview<T>(c, p, D, true, apic, P, x64, prm->material)) != TB_OK) return rc;
     if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
     if ((rc = make_adjview(c, adj, D, P.n, A, apic)) != TB_OK) return rc;
     if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
@@ -954,23 +954,33 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
 template <class T>
 int adjoint_dispatch(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
                      const tb_step_params* prm, const tb_adjoint* adj, bool recompute = true,
-                     const int* totals = nullptr) {
-    if (m->dim == 3) return adjoint_impl<3, T, 4>(c, m, p, part, g, prm, adj, recompute, totals);
-    if (m->block_log2 == 3) return adjoint_impl<2, T, 8>(c, m, p, part, g, prm, adj, recompute, totals);
-    return adjoint_impl<2, T, 4>(c, m, p, part, g, prm, adj, recompute, totals);
+                     const int* totals = nullptr, bool x64 = false) {
+    if (m->dim == 3) return adjoint_impl<3, T, 4>(c, m, p, part, g, prm, adj, recompute, totals, x64);
+    if (m->block_log2 == 3) return adjoint_impl<2, T, 8>(c, m, p, part, g, prm, adj, recompute, totals, x64);
+    return adjoint_impl<2, T, 4>(c, m, p, part, g, prm, adj, recompute, totals, x64);
+}
+
+// The FP64-position form of the reverse step takes the forward form's cases.
+int check_x64_adjoint(tb_ctx* c, const tb_mesh* m, const tb_step_params* prm) {
+    if (m->dim != 3 && (prm->transfer != TB_TRANSFER_FLIP || prm->basis == TB_WLS_BSPLINE_QUADRATIC ||
+                        prm->basis == TB_WLS_UGIMP))
+        return fail(c, TB_ERR_UNSUPPORTED, "the FP64-position form runs WLS and APIC in 3D only");
+    return TB_OK;
 }
 
 template <class T>
 int do_adjoint_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                    const tb_step_params* prm, const tb_adjoint* adj) {
+                    const tb_step_params* prm, const tb_adjoint* adj, bool x64 = false) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
         return rc;
-    return adjoint_dispatch<T>(c, m, p, part, g, prm, adj);
+    if (x64 && (rc = check_x64_adjoint(c, m, prm)) != TB_OK) return rc;
+    return adjoint_dispatch<T>(c, m, p, part, g, prm, adj, true, nullptr, x64);
 }
 
 // The state tb_step_* reads and writes, as (particle array, element size)
-// fields: x, v (T), F (double), sigma (T), V (T). grad_v is output only.
+// fields: x (T, or double in the FP64-position form), v (T), F (double),
+// sigma (T), V (T), B (T, APIC). grad_v is output only.
 struct StateFields {
     int count = 0;
     void** slot[32];
@@ -978,14 +988,14 @@ struct StateFields {
 };
 
 template <class T>
-StateFields state_fields(tb_particles* p, int D, bool apic) {
+StateFields state_fields(tb_particles* p, int D, bool apic, bool x64 = false) {
     StateFields f;
     auto add = [&](void** s, size_t e) {
         f.slot[f.count] = s;
         f.elem[f.count] = e;
         ++f.count;
     };
-    for (int d = 0; d < D; ++d) add(&p->x[d], sizeof(T));
+    for (int d = 0; d < D; ++d) add(&p->x[d], x64 ? sizeof(double) : sizeof(T));
     for (int d = 0; d < D; ++d) add(&p->v[d], sizeof(T));
     for (int k = 0; k < D * D; ++k) add(&p->F[k], sizeof(double));
     for (int k = 0; k < (D == 3 ? 6 : 3); ++k) add(&p->sigma[k], sizeof(T));
@@ -998,24 +1008,25 @@ StateFields state_fields(tb_particles* p, int D, bool apic) {
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 template <class T>
-size_t state_bytes(int D, long long n, bool apic) {
-    const int nf = 2 * D + (D == 3 ? 6 : 3) + 1 + (apic ? D * D : 0);
-    return size_t(nf) * align256(sizeof(T) * size_t(n)) + size_t(D * D) * align256(sizeof(double) * size_t(n));
+size_t state_bytes(int D, long long n, bool apic, bool x64 = false) {
+    const int nf = D + (D == 3 ? 6 : 3) + 1 + (apic ? D * D : 0);  // v, sigma, V, B
+    return size_t(nf) * align256(sizeof(T) * size_t(n)) + size_t(D) * align256((x64 ? 8 : sizeof(T)) * size_t(n)) +
+           size_t(D * D) * align256(sizeof(double) * size_t(n));
 }
 
 // One step of a tape segment: the state before the step, the step's forward
 // grid and partition, and its device totals.
 template <class T>
-size_t slot_bytes(int D, long long n, long long nn, long long nb, bool apic) {
-    return state_bytes<T>(D, n, apic) + size_t(1 + 4 * D) * align256(sizeof(T) * size_t(nn)) +
+size_t slot_bytes(int D, long long n, long long nn, long long nb, bool apic, bool x64 = false) {
+    return state_bytes<T>(D, n, apic, x64) + size_t(1 + 4 * D) * align256(sizeof(T) * size_t(nn)) +
            2 * align256(sizeof(int) * size_t(n)) + 2 * align256(sizeof(int) * size_t(nb)) +
            align256(sizeof(int) * size_t(nb + 1)) + 256;
 }
 
 template <class T>
 void slot_views(char* base, int D, long long n, long long nn, long long nb, bool apic, tb_grid& g,
-                tb_partition& part, int*& totals) {
-    char* q = base + state_bytes<T>(D, n, apic);
+                tb_partition& part, int*& totals, bool x64 = false) {
+    char* q = base + state_bytes<T>(D, n, apic, x64);
     auto take = [&](size_t bytes) {
         char* r = q;
         q += align256(bytes);
@@ -1041,9 +1052,9 @@ void slot_views(char* base, int D, long long n, long long nn, long long nb, bool
 
 // Particles whose state fields point into the snapshot at `base`.
 template <class T>
-tb_particles snapshot_view(const tb_particles* p, int D, char* base, bool apic) {
+tb_particles snapshot_view(const tb_particles* p, int D, char* base, bool apic, bool x64 = false) {
     tb_particles q = *p;
-    StateFields f = state_fields<T>(&q, D, apic);
+    StateFields f = state_fields<T>(&q, D, apic, x64);
     size_t off = 0;
     for (int i = 0; i < f.count; ++i) {
         *f.slot[i] = base + off;
@@ -1053,9 +1064,9 @@ tb_particles snapshot_view(const tb_particles* p, int D, char* base, bool apic) 
 }
 
 template <class T>
-int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int D, bool apic) {
-    StateFields fd = state_fields<T>(const_cast<tb_particles*>(dst), D, apic);
-    StateFields fs = state_fields<T>(const_cast<tb_particles*>(src), D, apic);
+int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int D, bool apic, bool x64 = false) {
+    StateFields fd = state_fields<T>(const_cast<tb_particles*>(dst), D, apic, x64);
+    StateFields fs = state_fields<T>(const_cast<tb_particles*>(src), D, apic, x64);
     for (int i = 0; i < fd.count; ++i) {
         if (!*fs.slot[i] || !*fd.slot[i]) return fail(c, TB_ERR_ARG, "particle state field %d is NULL", i);
         const cudaError_t e = cudaMemcpyAsync(*fd.slot[i], *fs.slot[i], fd.elem[i] * size_t(src->n),
@@ -1067,16 +1078,17 @@ int copy_state(tb_ctx* c, const tb_particles* dst, const tb_particles* src, int 
 
 template <class T>
 int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                    const tb_step_params* prm, int nsteps, int every) {
+                    const tb_step_params* prm, int nsteps, int every, bool x64 = false) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
         return rc;
+    if (x64 && (rc = check_x64_adjoint(c, m, prm)) != TB_OK) return rc;
     if (nsteps < 0 || every < 1) return fail(c, TB_ERR_ARG, "nsteps must be >= 0 and checkpoint_every >= 1");
     if (!p) return fail(c, TB_ERR_ARG, "particles is NULL");
     const int D = m->dim;
     PView<T> P;
     const bool apic = prm->transfer == TB_TRANSFER_APIC;
-    if ((rc = make_pview<T>(c, p, D, true, apic, P)) != TB_OK) return rc;
+    if ((rc = make_pview<T>(c, p, D, true, apic, P, x64, prm->material)) != TB_OK) return rc;
     c->tape_valid = false;
     if (every == 1) {
         // every step kept whole: its input state, grid and partition (the slots
@@ -1085,33 +1097,33 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
         long long nn = 1;
         for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
         const long long nb = mesh_nblocks(m);
-        const size_t slot = slot_bytes<T>(D, p->n, nn, nb, apic);
+        const size_t slot = slot_bytes<T>(D, p->n, nn, nb, apic, x64);
         const long long nslot = std::max(nsteps, 1);
         cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(nslot * slot));
         if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape");
         for (long long j = 0; j < nslot; ++j) {
             char* base = c->tape_cp + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic, x64);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
-            if ((rc = copy_state<T>(c, &sj, p, D, apic)) != TB_OK) return rc;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj, x64);
+            if ((rc = copy_state<T>(c, &sj, p, D, apic, x64)) != TB_OK) return rc;
             if (j >= nsteps) continue;
-            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, true)) != TB_OK) return rc;
+            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, true, x64)) != TB_OK) return rc;
             e = cudaMemcpyAsync(tj, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
             if (e != cudaSuccess) return cuda_fail(c, e, "tape totals copy");
         }
     } else {
     const long long ncp = nsteps > 0 ? (nsteps + every - 1) / every : 1;
-    const size_t sb = state_bytes<T>(D, p->n, apic);
+    const size_t sb = state_bytes<T>(D, p->n, apic, x64);
     cudaError_t e = grow(c->tape_cp, c->tape_cp_cap, (long long)(ncp * sb));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc checkpoints");
     for (long long k = 0; k < ncp; ++k) {
-        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic);
-        if ((rc = copy_state<T>(c, &cp, p, D, apic)) != TB_OK) return rc;
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic, x64);
+        if ((rc = copy_state<T>(c, &cp, p, D, apic, x64)) != TB_OK) return rc;
         const int steps = std::min<long long>(every, nsteps - k * every);
-        if (steps > 0 && (rc = dispatch_step<T>(c, m, p, part, g, prm, steps, true, true, true, true)) != TB_OK)
+        if (steps > 0 && (rc = dispatch_step<T>(c, m, p, part, g, prm, steps, true, true, true, true, x64)) != TB_OK)
             return rc;
     }
     }
@@ -1120,6 +1132,7 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     c->tape_dim = D;
     c->tape_elem = int(sizeof(T));
     c->tape_apic = apic;
+    c->tape_x64 = x64;
     c->tape_nsteps = nsteps;
     c->tape_every = every;
     return TB_OK;
@@ -1127,7 +1140,7 @@ int do_tape_forward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
 
 template <class T>
 int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
-                     const tb_step_params* prm, const tb_adjoint* adj) {
+                     const tb_step_params* prm, const tb_adjoint* adj, bool x64 = false) {
     int rc;
     if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
         return rc;
@@ -1135,7 +1148,7 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
     const int D = m->dim;
     const bool apic = prm->transfer == TB_TRANSFER_APIC;
     if (!c->tape_valid || c->tape_n != p->n || c->tape_dim != D || c->tape_elem != int(sizeof(T)) ||
-        c->tape_apic != apic)
+        c->tape_apic != apic || c->tape_x64 != x64)
         return fail(c, TB_ERR_ARG, "no forward tape for these particles on this context (run tb_tape_forward first)");
     (void)part;
     (void)g;
@@ -1143,52 +1156,52 @@ int do_tape_backward(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition*
     long long nn = 1;
     for (int d = 0; d < D; ++d) nn *= m->n_nodes[d];
     const long long nb = mesh_nblocks(m);
-    const size_t sb = state_bytes<T>(D, p->n, apic), slot = slot_bytes<T>(D, p->n, nn, nb, apic);
+    const size_t sb = state_bytes<T>(D, p->n, apic, x64), slot = slot_bytes<T>(D, p->n, nn, nb, apic, x64);
     if (K == 1) {  // the whole tape: the adjoint steps read the slots the forward kept
         for (long long j = nsteps - 1; j >= 0; --j) {
             char* base = c->tape_cp + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic, x64);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
-            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj)) != TB_OK) return rc;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj, x64);
+            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj, x64)) != TB_OK) return rc;
         }
-        tb_particles s0 = snapshot_view<T>(p, D, c->tape_cp, apic);
-        return copy_state<T>(c, p, &s0, D, apic);
+        tb_particles s0 = snapshot_view<T>(p, D, c->tape_cp, apic, x64);
+        return copy_state<T>(c, p, &s0, D, apic, x64);
     }
     cudaError_t e = grow(c->tape_seg, c->tape_seg_cap, (long long)(K * slot));
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc tape segment");
     const long long ncp = nsteps > 0 ? (nsteps + K - 1) / K : 1;
     for (long long k = ncp - 1; k >= 0 && nsteps > 0; --k) {
         const int len = int(std::min<long long>(K, nsteps - k * K));
-        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic);
-        if ((rc = copy_state<T>(c, p, &cp, D, apic)) != TB_OK) return rc;
+        tb_particles cp = snapshot_view<T>(p, D, c->tape_cp + k * sb, apic, x64);
+        if ((rc = copy_state<T>(c, p, &cp, D, apic, x64)) != TB_OK) return rc;
         // re-run the segment, keeping each step's input state, grid and partition
         for (int j = 0; j < len; ++j) {
             char* base = c->tape_seg + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic, x64);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
-            if ((rc = copy_state<T>(c, &sj, p, D, apic)) != TB_OK) return rc;
-            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, j + 1 < len)) != TB_OK) return rc;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj, x64);
+            if ((rc = copy_state<T>(c, &sj, p, D, apic, x64)) != TB_OK) return rc;
+            if ((rc = dispatch_step<T>(c, m, p, &pj, &gj, prm, 1, true, true, true, j + 1 < len, x64)) != TB_OK) return rc;
             e = cudaMemcpyAsync(tj, c->d_totals, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
             if (e != cudaSuccess) return cuda_fail(c, e, "tape totals copy");
         }
         for (int j = len - 1; j >= 0; --j) {
             char* base = c->tape_seg + j * slot;
-            tb_particles sj = snapshot_view<T>(p, D, base, apic);
+            tb_particles sj = snapshot_view<T>(p, D, base, apic, x64);
             tb_grid gj;
             tb_partition pj;
             int* tj;
-            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj);
-            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj)) != TB_OK) return rc;
+            slot_views<T>(base, D, p->n, nn, nb, apic, gj, pj, tj, x64);
+            if ((rc = adjoint_dispatch<T>(c, m, &sj, &pj, &gj, prm, adj, false, tj, x64)) != TB_OK) return rc;
         }
     }
-    tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp, apic);
-    return copy_state<T>(c, p, &cp0, D, apic);
+    tb_particles cp0 = snapshot_view<T>(p, D, c->tape_cp, apic, x64);
+    return copy_state<T>(c, p, &cp0, D, apic, x64);
 }
 
 }  // namespace
@@ -1440,6 +1453,10 @@ int32_t tb_adjoint_step_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_par
                             const tb_step_params* prm, tb_adjoint* adj) {
     return do_adjoint_step<float>(c, m, p, part, g, prm, adj);
 }
+int32_t tb_adjoint_step_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                               const tb_step_params* prm, tb_adjoint* adj) {
+    return do_adjoint_step<float>(c, m, p, part, g, prm, adj, true);
+}
 
 int32_t tb_tape_forward_f64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
                             const tb_step_params* prm, int32_t nsteps, int32_t every) {
@@ -1457,8 +1474,16 @@ int32_t tb_tape_backward_f32(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_pa
                              const tb_step_params* prm, tb_adjoint* adj) {
     return do_tape_backward<float>(c, m, p, part, g, prm, adj);
 }
+int32_t tb_tape_forward_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                               const tb_step_params* prm, int32_t nsteps, int32_t every) {
+    return do_tape_forward<float>(c, m, p, part, g, prm, nsteps, every, true);
+}
+int32_t tb_tape_backward_f32x64(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, tb_grid* g,
+                                const tb_step_params* prm, tb_adjoint* adj) {
+    return do_tape_backward<float>(c, m, p, part, g, prm, adj, true);
+}
 
-int64_t tb_tape_bytes(const tb_mesh* m, int64_t n, int32_t elem, int32_t apic, int32_t nsteps,
+int64_t tb_tape_bytes(const tb_mesh* m, int64_t n, int32_t elem, int32_t apic, int32_t x64, int32_t nsteps,
                       int32_t checkpoint_every) {
     if (!m || (m->dim != 2 && m->dim != 3) || n < 0 || (elem != 4 && elem != 8) || nsteps < 0 ||
         checkpoint_every < 1)
@@ -1470,9 +1495,9 @@ int64_t tb_tape_bytes(const tb_mesh* m, int64_t n, int32_t elem, int32_t apic, i
         nn *= m->n_nodes[d];
     }
     const long long nb = mesh_nblocks(m);
-    const bool ap = apic != 0;
-    const size_t sb = elem == 4 ? state_bytes<float>(D, n, ap) : state_bytes<double>(D, n, ap);
-    const size_t slot = elem == 4 ? slot_bytes<float>(D, n, nn, nb, ap) : slot_bytes<double>(D, n, nn, nb, ap);
+    const bool ap = apic != 0, xd = x64 != 0 && elem == 4;
+    const size_t sb = elem == 4 ? state_bytes<float>(D, n, ap, xd) : state_bytes<double>(D, n, ap);
+    const size_t slot = elem == 4 ? slot_bytes<float>(D, n, nn, nb, ap, xd) : slot_bytes<double>(D, n, nn, nb, ap);
     if (checkpoint_every == 1) return (int64_t)(std::max(nsteps, 1) * slot);
     const long long ncp = nsteps > 0 ? (nsteps + checkpoint_every - 1) / checkpoint_every : 1;
     return (int64_t)(ncp * sb + (long long)checkpoint_every * slot);

@@ -14,6 +14,8 @@
 // H is the Hessian of the kernel with respect to x_p (per-axis second
 // derivatives of the quadratic B-spline or uGIMP). The forward values (weights,
 // grid velocities) are read in the state type T; every adjoint quantity is FP64.
+// In the FP64-position form (P.x64 set) the windows and in-window offsets come
+// from the FP64 positions, as in the forward kernels of that form.
 // Both particle passes keep the (BW+3)^D halo tile of the block they work on
 // in shared memory, so the gathers stay on chip, and evaluate their sums over the
 // window as separable moments (one axis at a time). The scatter of 1. is a
@@ -39,6 +41,16 @@ __device__ __forceinline__ double d2_ugimp(double xi, double l) {
     return 0.0;
 }
 
+// Position of particle p in FP64: the FP64-position form's own array, else the
+// state type's value.
+template <int D, class T>
+__device__ __forceinline__ void load_xd(const PView<T>& P, long long p, double (&xd)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xd[d] = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) xd[d] = P.x64[0] ? P.x64[d][p] : double(P.x[d][p]);
+}
+
 // Per-axis jets (value, first and second derivative in xi) of one particle's window.
 template <int D>
 struct AdjAxes {
@@ -48,13 +60,18 @@ struct AdjAxes {
 };
 
 template <int D, class T>
-__device__ __forceinline__ bool adj_axes(const DMesh<D, T>& M, const Scalars<T>& s, const T* x, T l_abs,
-                                         AdjAxes<D>& A, int* err) {
+__device__ __forceinline__ bool adj_axes(const DMesh<D, T>& M, const Scalars<T>& s, const double* xd, bool x64,
+                                         T l_abs, AdjAxes<D>& A, int* err) {
     Basis<D, T> B;
-    if (!prepare_basis<D, T, false>(M, s.basis, x, l_abs, B, err)) return false;
+    if (x64) {
+        if (!prepare_basis_x64<D, T>(M, s.basis, xd, l_abs, B, err)) return false;
+    } else {
+        const T x[3] = {T(xd[0]), T(xd[1]), T(xd[2])};
+        if (!prepare_basis<D, T, false>(M, s.basis, x, l_abs, B, err)) return false;
+    }
     const bool gimp = s.basis == TB_UGIMP;
-    const double lnorm = gimp ? double(T(l_abs / M.h)) : 0.0;
-    A.hi = double(M.h_inv);
+    const double lnorm = gimp ? (x64 ? double(l_abs) / M.h64 : double(T(l_abs / M.h))) : 0.0;
+    A.hi = x64 ? M.h_inv64 : double(M.h_inv);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         A.lo[d] = B.ax[d].lo;
@@ -63,7 +80,9 @@ __device__ __forceinline__ bool adj_axes(const DMesh<D, T>& M, const Scalars<T>&
         for (int k = 0; k < 3; ++k) {
             A.val[d][k] = double(B.ax[d].val[k]);
             A.der[d][k] = double(B.ax[d].der[k]);
-            double xi = (double(x[d]) - double(node_coord(M, d, B.ax[d].lo + k))) * A.hi;
+            const double X = x64 ? __dadd_rn(M.xmin64[d], __dmul_rn(double(B.ax[d].lo + k), M.h64))
+                                 : double(node_coord(M, d, B.ax[d].lo + k));
+            const double xi = (xd[d] - X) * A.hi;
             A.d2[d][k] = (k < B.ax[d].cnt) ? (gimp ? d2_ugimp(xi, lnorm) : d2_bspline_quadratic(xi)) : 0.0;
         }
     }
@@ -269,9 +288,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
             const long long p = pnext - 1;
             if (j + ADJ_THREADS < s1) pnext = perm[j + ADJ_THREADS];
-            T x[3] = {T(0), T(0), T(0)};
-#pragma unroll
-            for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+            double xd[3];
+            load_xd<D, T>(P, p, xd);
             const T l = P.l ? P.l[p] : s.gimp_l;
             double F[3][3] = {}, Fb[3][3] = {};
 #pragma unroll
@@ -306,7 +324,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_g2p_kernel(DMesh<D, T> M, GVi
             }
             AdjAxes<D> ax;
             int q0[3];
-            const bool in = adj_axes<D, T>(M, s, x, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err);
+            const bool in = adj_axes<D, T>(M, s, xd, P.x64[0] != nullptr, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err);
             double L[3][3] = {};
             if (in) {
                 double J[3][3][3];
@@ -459,12 +477,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
             rank[u] = 0;
             pid[u] = tid + u * NT < c1 - c0 ? perm[c0 + tid + u * NT] - 1 : -1;
         }
-        T px[ITEMS][3], pl[ITEMS];
+        double px[ITEMS][3];
+        T pl[ITEMS];
 #pragma unroll
         for (int u = 0; u < ITEMS; ++u) {
             const long long p = pid[u] >= 0 ? pid[u] : 0;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) px[u][d] = (pid[u] >= 0 && d < D) ? P.x[d < D ? d : 0][p] : T(0);
+            load_xd<D, T>(P, p, px[u]);
             pl[u] = (pid[u] >= 0 && P.l) ? P.l[p] : s.gimp_l;
         }
         // the coefficients go to the record slot at once (used only if the
@@ -487,7 +505,14 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
             if (pid[u] < 0) continue;
             const int slot = tid + u * NT;
             Basis<D, T> B;
-            if (prepare_basis<D, T, false>(M, s.basis, px[u], pl[u], B, err)) {
+            bool in;
+            if (P.x64[0]) {
+                in = prepare_basis_x64<D, T>(M, s.basis, px[u], pl[u], B, err);
+            } else {
+                const T x[3] = {T(px[u][0]), T(px[u][1]), T(px[u][2])};
+                in = prepare_basis<D, T, false>(M, s.basis, x, pl[u], B, err);
+            }
+            if (in) {
                 int gi = 0;
                 bool ok = true;
 #pragma unroll
@@ -712,14 +737,13 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_p2g_kernel(DMesh<D, T> M, PVi
         for (int j = s0 + tid; j < s1; j += ADJ_THREADS) {
             const long long p = pnext - 1;
             if (j + ADJ_THREADS < s1) pnext = perm[j + ADJ_THREADS];
-            T x[3] = {T(0), T(0), T(0)};
-#pragma unroll
-            for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+            double xd[3];
+            load_xd<D, T>(P, p, xd);
             const T l = P.l ? P.l[p] : s.gimp_l;
             double xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, sb[3][3] = {}, Vb = 0.0;
             AdjAxes<D> ax;
             int q0[3];
-            if (adj_axes<D, T>(M, s, x, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err)) {
+            if (adj_axes<D, T>(M, s, xd, P.x64[0] != nullptr, l, ax, err) && window_in_tile<D, TS>(ax, org, q0, err)) {
                 const double mp = double(P.m ? P.m[p] : s.mass), Vp = double(P.V[p]);
                 double vp[3] = {0, 0, 0}, grav[3] = {0, 0, 0}, sig[3][3] = {};
 #pragma unroll
@@ -863,20 +887,22 @@ __global__ void __launch_bounds__(256) adj_material_kernel(PView<T> P, Scalars<T
 // v / vn sensitivities of G2P backwards are scattered with FP64 global atomics
 // (27 nodes x 2D per particle); P2G backwards gathers m_bar, mv_bar, f_bar over
 // the window and leaves sigma_bar, V_bar for adj_material_kernel.
+// The mesh in Dual3: the state type's spacing and origin, or the FP64 ones in
+// the FP64-position form (whose forward windows come from them).
 template <int D, class T>
-__device__ __forceinline__ DMesh<D, Dual3> dual_mesh(const DMesh<D, T>& M) {
+__device__ __forceinline__ DMesh<D, Dual3> dual_mesh(const DMesh<D, T>& M, bool x64) {
     DMesh<D, Dual3> R;
     for (int d = 0; d < 3; ++d) {
         R.n[d] = M.n[d];
         R.nb[d] = M.nb[d];
-        R.xmin[d] = Dual3(double(M.xmin[d]));
+        R.xmin[d] = Dual3(x64 ? M.xmin64[d] : double(M.xmin[d]));
         R.xmin64[d] = M.xmin64[d];
     }
     R.L = M.L;
     R.nblocks = M.nblocks;
     R.nnodes = M.nnodes;
-    R.h = Dual3(double(M.h));
-    R.h_inv = Dual3(double(M.h_inv));
+    R.h = Dual3(x64 ? M.h64 : double(M.h));
+    R.h_inv = Dual3(x64 ? M.h_inv64 : double(M.h_inv));
     R.h64 = M.h64;
     R.h_inv64 = M.h_inv64;
     return R;
@@ -884,12 +910,12 @@ __device__ __forceinline__ DMesh<D, Dual3> dual_mesh(const DMesh<D, T>& M) {
 
 // Basis of particle x in Dual3: dual seeds e_0 .. e_{D-1} on the position.
 template <int D, class T>
-__device__ __forceinline__ bool dual_basis(const DMesh<D, Dual3>& MD, const Scalars<T>& s, const T* x, T l,
+__device__ __forceinline__ bool dual_basis(const DMesh<D, Dual3>& MD, const Scalars<T>& s, const double* x, T l,
                                            Basis<D, Dual3>& B, int* err) {
     Dual3 xd[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        xd[d] = Dual3(d < D ? double(x[d]) : 0.0);
+        xd[d] = Dual3(d < D ? x[d] : 0.0);
         if (d < D) xd[d].d[d] = 1.0;
     }
     return prepare_basis<D, Dual3, true>(MD, s.basis, xd, Dual3(double(l)), B, err);
@@ -906,14 +932,13 @@ template <int D, class T>
 __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T> G, PView<T> P, Scalars<T> s,
                                                           AdjView A, GradGrid GB, const int* __restrict__ blockids,
                                                           int* err) {
-    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M);
+    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M, P.x64[0] != nullptr);
     const bool apic = s.transfer == TB_TRANSFER_APIC;
     const double dt = s.dt64, alpha = double(s.alpha);
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P.n;
          p += (long long)gridDim.x * blockDim.x) {
-        T x[3] = {T(0), T(0), T(0)};
-#pragma unroll
-        for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+        double x[3];
+        load_xd<D, T>(P, p, x);
         const T l = P.l ? P.l[p] : s.gimp_l;
         Basis<D, Dual3> B;
         const bool in = blockids[p] != 0 && dual_basis<D, T>(MD, s, x, l, B, err);
@@ -936,7 +961,7 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
             for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(double(x[d]));
+                rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(x[d]);
                 rel[d].d[d] = -1.0;
             }
         };
@@ -1056,16 +1081,15 @@ template <int D, class T>
 __global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T> P, Scalars<T> s, AdjView A,
                                                           GradGrid GB, double* __restrict__ sbar,
                                                           const int* __restrict__ blockids, int* err) {
-    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M);
+    const DMesh<D, Dual3> MD = dual_mesh<D, T>(M, P.x64[0] != nullptr);
     const bool apic = s.transfer == TB_TRANSFER_APIC;
     const double dinv = 4.0 / (double(M.h) * double(M.h));
     const long long n = P.n;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {
         if (blockids[p] == 0) continue;
-        T x[3] = {T(0), T(0), T(0)};
-#pragma unroll
-        for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
+        double x[3];
+        load_xd<D, T>(P, p, x);
         const T l = P.l ? P.l[p] : s.gimp_l;
         Basis<D, Dual3> B;
         if (!dual_basis<D, T>(MD, s, x, l, B, err)) continue;
@@ -1099,7 +1123,7 @@ __global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T
                     for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
 #pragma unroll
                     for (int d = 0; d < D; ++d) {
-                        rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(double(x[d]));
+                        rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(x[d]);
                         rel[d].d[d] = -1.0;
                     }
                     Dual3 N, Gn[3];

@@ -641,15 +641,16 @@ function b200_rollout(v0::CuMatrix, particles, grid, partition, prm::TbParams, n
     if checkpoint_every === nothing
         elem = form(particles) === :f64 ? 8 : 4
         bytes = GC.@preserve grid ccall((:tb_tape_bytes, libtb), Int64,
-                                        (Ref{TbMesh}, Int64, Int32, Int32, Int32, Int32),
+                                        (Ref{TbMesh}, Int64, Int32, Int32, Int32, Int32, Int32),
                                         tbmesh(grid.x), length(particles), Int32(elem),
-                                        Int32(prm.transfer == TB_TRANSFER_APIC), Int32(nsteps), Int32(1))
+                                        Int32(prm.transfer == TB_TRANSFER_APIC), Int32(form(particles) === :f32x64),
+                                        Int32(nsteps), Int32(1))
         checkpoint_every = 0 <= bytes <= 0.6 * CUDA.available_memory() ? 1 : 20
     end
     setv!(particles, v0)
     pd, gd = tbparticles(particles), tbgrid(grid)
     GC.@preserve grid particles partition begin
-        rc = ccall((sym(:tb_tape_forward, form(particles) === :f64 ? :f64 : :f32), libtb), Int32,
+        rc = ccall((sym(:tb_tape_forward, form(particles)), libtb), Int32,
                    (Ptr{Cvoid}, Ref{TbMesh}, Ref{TbParticles}, Ref{TbPartition}, Ref{TbGrid}, Ref{TbParams},
                     Int32, Int32),
                    ctx(), tbmesh(grid.x), pd, tbpartition(Tesserae.strategy(partition)), gd, prm, Int32(nsteps),
@@ -684,7 +685,7 @@ function ChainRulesCore.rrule(::typeof(b200_rollout), v0, particles, grid, parti
                         Ptr{Float64}(0), Ptr{Float64}(0), ntuple(_ -> Ptr{Float64}(0), 9))
         pd, gd = tbparticles(particles), tbgrid(grid)
         GC.@preserve grid particles partition gx gv gF begin
-            rc = ccall((sym(:tb_tape_backward, form(particles) === :f64 ? :f64 : :f32), libtb), Int32,
+            rc = ccall((sym(:tb_tape_backward, form(particles)), libtb), Int32,
                        (Ptr{Cvoid}, Ref{TbMesh}, Ref{TbParticles}, Ref{TbPartition}, Ref{TbGrid}, Ref{TbParams},
                         Ref{TbAdjoint}),
                        ctx(), tbmesh(grid.x), pd, tbpartition(Tesserae.strategy(partition)), gd, prm, adj)

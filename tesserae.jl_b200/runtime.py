@@ -249,36 +249,38 @@ def adjoint_step(grid: Grid, particles: Particles, partition: Partition, mesh: C
     `adj` (float64 device arrays) maps end-of-step sensitivities to start-of-step
     ones in place (mu / lam accumulate)."""
     ctx = ctx or _default()
-    rc = ctx.pfn("tb_adjoint_step", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_adjoint_step", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                     _ref(adj.struct()))
     ctx.check(rc, "adjoint_step")
 
 
-def tape_bytes(mesh: CartesianMesh, n: int, dtype, nsteps: int, checkpoint_every: int, apic: bool = False) -> int:
+def tape_bytes(mesh: CartesianMesh, n: int, dtype, nsteps: int, checkpoint_every: int, apic: bool = False,
+               x64: bool = False) -> int:
     """Device bytes a tape holds (forward and backward pass) for `n` particles of
-    element type `dtype` over `nsteps` steps, checkpointed every
-    `checkpoint_every` steps (1: the whole tape, no recompute in the backward)."""
+    element type `dtype` (with FP64 positions if `x64`) over `nsteps` steps,
+    checkpointed every `checkpoint_every` steps (1: the whole tape, no recompute
+    in the backward)."""
     lib = _abi.load_library()
     b = int(lib.tb_tape_bytes(C.byref(mesh.struct()), int(n), int(np.dtype(dtype).itemsize), int(bool(apic)),
-                              int(nsteps), int(checkpoint_every)))
+                              int(bool(x64)), int(nsteps), int(checkpoint_every)))
     if b < 0:
         raise ValueError("tape_bytes: invalid arguments")
     return b
 
 
-def tape_slot_bytes(mesh: CartesianMesh, n: int, dtype, apic: bool = False) -> int:
+def tape_slot_bytes(mesh: CartesianMesh, n: int, dtype, apic: bool = False, x64: bool = False) -> int:
     """Device bytes one step of the whole tape holds (state, grid, partition)."""
-    return tape_bytes(mesh, n, dtype, 1, 1, apic)
+    return tape_bytes(mesh, n, dtype, 1, 1, apic, x64)
 
 
 def choose_checkpoint_every(mesh: CartesianMesh, n: int, dtype, nsteps: int, apic: bool = False,
-                            device=None, budget: float = 0.6, fallback: int = 20) -> int:
+                            device=None, budget: float = 0.6, fallback: int = 20, x64: bool = False) -> int:
     """1 (the whole tape in device memory) when it takes at most `budget` of the
     device's free memory, else `fallback`."""
     import torch
     free, _ = torch.cuda.mem_get_info(device)
-    return 1 if tape_bytes(mesh, n, dtype, nsteps, 1, apic) <= budget * free else fallback
+    return 1 if tape_bytes(mesh, n, dtype, nsteps, 1, apic, x64) <= budget * free else fallback
 
 
 def tape_forward(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params,
@@ -287,7 +289,7 @@ def tape_forward(grid: Grid, particles: Particles, partition: Partition, mesh: C
     `checkpoint_every` steps; 1 keeps every step's state, grid and partition (the
     whole tape), so tape_backward runs no forward step."""
     ctx = ctx or _default()
-    rc = ctx.pfn("tb_tape_forward", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_tape_forward", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                     _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                     int(nsteps), int(checkpoint_every))
     ctx.check(rc, "tape_forward")
@@ -298,7 +300,7 @@ def tape_backward(grid: Grid, particles: Particles, partition: Partition, mesh: 
     """Sensitivities to the final state (in `adj`) -> sensitivities to the step-0
     state; `particles` is restored to the step-0 state."""
     ctx = ctx or _default()
-    rc = ctx.pfn("tb_tape_backward", particles)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
+    rc = ctx.pfn("tb_tape_backward", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                      _ref(partition.struct()), _ref(grid.struct()), _ref(params),
                                                      _ref(adj.struct()))
     ctx.check(rc, "tape_backward")
@@ -321,7 +323,8 @@ def rollout_grad(particles: Particles, mesh: CartesianMesh, params, nsteps: int,
     D, n = particles.dim, particles.n
     if checkpoint_every is None:
         checkpoint_every = choose_checkpoint_every(mesh, n, particles.dtype, nsteps,
-                                                   params.transfer == _abi.TB_TRANSFER_APIC, particles.device)
+                                                   params.transfer == _abi.TB_TRANSFER_APIC, particles.device,
+                                                   x64=getattr(particles, "x64", False))
     part = Partition(mesh, n, backend="torch", device=particles.device or "cuda")
     grid = Grid(mesh, particles.dtype, backend="torch", device=particles.device or "cuda")
     tape_forward(grid, particles, part, mesh, params, nsteps, checkpoint_every, ctx=ctx)
@@ -350,7 +353,8 @@ class RolloutFunction:
         import torch
         if checkpoint_every is None:
             checkpoint_every = choose_checkpoint_every(mesh, particles.n, particles.dtype, nsteps,
-                                                       params.transfer == _abi.TB_TRANSFER_APIC, v0.device)
+                                                       params.transfer == _abi.TB_TRANSFER_APIC, v0.device,
+                                                       x64=getattr(particles, "x64", False))
 
         class _F(torch.autograd.Function):
             @staticmethod

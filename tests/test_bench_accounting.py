@@ -60,3 +60,18 @@ def test_config_bytes(bench, s, sx):
     pp, pn = bench.config_bytes(s, sx, apic=True)
     assert pp == bench.step_bytes(s, sx)[0] + 18 * s - 3 * s
     assert pn == bench.step_bytes(s, sx)[1] - 3 * s
+
+
+def test_fd_summary_normalises_by_field_rms(bench):
+    """fd_summary: per form the largest per-direction relative error and the
+    largest error over the field's RMS derivative."""
+    checks = [{"field": "v", "fd": 1.0, "adjoint_f64": 1.0, "adjoint_x64": 1.0001, "adjoint_f32": 1.001},
+              {"field": "v", "fd": 0.01, "adjoint_f64": 0.01, "adjoint_x64": 0.0101, "adjoint_f32": 0.011}]
+    for ch in checks:
+        for f in ("f64", "x64", "f32"):
+            ch[f"rel_err_{f}"] = abs(ch[f"adjoint_{f}"] - ch["fd"]) / abs(ch["fd"])
+    out = bench.fd_summary(checks, 2)
+    rms = ((1.0 + 1e-4) / 2) ** 0.5
+    assert abs(out["max_rel_err_x64"] - 0.01) < 1e-12
+    assert abs(out["max_err_over_rms_x64"] - 1e-4 / rms) < 1e-12
+    assert out["max_rel_err_fp32_tape"] == out["max_rel_err_x64"]
