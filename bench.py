@@ -686,6 +686,50 @@ def dambreak_adjoint_leg(tb, runtime, ctx, scale: int = 2, fd_scale: int = 4, fo
                          "directions": checks}}
 
 
+def kernel_case(tb, runtime, ctx, spec: str, steps: int, warmup: int) -> dict:
+    """One scene's steps alone, the workload of the per-kernel profiler
+    captures: SCENE:SCALE[:FORM][:adjoint] (FORM x64, f32 or f64; default x64).
+    Without `adjoint`: `warmup` steps, then `steps` steps in one call. With it: a
+    whole tape of warmup + steps steps (interval 1), then its backward pass
+    (only the adjoint kernels). Prints each kernel family's device time."""
+    parts = spec.split(":")
+    name, scale = parts[0], int(parts[1]) if len(parts) > 1 else 1
+    form = next((q for q in parts[2:] if q in FORMS), "x64")
+    adjoint = "adjoint" in parts[2:]
+    if name == "dambreak3d":
+        sc = tb.scenes.dambreak3d(scale=scale, particles=False)
+    else:
+        sc = getattr(tb.scenes, name)(scale=scale)
+    mesh, prm = sc.mesh, sc.params
+    P = _form_particles(tb, runtime, ctx, sc, form)
+    dtype = FORMS[form][0]
+    part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+    G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda")
+    if adjoint:
+        import torch
+        runtime.tape_forward(G, P, part, mesh, prm, warmup + steps, 1, ctx=ctx)
+        adj = tb.Adjoint(P.n, mesh.dim, backend="torch", device="cuda", lame=P.mu is not None,
+                         apic=prm.transfer == tb._abi.TB_TRANSFER_APIC)
+        gen = torch.Generator(device="cuda").manual_seed(5)
+        adj.x.copy_(torch.randn(adj.x.shape, generator=gen, device="cuda", dtype=torch.float64))
+        ctx.profile(True)
+        runtime.tape_backward(G, P, part, mesh, prm, adj, ctx=ctx)
+        kt = ctx.profile_read()
+        ctx.profile(False)
+        nsteps = warmup + steps
+    else:
+        runtime.step(G, P, part, mesh, prm, warmup, ctx=ctx)
+        ctx.synchronize()
+        ctx.profile(True)
+        runtime.step(G, P, part, mesh, prm, steps, ctx=ctx)
+        kt = ctx.profile_read()
+        ctx.profile(False)
+        nsteps = steps
+    return {"kernel_case": spec, "n_particles": P.n, "form": form, "adjoint": adjoint, "steps": nsteps,
+            "kernels_ms_per_step": {k: v[1] / nsteps for k, v in sorted(kt.items())},
+            "launches_per_step": {k: v[0] / nsteps for k, v in sorted(kt.items())}}
+
+
 def fullsize_oracle_check(tb, runtime, ctx, sc, nsteps: int = 3) -> dict:
     """The plain FP64 device step against the FP64 oracle (the OpenMP
     restatement of the reference's CPU step) on the full headline scene,
@@ -765,6 +809,8 @@ def main():
     ap.add_argument("--no-oracle-check", action="store_true", help="skip the full-size FP64 oracle check")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed FP32 leg (for profiler captures); prints a reduced line")
+    ap.add_argument("--kernel-case", default=None, metavar="SCENE:SCALE[:FORM][:adjoint]",
+                    help="only this scene's steps (or its tape's backward pass), for per-kernel profiler captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -788,6 +834,13 @@ def main():
     tb = load_package()
     from tesserae_b200 import runtime
     ctx = runtime.Context(local)
+
+    if args.kernel_case:
+        if rank == 0:
+            print(json.dumps(kernel_case(tb, runtime, ctx, args.kernel_case, args.steps, args.warmup)), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     sc = tb.scenes.cube3d(scale=args.scale)
     mesh, prm = sc.mesh, sc.params
