@@ -507,11 +507,14 @@ def _form_particles(tb, runtime, ctx, sc, name, device="cuda"):
 
 
 def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: int, peak: float,
-               per_particle=(), apic=False) -> dict:
+               per_particle=(), apic=False, sparse_forms=()) -> dict:
     """One configuration: device time per step of each precision form (a fused
     call of `steps` steps after `warmup`), its per-kernel split, the whole-step
     and dominant-kernel roofline fractions, and the FP32 form's error against
-    the FP64 form after `acc_steps` steps from the same initial state."""
+    the FP64 form after `acc_steps` steps from the same initial state. For each
+    form in `sparse_forms`, the same timing on a block-sparse grid (SpGrid,
+    its sparsity updated every step), its grid memory against the dense grid's,
+    and its state after `steps` steps against the dense grid's."""
     import torch
     mesh, prm = sc.mesh, sc.params
     out = {"n_particles": None, "steps": steps, "warmup": warmup, "forms": {}}
@@ -563,6 +566,36 @@ def config_leg(tb, runtime, ctx, sc, forms, steps: int, warmup: int, acc_steps: 
                         "finite": bool(torch.isfinite(P.x).all() and torch.isfinite(P.v).all())}
         del part, G, P
         torch.cuda.empty_cache()
+    for name in sparse_forms:
+        dtype = FORMS[name][0]
+        s_b = np.dtype(dtype).itemsize
+        nfield = 1 + 4 * mesh.dim
+        res = {}
+        for sparse in (False, True):
+            P = _form_particles(tb, runtime, ctx, sc, name)
+            part = tb.Partition(mesh, P.n, backend="torch", device="cuda")
+            G = tb.generate_grid(mesh, dtype, backend="torch", device="cuda", sparse=sparse)
+            runtime.step(G, P, part, mesh, prm, warmup, ctx=ctx)
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            runtime.step(G, P, part, mesh, prm, steps, ctx=ctx)
+            e1.record()
+            torch.cuda.synchronize()
+            ctx.synchronize()
+            res[sparse] = {"ms": e0.elapsed_time(e1) / steps, "x": P.x.double().clone(),
+                           "nodes": G.capacity if sparse else mesh.nnodes}
+            del part, G, P
+            torch.cuda.empty_cache()
+        dx = float(torch.linalg.vector_norm(res[True]["x"] - res[False]["x"]) /
+                   torch.linalg.vector_norm(res[False]["x"]))
+        out.setdefault("sparse_grid", {})[name] = {
+            "ms_per_step": res[True]["ms"], "dense_ms_per_step": res[False]["ms"],
+            "grid_bytes": res[True]["nodes"] * nfield * s_b, "dense_grid_bytes": mesh.nnodes * nfield * s_b,
+            "rel_err_x_vs_dense": dx, "steps": warmup + steps,
+            "note": "SpGrid (generate_grid(SpArray, ...)): sparsity updated on the device every step; "
+                    "field arrays sized for the initial active blocks x 1.5"}
     ref = finals.get("f64")
     if ref is not None:
         def rel(a, b):
@@ -996,7 +1029,7 @@ def main():
         if cname == "clusters3d":
             csc = tb.scenes.clusters3d(scale=cs)
             configs[cname] = config_leg(tb, runtime, ctx, csc, ("x64", "f64"), steps=10, warmup=3,
-                                        acc_steps=csc.nsteps, peak=peak, per_particle=("m",))
+                                        acc_steps=csc.nsteps, peak=peak, per_particle=("m",), sparse_forms=("x64",))
             configs[cname]["workload"] = ("clusters3d: 512^3 cells, 64 Gaussian clusters (sigma 0.02), lognormal "
                                           "masses, Neo-Hookean E=1e5 nu=0.35, dt=2.5e-5; block order")
         elif cname == "sphere3d":

@@ -48,7 +48,7 @@ extern "C" {
 #define TB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
 #define TB_ERR_CAPACITY (-3)    /* a size exceeds the Int32 capacity of the partition */
 #define TB_ERR_UNSUPPORTED (-4) /* combination not supported (e.g. dim 1) */
-#define TB_ERR_DEVICE (-5)      /* a kernel reported an error status (e.g. bounded wait expired) */
+#define TB_ERR_DEVICE (-5)      /* a kernel reported an error status (e.g. a window left its block tile) */
 
 /* Uniform Cartesian mesh (reference: src/Mesh/cartesian.jl:38-102).
  * xmin, h and h_inv are given in FP64 exactly as the caller's mesh stores them;
@@ -110,13 +110,28 @@ typedef struct tb_particles {
 } tb_particles;
 
 /* Grid fields as SoA component pointers (scalar type T), each of length
- * prod(n_nodes), column-major node order (src/Grids/grid.jl:70-78). */
+ * prod(n_nodes), column-major node order (src/Grids/grid.jl:70-78).
+ *
+ * Block-sparse grid (SpGrid, src/Grids/sparray.jl, spindices.jl): with
+ * block_numbering set, the fields store only the active node blocks (blocks of
+ * (1 << mesh.block_log2)^dim nodes, node block of node i = i >> block_log2 per
+ * axis, nblocks(mesh) of them): node I of block B lives at
+ *   (block_numbering[B] - 1) * blocklength + (I's column-major index inside B)
+ * (the reference's storageindex), and a node of an inactive block
+ * (block_numbering[B] == 0) reads as zero and takes no scatter.
+ * tb_update_sparsity_* fills block_numbering, active_blocks and *nactive from
+ * the particle positions; the fused steps update them every step. Leave the
+ * four fields zero for a dense grid. */
 typedef struct tb_grid {
     void* m;
     void* mv[3];
     void* f[3];
     void* v[3];
     void* vn[3];
+    int32_t* block_numbering; /* [nblocks(mesh)] device: 0 inactive, k >= 1 storage block k */
+    int32_t* active_blocks;   /* [nblocks(mesh)] device: 1-based id of the node block stored as block k at [k-1] */
+    int32_t* nactive;         /* [2] device: active node blocks at [0] (scratch at [1]) */
+    int64_t capacity;         /* nodes each field array holds (a multiple of blocklength) */
 } tb_grid;
 
 /* The GPUBlockStrategy arrays (src/Parallel/gpu_block_strategy.jl:10-22). */
@@ -204,6 +219,22 @@ int32_t tb_bin_particles_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particle
                              tb_partition* partition, int64_t* nactive, int64_t* nassigned);
 int32_t tb_bin_particles_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
                              tb_partition* partition, int64_t* nactive, int64_t* nassigned);
+
+/* ---- update_sparsity!(grid::SpGrid, particles.x) -----------------------
+ * reference: src/Grids/sparsity.jl:19-60 (particle-driven update: blocks that
+ * hold a particle inside the mesh, each with its 3^dim neighbourhood of node
+ * blocks, numbered in ascending block order). Bins the particles into
+ * `partition` (as tb_bin_particles_*), then numbers the active node blocks of
+ * the sparse `grid`. Synchronises once and returns in *nstored the nodes each
+ * field must hold (active blocks x blocklength); TB_ERR_CAPACITY if that exceeds
+ * grid.capacity (the numbering is written all the same, so a caller can grow
+ * the fields and go on). */
+int32_t tb_update_sparsity_f64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                               tb_partition* partition, tb_grid* grid, int64_t* nstored);
+int32_t tb_update_sparsity_f32(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                               tb_partition* partition, tb_grid* grid, int64_t* nstored);
+int32_t tb_update_sparsity_f32x64(tb_ctx* ctx, const tb_mesh* mesh, const tb_particles* particles,
+                                  tb_partition* partition, tb_grid* grid, int64_t* nstored);
 
 /* ---- @P2G scatter half: m, mv, f (assigned targets are zeroed first) ----
  * reference: src/Transfer/gpu.jl:196-223 (block-scheduled) with the sums of

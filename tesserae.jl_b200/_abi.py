@@ -66,7 +66,8 @@ class tb_particles(C.Structure):
 
 
 class tb_grid(C.Structure):
-    _fields_ = [("m", VP), ("mv", VP * 3), ("f", VP * 3), ("v", VP * 3), ("vn", VP * 3)]
+    _fields_ = [("m", VP), ("mv", VP * 3), ("f", VP * 3), ("v", VP * 3), ("vn", VP * 3),
+                ("block_numbering", VP), ("active_blocks", VP), ("nactive", VP), ("capacity", C.c_int64)]
 
 
 class tb_partition(C.Structure):
@@ -130,6 +131,9 @@ SIGNATURES = [
     ("tb_bin_particles_noalloc", I32, [P(tb_mesh), P(tb_particles), I32, P(tb_partition), VP, P(I64), P(I64),
                                        C.c_char_p, I32]),
     ("tb_tape_bytes", I64, [P(tb_mesh), I64, I32, I32, I32, I32, I32]),
+    ("tb_update_sparsity_f64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(I64)]),
+    ("tb_update_sparsity_f32", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(I64)]),
+    ("tb_update_sparsity_f32x64", I32, [VP, P(tb_mesh), P(tb_particles), P(tb_partition), P(tb_grid), P(I64)]),
     ("tb_tape_release", I32, [VP]),
 ]
 for _p in ("f64", "f32"):

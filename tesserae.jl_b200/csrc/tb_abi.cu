@@ -88,6 +88,17 @@ struct tb_ctx {
     unsigned long long* sort_scratch = nullptr;
     long long sort_scratch_cap = 0;
     // touched node blocks of the last two transfers (sparse grid zero/update)
+    // sparse grid numbering scratch
+    int* sp_act = nullptr;
+    long long sp_act_cap = 0;
+    int* sp_off = nullptr;
+    long long sp_off_cap = 0;
+    int* sp_cur = nullptr;
+    long long sp_cur_cap = 0;
+    unsigned long long* sp_part = nullptr;
+    long long sp_part_cap = 0;
+    int* sp_tot = nullptr;
+    long long sp_tot_cap = 0;
     unsigned char* touched_cur = nullptr;
     unsigned char* touched_prev = nullptr;
     int* touched_list = nullptr;  // [nblocks] blocks with cur or prev set, count in touched_count
@@ -249,7 +260,7 @@ int make_pview(tb_ctx* c, const tb_particles* p, int dim, bool need_state, bool 
 }
 
 template <class T>
-int make_gview(tb_ctx* c, const tb_grid* g, int dim, GView<T>& G) {
+int make_gview(tb_ctx* c, const tb_grid* g, int dim, GView<T>& G, int block_log2 = 0) {
     if (!g) return fail(c, TB_ERR_ARG, "grid is NULL");
     std::memset(&G, 0, sizeof G);
     G.m = static_cast<T*>(g->m);
@@ -261,6 +272,31 @@ int make_gview(tb_ctx* c, const tb_grid* g, int dim, GView<T>& G) {
         G.vn[d] = static_cast<T*>(g->vn[d]);
         if (!G.mv[d] || !G.f[d] || !G.v[d] || !G.vn[d]) return fail(c, TB_ERR_ARG, "grid component %d is NULL", d);
     }
+    if (g->block_numbering || g->active_blocks || g->nactive) {  // block-sparse grid
+        if (!g->block_numbering || !g->active_blocks || !g->nactive)
+            return fail(c, TB_ERR_ARG, "a sparse grid needs block_numbering, active_blocks and nactive");
+        const long long bl = 1ll << (block_log2 * dim);
+        if (g->capacity < 0 || g->capacity % bl != 0)
+            return fail(c, TB_ERR_ARG, "sparse grid capacity %lld is not a multiple of the block length %lld",
+                        (long long)g->capacity, bl);
+        G.bnum = g->block_numbering;
+        G.blist = g->active_blocks;
+        G.nact = g->nactive;
+        G.cap = g->capacity;
+        G.L = block_log2;
+    }
+    return TB_OK;
+}
+
+int sparse_scratch(tb_ctx* c, long long nb, SparseScratch& sc) {
+    cudaError_t e;
+    if ((e = grow(c->sp_act, c->sp_act_cap, nb)) != cudaSuccess ||
+        (e = grow(c->sp_off, c->sp_off_cap, nb + 1)) != cudaSuccess ||
+        (e = grow(c->sp_cur, c->sp_cur_cap, nb)) != cudaSuccess ||
+        (e = grow(c->sp_part, c->sp_part_cap, scan_tiles(int(nb)))) != cudaSuccess ||
+        (e = grow(c->sp_tot, c->sp_tot_cap, 2)) != cudaSuccess)
+        return cuda_fail(c, e, "cudaMalloc sparse grid scratch");
+    sc = SparseScratch{c->sp_act, c->sp_off, c->sp_cur, c->sp_part, c->sp_tot};
     return TB_OK;
 }
 
@@ -306,6 +342,9 @@ int check_device_status(tb_ctx* c) {
         if (h & ERR_WLS_SINGULAR) why += " singular WLS moment matrix;";
         if (h & ERR_REORDER_OUTSIDE)
             why += " reorder_particles!: some particles are outside the mesh and were not assigned to any block;";
+        if (h & ERR_INACTIVE_NODE)
+            why += " @P2G: a support node of an inactive sparse-grid block (run update_sparsity for these positions);";
+        if (h & ERR_SPGRID_CAPACITY) why += " the sparse grid's active blocks exceed its field arrays' capacity;";
         return fail(c, TB_ERR_DEVICE, "kernel reported:%s", why.c_str());
     }
     return TB_OK;
@@ -389,6 +428,12 @@ int touched_buffers(tb_ctx* c, long long nb) {
 template <int D, class T, int BW>
 cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, const GView<T>& G,
                           const Scalars<T>& S, const BinBuffers& B, const LaunchCfg& cfg) {
+    if (G.bnum) {  // block-sparse grid: zero the stored nodes, scatter
+        c->grid_sparse_ok = false;
+        c->grid_zeroed = false;
+        cudaError_t e = launch_grid_zero<D, T>(M, G, cfg);
+        return e == cudaSuccess ? launch_p2g<D, T, BW>(M, P, G, S, B, cfg) : e;
+    }
     const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks;
     // after a grid half that zeroed its blocks once read, every P2G target is zero
     const bool zeroed = known && c->grid_zeroed;
@@ -418,6 +463,7 @@ cudaError_t p2g_with_zero(tb_ctx* c, const DMesh<D, T>& M, const PView<T>& P, co
 template <int D, class T, int BW>
 cudaError_t grid_update_sparse_or_dense(tb_ctx* c, const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& S,
                                         const LaunchCfg& cfg, bool zero_after = false) {
+    if (G.bnum) return launch_grid_update<D, T>(M, G, S, cfg);  // over the stored nodes
     const bool known = c->grid_sparse_ok && c->grid_key == G.m && c->grid_nblocks == M.nblocks &&
                        !c->grid_dense_pending;
     c->grid_dense_pending = false;
@@ -442,7 +488,7 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
     int rc;
     if ((rc = make_pview<T>(c, p, D, true, prm->transfer == TB_TRANSFER_APIC, P, x64, prm->material)) != TB_OK)
         return rc;
-    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G, m->block_log2)) != TB_OK) return rc;
     BinBuffers B;
     if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
     const LaunchCfg cfg = cfg_of(c);
@@ -467,10 +513,15 @@ int run_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part, t
     // step s + 1 (the count pass of its binning); the last step does not, so the
     // partition left to the caller is the last step's own.
     bool counted = false;
+    SparseScratch SC{};
+    if (G.bnum && do_bin && (rc = sparse_scratch(c, M.nblocks, SC)) != TB_OK) return rc;
     for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
         if (do_bin) {
             if (counted) e = launch_bin_rest(M.nblocks, P.n, B, cfg);
             else e = x64 ? launch_bin<D, double>(M64, xs64, P.n, B, cfg) : launch_bin<D, T>(M, xs, P.n, B, cfg);
+            // a sparse grid follows the particles: update_sparsity! every step
+            if (e == cudaSuccess && G.bnum)
+                e = launch_sparsity(D, M.nb, M.nblocks, B, SC, g->block_numbering, g->active_blocks, g->nactive, cfg);
         }
         const bool count_next = do_bin && do_g2p && s + 1 < nsteps;
         counted = false;
@@ -568,6 +619,62 @@ int do_bin_only(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition
     return TB_OK;
 }
 
+// update_sparsity!(grid, particles.x): bin, number the active node blocks, read
+// the count back (src/Grids/sparsity.jl:19-60; the reference also reads its
+// active count back to size SpArray.data) and zero the stored fields.
+template <int D, class T>
+int sparsity_impl(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part, tb_grid* g,
+                  int64_t* nstored, bool x64) {
+    PView<T> P;
+    int rc;
+    if ((rc = make_pview<T>(c, p, D, false, false, P, x64)) != TB_OK) return rc;
+    if (!g || !g->block_numbering || !g->active_blocks || !g->nactive)
+        return fail(c, TB_ERR_ARG, "update_sparsity needs a sparse grid (block_numbering, active_blocks, nactive)");
+    const auto M = make_dmesh<D, T>(*m);
+    BinBuffers B;
+    if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
+    SparseScratch SC;
+    if ((rc = sparse_scratch(c, M.nblocks, SC)) != TB_OK) return rc;
+    const LaunchCfg cfg = cfg_of(c);
+    const T* xs[3] = {P.x[0], P.x[1], D == 3 ? P.x[2] : P.x[1]};
+    const double* xs64[3] = {P.x64[0], P.x64[1], D == 3 ? P.x64[2] : P.x64[1]};
+    cudaError_t e = x64 ? launch_bin<D, double>(make_dmesh<D, double>(*m), xs64, P.n, B, cfg)
+                        : launch_bin<D, T>(M, xs, P.n, B, cfg);
+    if (e == cudaSuccess)
+        e = launch_sparsity(D, M.nb, M.nblocks, B, SC, g->block_numbering, g->active_blocks, g->nactive, cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "update_sparsity launch");
+    e = cudaMemcpyAsync(c->h_totals, g->nactive, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "sparse grid count readback");
+    const long long need = (long long)c->h_totals[0] << (m->block_log2 * D);
+    if (nstored) *nstored = need;
+    if (need > g->capacity)
+        return fail(c, TB_ERR_CAPACITY, "the sparse grid needs %lld nodes per field, its arrays hold %lld", need,
+                    (long long)g->capacity);
+    // the renumbered storage starts zero (SpArray data after update_sparsity!)
+    void* fields[1 + 4 * 3] = {g->m};
+    for (int d = 0; d < D; ++d) {
+        fields[1 + d] = g->mv[d];
+        fields[1 + D + d] = g->f[d];
+        fields[1 + 2 * D + d] = g->v[d];
+        fields[1 + 3 * D + d] = g->vn[d];
+    }
+    for (int i = 0; i < 1 + 4 * D && e == cudaSuccess; ++i)
+        e = fields[i] ? cudaMemsetAsync(fields[i], 0, sizeof(T) * size_t(need), c->stream) : cudaErrorInvalidValue;
+    if (e != cudaSuccess) return cuda_fail(c, e, "sparse grid zero fill");
+    return TB_OK;
+}
+
+template <class T>
+int do_update_sparsity(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part, tb_grid* g,
+                       int64_t* nstored, bool x64 = false) {
+    int rc;
+    if ((rc = check_ctx(c)) != TB_OK) return rc;
+    if ((rc = check_mesh(c, m)) != TB_OK) return rc;
+    if (m->dim == 3) return sparsity_impl<3, T>(c, m, p, part, g, nstored, x64);
+    return sparsity_impl<2, T>(c, m, p, part, g, nstored, x64);
+}
+
 template <class T>
 int do_weights(tb_ctx* c, const tb_mesh* m, const tb_particles* p, const tb_step_params* prm, tb_weights* w) {
     int rc;
@@ -598,7 +705,7 @@ int do_grid_update(tb_ctx* c, const tb_mesh* m, tb_grid* g, const tb_step_params
     const LaunchCfg cfg = cfg_of(c);
     cudaError_t e;
     GView<T> G;
-    if ((rc = make_gview<T>(c, g, m->dim, G)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, m->dim, G, m->block_log2)) != TB_OK) return rc;
     c->grid_sparse_ok = false;  // a standalone call cannot know which nodes are non-zero
     if (m->dim == 3)
         e = grid_update_sparse_or_dense<3, T, 4>(c, make_dmesh<3, T>(*m), G, make_scalars<T>(*prm), cfg);
@@ -619,7 +726,7 @@ int do_g2p_direct(tb_ctx* c, const tb_mesh* m, const tb_grid* g, tb_particles* p
     if ((rc = make_pview<T>(c, p, m->dim, true, prm->transfer == TB_TRANSFER_APIC, P, false, prm->material)) !=
         TB_OK)
         return rc;
-    if ((rc = make_gview<T>(c, g, m->dim, G)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, m->dim, G, m->block_log2)) != TB_OK) return rc;
     const LaunchCfg cfg = cfg_of(c);
     cudaError_t e = (m->dim == 3) ? launch_g2p_direct<3, T>(make_dmesh<3, T>(*m), G, P, make_scalars<T>(*prm), cfg)
                                   : launch_g2p_direct<2, T>(make_dmesh<2, T>(*m), G, P, make_scalars<T>(*prm), cfg);
@@ -805,7 +912,8 @@ int g2p2g_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* part,
     GView<T> G;
     int rc;
     if ((rc = make_pview<T>(c, p, D, true, false, P, x64, prm->material)) != TB_OK) return rc;
-    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G, m->block_log2)) != TB_OK) return rc;
+    if (G.bnum) return fail(c, TB_ERR_UNSUPPORTED, "g2p2g runs on a dense grid");
     BinBuffers B;
     if ((rc = bin_buffers(c, part, P.n, M.nblocks, B)) != TB_OK) return rc;
     if ((rc = touched_buffers(c, M.nblocks)) != TB_OK) return rc;
@@ -936,7 +1044,8 @@ int adjoint_impl(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* par
     GradGrid GB;
     const bool apic = prm->transfer == TB_TRANSFER_APIC;
     if ((rc = make_pview<T>(c, p, D, true, apic, P, x64, prm->material)) != TB_OK) return rc;
-    if ((rc = make_gview<T>(c, g, D, G)) != TB_OK) return rc;
+    if ((rc = make_gview<T>(c, g, D, G, m->block_log2)) != TB_OK) return rc;
+    if (G.bnum) return fail(c, TB_ERR_UNSUPPORTED, "the reverse step runs on a dense grid");
     if ((rc = make_adjview(c, adj, D, P.n, A, apic)) != TB_OK) return rc;
     if ((rc = grad_grid(c, D, M.nnodes, GB)) != TB_OK) return rc;
     if (cudaError_t ce = grow(c->adj_coef, c->adj_coef_cap, std::max<long long>(1, P.n) * (2 * D + D * D));
@@ -975,6 +1084,8 @@ int do_adjoint_step(tb_ctx* c, const tb_mesh* m, tb_particles* p, tb_partition* 
     if ((rc = check_ctx(c)) != TB_OK || (rc = check_mesh(c, m)) != TB_OK || (rc = check_adjoint_params(c, prm)) != TB_OK)
         return rc;
     if (x64 && (rc = check_x64_adjoint(c, m, prm)) != TB_OK) return rc;
+    if (g && (g->block_numbering || g->active_blocks || g->nactive))
+        return fail(c, TB_ERR_UNSUPPORTED, "the reverse step runs on a dense grid");
     return adjoint_dispatch<T>(c, m, p, part, g, prm, adj, true, nullptr, x64);
 }
 
@@ -1240,6 +1351,11 @@ void tb_destroy(tb_ctx* c) {
     cudaFree(c->partials);
     cudaFree(c->sort_scratch);
     cudaFree(c->roll_buf);
+    cudaFree(c->sp_act);
+    cudaFree(c->sp_off);
+    cudaFree(c->sp_cur);
+    cudaFree(c->sp_part);
+    cudaFree(c->sp_tot);
     cudaFree(c->touched_cur);
     cudaFree(c->touched_prev);
     cudaFree(c->touched_list);
@@ -1318,6 +1434,18 @@ int32_t tb_update_weights_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p
     return do_weights<float>(c, m, p, prm, w);
 }
 
+int32_t tb_update_sparsity_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part, tb_grid* g,
+                               int64_t* nstored) {
+    return do_update_sparsity<double>(c, m, p, part, g, nstored);
+}
+int32_t tb_update_sparsity_f32(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part, tb_grid* g,
+                               int64_t* nstored) {
+    return do_update_sparsity<float>(c, m, p, part, g, nstored);
+}
+int32_t tb_update_sparsity_f32x64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part,
+                                  tb_grid* g, int64_t* nstored) {
+    return do_update_sparsity<float>(c, m, p, part, g, nstored, true);
+}
 int32_t tb_bin_particles_f64(tb_ctx* c, const tb_mesh* m, const tb_particles* p, tb_partition* part,
                              int64_t* nactive, int64_t* nassigned) {
     return do_bin_only<double>(c, m, p, part, nactive, nassigned);

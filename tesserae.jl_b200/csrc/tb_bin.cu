@@ -468,7 +468,60 @@ __global__ void __launch_bounds__(FIXW_THREADS) bin_fixup_warp_kernel(const int*
 
 inline unsigned grid_for(long long n, int threads) { return unsigned((n + threads - 1) / threads); }
 
+// ---- sparse grid numbering ----------------------------------------------
+// act[B] = 1 for every node block B within one block per axis of a block that
+// holds particles (act zeroed before). Several threads may store the same 1.
+template <int D>
+__global__ void __launch_bounds__(128) sparse_mark_kernel(const int* __restrict__ totals,
+                                                          const int* __restrict__ blocklist, int3 nb,
+                                                          int* __restrict__ act) {
+    const int nactive = totals[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nactive; i += gridDim.x * blockDim.x) {
+        const int b = blocklist[i] - 1;
+        const int bx = b % nb.x, by = (b / nb.x) % nb.y, bz = (D == 3) ? b / (nb.x * nb.y) : 0;
+        for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = bx + dx, y = by + dy, z = bz + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= nb.x || y >= nb.y || (D == 3 && z >= nb.z)) continue;
+                    act[x + nb.x * (y + nb.y * z)] = 1;
+                }
+    }
+}
+
+// bnum[B] = (rank of B among the active blocks) + 1, or 0; the count to nact[0].
+__global__ void __launch_bounds__(256) sparse_number_kernel(const int* __restrict__ act,
+                                                            const int* __restrict__ offsets, int nb,
+                                                            const int* __restrict__ totals, int* __restrict__ bnum,
+                                                            int* __restrict__ nact) {
+    for (int B = blockIdx.x * blockDim.x + threadIdx.x; B < nb; B += gridDim.x * blockDim.x) {
+        bnum[B] = act[B] ? offsets[B] + 1 : 0;
+        if (B == 0) nact[0] = totals[0];
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_sparsity(int dim, const int* nbv, int nblocks, const BinBuffers& b, const SparseScratch& sc,
+                            int* bnum, int* blist, int* nact, const LaunchCfg& cfg) {
+    cudaError_t e = cudaMemsetAsync(sc.act, 0, sizeof(int) * size_t(nblocks), cfg.stream);
+    if (e != cudaSuccess) return e;
+    KernelScope ks(cfg, "sparsity");
+    const int3 nb = make_int3(nbv[0], nbv[1], nbv[2]);
+    const int mgrid = std::max(1, std::min((nblocks + 127) / 128, cfg.num_sms * 8));
+    if (dim == 3) sparse_mark_kernel<3><<<mgrid, 128, 0, cfg.stream>>>(b.totals, b.blocklist, nb, sc.act);
+    else sparse_mark_kernel<2><<<mgrid, 128, 0, cfg.stream>>>(b.totals, b.blocklist, nb, sc.act);
+    // the binning's scan over the activity: offsets = ranks, blocklist = the active list
+    const int nt = scan_tiles(nblocks);
+    scan_reduce_kernel<<<nt, 256, 0, cfg.stream>>>(sc.act, nblocks, sc.partials);
+    scan_spine_kernel<<<1, 256, 0, cfg.stream>>>(sc.partials, nt);
+    scan_finalize_kernel<<<nt, 256, 0, cfg.stream>>>(sc.act, nblocks, sc.partials, sc.offsets, sc.cursors, blist,
+                                                     sc.totals);
+    sparse_number_kernel<<<std::max(1, std::min((nblocks + 255) / 256, cfg.num_sms * 8)), 256, 0, cfg.stream>>>(
+        sc.act, sc.offsets, nblocks, sc.totals, bnum, nact);
+    *cfg.launches += 5;
+    return cudaGetLastError();
+}
 
 template <int D, class T>
 cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,

@@ -23,7 +23,9 @@ enum : int {
     ERR_TILE_RANGE = 1,   // a support window left its block tile
     ERR_GIMP_LENGTH = 2,  // uGIMP requires 0 <= l <= h (gimp.jl:22)
     ERR_WLS_SINGULAR = 4,  // WLS moment matrix not invertible
-    ERR_REORDER_OUTSIDE = 8   // a reorder was due but particles lie outside the mesh
+    ERR_REORDER_OUTSIDE = 8,  // a reorder was due but particles lie outside the mesh
+    ERR_INACTIVE_NODE = 16,   // a scatter reached a node of an inactive block of a sparse grid
+    ERR_SPGRID_CAPACITY = 32  // a sparse grid's active blocks exceed its field arrays
 };
 
 // CTAs that share one block of the block list: the average particle count of
@@ -168,7 +170,57 @@ struct GView {
     T* f[3];
     T* v[3];
     T* vn[3];
+    // block-sparse grid (bnum set): node block numbering (0 inactive, k >= 1
+    // storage block k), the node block of each storage block (1-based ids),
+    // the active block count (device), the nodes the fields hold and log2 of
+    // the block edge
+    const int* bnum;
+    const int* blist;
+    const int* nact;
+    long long cap;
+    int L;
 };
+
+// Storage slot of node (x, y, z) (z = 0 in 2D): the column-major linear index
+// on a dense grid; on a block-sparse grid (src/Grids/spindices.jl storageindex)
+// (k - 1) blocklength + the node's column-major index inside its block, k the
+// block's storage number. -1: the block is inactive; -2: past the fields'
+// capacity.
+template <int D, class T, class MT>
+__device__ __forceinline__ long long grid_slot(const GView<T>& G, const MT& M, int x, int y, int z) {
+    if (!G.bnum) return (long long)x + (long long)M.n[0] * ((long long)y + (D == 3 ? (long long)M.n[1] * z : 0ll));
+    const int L = G.L, W = 1 << L, mk = W - 1;
+    const int B = (x >> L) + M.nb[0] * ((y >> L) + (D == 3 ? M.nb[1] * (z >> L) : 0));
+    const int k = G.bnum[B];
+    if (k <= 0) return -1;
+    const int q = (x & mk) + W * ((y & mk) + (D == 3 ? W * (z & mk) : 0));
+    const long long sl = (long long)(k - 1) * (D == 3 ? W * W * W : W * W) + q;
+    return sl < G.cap ? sl : -2;
+}
+
+// Adds one node's P2G sums (m, mv[D], f[D], gravity already in f) to the grid,
+// one atomic per non-zero value. A non-zero sum for a node that a sparse grid
+// does not store sets ERR_INACTIVE_NODE (update_sparsity! was not run for these
+// positions: src/Transfer/runtime.jl:152-161) or ERR_SPGRID_CAPACITY.
+template <int D, class T, class MT, class V>
+__device__ __forceinline__ void grid_add(const GView<T>& G, const MT& M, int* err, int x, int y, int z,
+                                         const V* val) {
+    bool any = val[0] != V(0);
+#pragma unroll
+    for (int c = 1; c < 1 + 2 * D; ++c) any = any || val[c] != V(0);
+    if (!any) return;
+    const long long sl = grid_slot<D>(G, M, x, y, z);
+    if (sl < 0) {
+        atomicOr(err, sl == -1 ? ERR_INACTIVE_NODE : ERR_SPGRID_CAPACITY);
+        return;
+    }
+    if (val[0] != V(0)) atomicAdd(G.m + sl, T(val[0]));
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        if (val[1 + d] != V(0)) atomicAdd(G.mv[d] + sl, T(val[1 + d]));
+        if (val[1 + D + d] != V(0)) atomicAdd(G.f[d] + sl, T(val[1 + D + d]));
+    }
+}
 
 // Step scalars, converted once to the state type.
 template <class T>

@@ -20,6 +20,16 @@ struct BinBuffers {
     int* totals;          // [2] device: nactive, nassigned
 };
 
+// Scratch of a sparse grid's numbering pass (one int per block each, the scan
+// partials, two totals).
+struct SparseScratch {
+    int* act;       // [nb] block activity
+    int* offsets;   // [nb+1]
+    int* cursors;   // [nb] (written by the shared scan, unused)
+    unsigned long long* partials;  // [ntiles]
+    int* totals;    // [2]
+};
+
 constexpr int SCAN_TILE = 1024;  // blocks per scan tile (256 threads x 4)
 
 inline int scan_tiles(int nb) { return (nb + SCAN_TILE - 1) / SCAN_TILE; }
@@ -61,6 +71,13 @@ template <int D, class T>
 cudaError_t launch_bin_count(const DMesh<D, T>& M, const T* const* x, long long n, const BinBuffers& b,
                              const LaunchCfg& cfg);
 cudaError_t launch_bin_rest(int nblocks, long long n, const BinBuffers& b, const LaunchCfg& cfg);
+
+// update_sparsity! from a binning pass: the node blocks within one block of a
+// block that holds particles (b.blocklist / b.totals), numbered in ascending
+// order into bnum (0 inactive, k >= 1), their 1-based ids into blist, the count
+// into nact[0] (src/Grids/sparsity.jl:19-60, 192-232).
+cudaError_t launch_sparsity(int dim, const int* nbv, int nblocks, const BinBuffers& b, const SparseScratch& sc,
+                            int* bnum, int* blist, int* nact, const LaunchCfg& cfg);
 
 // P2G scatter into a grid whose m, mv, f are already zero where it will add.
 template <int D, class T, int BW>

@@ -413,9 +413,8 @@ __global__ void __launch_bounds__(P2G_THREADS, (sizeof(T) == 4 && !GEN) ? 2 : 1)
         }
         // ---- flush the tile
         for (int t = tid; t < TN; t += NT) {
-            int node[3], rem = t;
+            int node[3] = {0, 0, 0}, rem = t;
             bool inside = true;
-            long long lin = 0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 node[d] = org[d] + rem % TS;
@@ -423,19 +422,12 @@ __global__ void __launch_bounds__(P2G_THREADS, (sizeof(T) == 4 && !GEN) ? 2 : 1)
                 inside = inside && node[d] >= 0 && node[d] < M.n[d];
             }
             if (!inside) continue;
-#pragma unroll
-            for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + node[d];
             double val[NC];
 #pragma unroll
             for (int c = 0; c < NC; ++c) val[c] = tile[c * TN + t];
 #pragma unroll
             for (int d = 0; d < D; ++d) val[1 + D + d] += double(s.g[d]) * val[0];
-            if (val[0] != 0.0) atomicAdd(G.m + lin, T(val[0]));
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-                if (val[1 + d] != 0.0) atomicAdd(G.mv[d] + lin, T(val[1 + d]));
-                if (val[1 + D + d] != 0.0) atomicAdd(G.f[d] + lin, T(val[1 + D + d]));
-            }
+            grid_add<D>(G, M, err, node[0], node[1], D == 3 ? node[2] : 0, val);
         }
         __syncthreads();
     }
@@ -1070,17 +1062,9 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
 #pragma unroll
                         for (int c = 0; c < NC; ++c) val[c] += double(part[idx + c * CSTR]);
                     }
-                long long lin = 0;
-#pragma unroll
-                for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + node[d];
 #pragma unroll
                 for (int d = 0; d < D; ++d) val[1 + D + d] += double(s.g[d]) * val[0];
-                if (val[0] != 0.0) atomicAdd(G.m + lin, T(val[0]));
-#pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    if (val[1 + d] != 0.0) atomicAdd(G.mv[d] + lin, T(val[1 + d]));
-                    if (val[1 + D + d] != 0.0) atomicAdd(G.f[d] + lin, T(val[1 + D + d]));
-                }
+                grid_add<D>(G, M, err, node[0], node[1], D == 3 ? node[2] : 0, val);
             }
         }
     };
@@ -1389,16 +1373,9 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
 #pragma unroll
                         for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
                     }
-                const long long lin =
-                    (long long)(org[0] + tx) + (long long)M.n[0] * ((org[1] + ty) + (long long)M.n[1] * (org[2] + tz));
 #pragma unroll
                 for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
-                if (val[0] != 0.0f) atomicAdd(G.m + lin, val[0]);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    if (val[1 + d] != 0.0f) atomicAdd(G.mv[d] + lin, val[1 + d]);
-                    if (val[4 + d] != 0.0f) atomicAdd(G.f[d] + lin, val[4 + d]);
-                }
+                grid_add<3>(G, M, err, org[0] + tx, org[1] + ty, org[2] + tz, val);
             }
         }
     }
@@ -1761,15 +1738,9 @@ __global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
                         for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
                     }
-                const long long lin = (long long)nx + (long long)M.n[0] * (ny + (long long)M.n[1] * nz);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
-                if (val[0] != T(0)) atomicAdd(G.m + lin, val[0]);
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    if (val[1 + d] != T(0)) atomicAdd(G.mv[d] + lin, val[1 + d]);
-                    if (val[4 + d] != T(0)) atomicAdd(G.f[d] + lin, val[4 + d]);
-                }
+                grid_add<3>(G, M, err, nx, ny, nz, val);
             }
         }
     }

@@ -26,8 +26,18 @@ __device__ __forceinline__ void load_x(const PView<T>& P, long long p, T* x) {
     for (int d = 0; d < D; ++d) x[d] = P.x[d][p];
 }
 
+// Stored nodes of a grid: every node of a dense grid; the active blocks' nodes
+// (up to the fields' capacity) of a sparse one.
 template <int D, class T>
-__global__ void __launch_bounds__(256) grid_zero_kernel(GView<T> G, long long nn) {
+__device__ __forceinline__ long long stored_nodes(const GView<T>& G, long long nnodes) {
+    if (!G.bnum) return nnodes;
+    const long long n = (long long)G.nact[0] << (G.L * D);
+    return n < G.cap ? n : G.cap;
+}
+
+template <int D, class T>
+__global__ void __launch_bounds__(256) grid_zero_kernel(GView<T> G, long long nnodes) {
+    const long long nn = stored_nodes<D>(G, nnodes);
     for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < nn; I += (long long)gridDim.x * blockDim.x) {
         G.m[I] = T(0);
 #pragma unroll
@@ -40,16 +50,36 @@ __global__ void __launch_bounds__(256) grid_zero_kernel(GView<T> G, long long nn
 
 template <int D, class T>
 __global__ void __launch_bounds__(256) grid_update_kernel(DMesh<D, T> M, GView<T> G, Scalars<T> s) {
-    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < M.nnodes;
+    const long long nn = stored_nodes<D>(G, M.nnodes);
+    for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < nn;
          I += (long long)gridDim.x * blockDim.x) {
-        const T m = G.m[I];
-        int idx[3];
-        long long r = I;
+        int idx[3] = {0, 0, 0};
+        if (G.bnum) {
+            // slot I of storage block k: node (B's origin) + (column-major local index)
+            const int W = 1 << G.L, k = int(I >> (G.L * D)), q = int(I & ((1ll << (G.L * D)) - 1));
+            const int B = G.blist[k] - 1;
+            const int bidx[3] = {B % M.nb[0], (B / M.nb[0]) % M.nb[1], D == 3 ? B / (M.nb[0] * M.nb[1]) : 0};
+            const int qidx[3] = {q % W, (q / W) % W, q / (W * W)};
+            bool inside = true;
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-            idx[d] = int(r % M.n[d]);
-            r /= M.n[d];
+            for (int d = 0; d < D; ++d) {
+                idx[d] = bidx[d] * W + qidx[d];
+                inside = inside && idx[d] < M.n[d];
+            }
+            if (!inside) {  // a block's nodes past the mesh edge
+#pragma unroll
+                for (int d = 0; d < D; ++d) G.vn[d][I] = G.v[d][I] = T(0);
+                continue;
+            }
+        } else {
+            long long r = I;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                idx[d] = int(r % M.n[d]);
+                r /= M.n[d];
+            }
         }
+        const T m = G.m[I];
 #pragma unroll
         for (int d = 0; d < D; ++d) {
             T vn = T(0), v = T(0);
@@ -259,22 +289,21 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
         const int s0 = offsets[b] + piece * nth, s1 = offsets[b + 1];
         int pnext = (s0 + tid < s1) ? perm[s0 + tid] : 1;
         for (int t = tid; t < TN; t += nth) {
-            int node[3], rem = t;
+            int node[3] = {0, 0, 0}, rem = t;
             bool inside = true;
-            long long lin = 0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 node[d] = org[d] + rem % TS;
                 rem /= TS;
                 inside = inside && node[d] >= 0 && node[d] < M.n[d];
             }
-#pragma unroll
-            for (int d = D - 1; d >= 0; --d) lin = lin * M.n[d] + (inside ? node[d] : 0);
+            // nodes outside the mesh, and nodes a sparse grid does not store, read as zero
+            const long long sl = inside ? grid_slot<D>(G, M, node[0], node[1], node[2]) : -1;
             T vi[3] = {T(0), T(0), T(0)}, dvi[3] = {T(0), T(0), T(0)};
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                vi[d] = inside ? G.v[d][lin] : T(0);
-                const T vni = inside ? G.vn[d][lin] : T(0);
+                vi[d] = sl >= 0 ? G.v[d][sl] : T(0);
+                const T vni = sl >= 0 ? G.vn[d][sl] : T(0);
                 dvi[d] = vi[d] - vni;
             }
             if constexpr (VEC) {
@@ -524,9 +553,11 @@ __global__ void __launch_bounds__(128) g2p_direct_kernel(DMesh<D, T> M, GView<T>
                         long long lin = 0;
                         bool valid = true;
 #pragma unroll
-                        for (int d = D - 1; d >= 0; --d) {
-                            valid = valid && idx[d] < B.ax[d].cnt;
-                            lin = lin * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
+                        for (int d = D - 1; d >= 0; --d) valid = valid && idx[d] < B.ax[d].cnt;
+                        if (valid) {
+                            lin = grid_slot<D>(G, M, B.ax[0].lo + idx[0], B.ax[1].lo + idx[1],
+                                               D == 3 ? B.ax[D - 1].lo + idx[D - 1] : 0);
+                            valid = lin >= 0;
                         }
                         T rel[3] = {T(0), T(0), T(0)};
                         if (need_rel) {
@@ -650,7 +681,7 @@ int occupancy_grid(K kernel, int threads, int num_sms) {
 
 template <int D, class T>
 cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const LaunchCfg& cfg) {
-    const long long nn = M.nnodes;
+    const long long nn = G.bnum ? G.cap : M.nnodes;  // a sparse grid's count is on the device
     const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_zero");
     grid_zero_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(G, nn);
@@ -660,7 +691,7 @@ cudaError_t launch_grid_zero(const DMesh<D, T>& M, const GView<T>& G, const Laun
 
 template <int D, class T>
 cudaError_t launch_grid_update(const DMesh<D, T>& M, const GView<T>& G, const Scalars<T>& s, const LaunchCfg& cfg) {
-    const long long nn = M.nnodes;
+    const long long nn = G.bnum ? G.cap : M.nnodes;  // a sparse grid's count is on the device
     const int grid = int(std::min<long long>((nn + 255) / 256, (long long)cfg.num_sms * 16));
     KernelScope ks(cfg, "grid_update");
     grid_update_kernel<D, T><<<grid, 256, 0, cfg.stream>>>(M, G, s);

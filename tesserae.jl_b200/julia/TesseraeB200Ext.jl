@@ -64,6 +64,7 @@ using Random
 const libtb = "libtesserae_b200"  # resolved through Libdl.DL_LOAD_PATH / LD_LIBRARY_PATH
 
 const TB_OK = Int32(0)
+const TB_ERR_CAPACITY = Int32(-3)
 const TB_ERR_UNSUPPORTED = Int32(-4)
 const TB_BSPLINE_QUADRATIC, TB_UGIMP, TB_WLS_BSPLINE_QUADRATIC, TB_WLS_UGIMP, TB_KC_BSPLINE_QUADRATIC, TB_KC_UGIMP =
     Int32.(0:5)
@@ -105,6 +106,10 @@ struct TbGrid
     f::NTuple{3,Ptr{Cvoid}}
     v::NTuple{3,Ptr{Cvoid}}
     vn::NTuple{3,Ptr{Cvoid}}
+    block_numbering::Ptr{Int32}   # SpGrid only (C_NULL for a dense grid)
+    active_blocks::Ptr{Int32}
+    nactive::Ptr{Int32}
+    capacity::Int64
 end
 
 struct TbPartition
@@ -277,7 +282,60 @@ function tbgrid(G::StructArray)
     m = first(something(ptrs(G.m, 1), (nothing,)))
     mv, f, v, vn = ptrs(G.mv, 3), ptrs(G.f, 3), ptrs(G.v, 3), ptrs(G.vⁿ, 3)
     any(isnothing, (m, mv, f, v, vn)) && return nothing
-    TbGrid(m, mv, f, v, vn)
+    sp = get(SPARSITY, G, nothing)  # the numbering b200_update_sparsity! keeps for this SpGrid
+    sp === nothing && return TbGrid(m, mv, f, v, vn, C_NULL, C_NULL, C_NULL, 0)
+    TbGrid(m, mv, f, v, vn, pointer(sp.numbering), pointer(sp.active), pointer(sp.nactive), sp.capacity)
+end
+
+# SpGrid (src/Grids/sparray.jl) on the B200 path: the library numbers the active
+# node blocks into Int32 arrays kept here per grid; the SpIndices' own Int
+# numbering gets a copy, so Tesserae's indexing of the SpArray agrees, and each
+# field's data vector is resized to the stored node count.
+mutable struct B200Sparsity
+    numbering::CuVector{Int32}
+    active::CuVector{Int32}
+    nactive::CuVector{Int32}
+    capacity::Int64
+end
+const SPARSITY = IdDict{Any,B200Sparsity}()
+
+"""
+    b200_update_sparsity!(grid::SpGrid, particles, partition)
+
+`update_sparsity!(grid, particles.x)` through `tb_update_sparsity_*`: bins the
+particles into `partition`, numbers the node blocks within one block of an
+occupied block (src/Grids/sparsity.jl:19-60), resizes the grid's SpArray data
+to the stored node count and zero-fills it. Returns that count.
+"""
+function b200_update_sparsity!(grid, particles, partition)
+    spinds = Tesserae.get_spinds(grid)
+    nb = length(Tesserae.blocknumbering(spinds))
+    sp = get!(SPARSITY, grid) do
+        B200Sparsity(CUDA.zeros(Int32, nb), CUDA.zeros(Int32, nb), CUDA.zeros(Int32, 2), 0)
+    end
+    bl = Tesserae.blocklength(spinds)
+    nstored = Ref{Int64}(0)
+    for attempt in 1:2
+        sp.capacity = length(Tesserae.get_data(grid.m))
+        gd = tbgrid(grid)
+        GC.@preserve grid particles partition sp begin
+            rc = ccall((sym(:tb_update_sparsity, form(particles)), libtb), Int32,
+                       (Ptr{Cvoid}, Ref{TbMesh}, Ref{TbParticles}, Ref{TbPartition}, Ref{TbGrid}, Ref{Int64}),
+                       ctx(), tbmesh(grid.x), tbparticles(particles), tbpartition(Tesserae.strategy(partition)),
+                       gd, nstored)
+        end
+        if rc == TB_ERR_CAPACITY && attempt == 1
+            for name in propertynames(grid)
+                A = getproperty(grid, name)
+                A isa Tesserae.SpArray && resize!(Tesserae.get_data(A), nstored[])
+            end
+            continue
+        end
+        check(rc, "update_sparsity")
+        break
+    end
+    Tesserae.blocknumbering(spinds) .= sp.numbering
+    nstored[]
 end
 
 tbpartition(bs::GPUBlockStrategy) =
@@ -696,6 +754,6 @@ function ChainRulesCore.rrule(::typeof(b200_rollout), v0, particles, grid, parti
     xT, pullback
 end
 
-export b200, b200_x64, b200_preserve, b200_step!, b200_rollout
+export b200, b200_x64, b200_preserve, b200_step!, b200_rollout, b200_update_sparsity!
 
 end # module

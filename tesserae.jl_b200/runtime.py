@@ -152,13 +152,41 @@ def G2P(grid: Grid, particles: Particles, mesh: CartesianMesh, params, ctx: Cont
     return particles
 
 
+def update_sparsity(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh,
+                    ctx: Context | None = None, headroom: float = 1.0) -> int:
+    """update_sparsity!(grid, particles.x) for a sparse grid (src/Grids/sparsity.jl:19-60):
+    bins the particles into `partition`, numbers the node blocks within one block
+    of a block that holds particles, zero-fills the stored fields, and returns
+    the number of stored nodes per field. The field arrays grow (to the count
+    times `headroom`) when they are too small."""
+    ctx = ctx or _default()
+    if not grid.sparse:
+        raise TypeError("update_sparsity needs a sparse grid (generate_grid(..., sparse=True))")
+    n = C.c_int64(0)
+    fn = ctx.pfn("tb_update_sparsity", particles, x64_ok=True)
+    rc = fn(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()), _ref(partition.struct()), _ref(grid.struct()),
+            C.byref(n))
+    need = int(n.value)
+    if rc == _abi.TB_ERR_CAPACITY or need * headroom > grid.capacity:
+        grid.reserve(int(need * max(headroom, 1.0)))
+        rc = fn(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()), _ref(partition.struct()),
+                _ref(grid.struct()), C.byref(n))
+    ctx.check(rc, "update_sparsity")
+    return need
+
+
 def step(grid: Grid, particles: Particles, partition: Partition, mesh: CartesianMesh, params, nsteps: int = 1,
-         ctx: Context | None = None, reorder_threshold: float | None = None):
+         ctx: Context | None = None, reorder_threshold: float | None = None, sparse_headroom: float = 1.5):
     """`nsteps` fused steps (bin -> P2G -> grid update -> G2P) without host sync.
     With `reorder_threshold`, every binning is followed by
     `reorder_particles!(particles, partition; threshold=reorder_threshold)`,
-    decided on the device."""
+    decided on the device. A sparse grid follows the particles (its sparsity is
+    updated at every step on the device); its field arrays are first sized for
+    the current positions times `sparse_headroom`, and a step whose active
+    blocks would exceed them is reported as a device error."""
     ctx = ctx or _default()
+    if grid.sparse:
+        update_sparsity(grid, particles, partition, mesh, ctx=ctx, headroom=sparse_headroom)
     if reorder_threshold is None:
         rc = ctx.pfn("tb_step", particles, x64_ok=True)(ctx.ptr, _ref(mesh.struct()), _ref(particles.struct()),
                                                         _ref(partition.struct()), _ref(grid.struct()), _ref(params),

@@ -295,17 +295,57 @@ class Adjoint:
 
 
 class Grid:
-    """SoA grid fields m, mv, f, v, vn over prod(n_nodes) column-major nodes."""
+    """SoA grid fields m, mv, f, v, vn over prod(n_nodes) column-major nodes.
 
-    def __init__(self, mesh: CartesianMesh, dtype=np.float64, backend="numpy", device=None):
-        self.mesh, self.dtype, self.backend = mesh, np.dtype(dtype).type, backend
+    `sparse=True`: the block-sparse grid (`generate_grid(SpArray, ...)`,
+    src/Grids/sparray.jl): the fields hold only the active node blocks
+    (blocks of blockwidth^dim nodes, node block of node i = i >> block_size_log2
+    per axis), `capacity` nodes each, in the storage order of the reference's
+    SpIndices (storage block k - 1, then the column-major node inside the
+    block); `block_numbering` (0 inactive, k >= 1), `active_blocks` (1-based
+    node block ids in storage order) and `nactive` describe them, and
+    runtime.update_sparsity fills them from particle positions."""
+
+    def __init__(self, mesh: CartesianMesh, dtype=np.float64, backend="numpy", device=None, sparse=False,
+                 capacity: int = 0):
+        self.mesh, self.dtype, self.backend, self.device = mesh, np.dtype(dtype).type, backend, device
+        self.sparse = bool(sparse)
         N, D = mesh.nnodes, mesh.dim
-        a = lambda shape: _alloc(backend, shape, self.dtype, device)  # noqa: E731
+        if self.sparse:
+            nb = mesh.nblocks_total
+            ai = lambda k: _alloc(backend, (k,), np.int32, device, 0)  # noqa: E731
+            self.block_numbering, self.active_blocks, self.nactive = ai(nb), ai(nb), ai(2)
+            N = self._round_capacity(capacity)
+        else:
+            self.block_numbering = self.active_blocks = self.nactive = None
+        self.capacity = N
+        self._alloc_fields(N)
+
+    @property
+    def blocklength(self) -> int:
+        return 1 << (self.mesh.block_size_log2 * self.mesh.dim)
+
+    def _round_capacity(self, n: int) -> int:
+        bl = self.blocklength
+        return max(bl, -(-int(n) // bl) * bl)
+
+    def _alloc_fields(self, N: int):
+        D = self.mesh.dim
+        a = lambda shape: _alloc(self.backend, shape, self.dtype, self.device)  # noqa: E731
         self.m = a((N,))
         self.mv = a((D, N))
         self.f = a((D, N))
         self.v = a((D, N))
         self.vn = a((D, N))
+
+    def reserve(self, nodes: int):
+        """Sparse grid: field arrays for at least `nodes` stored nodes (new,
+        zeroed arrays when they grow)."""
+        if not self.sparse:
+            raise TypeError("reserve() is for a sparse grid")
+        if nodes > self.capacity:
+            self.capacity = self._round_capacity(nodes)
+            self._alloc_fields(self.capacity)
 
     def struct(self) -> _abi.tb_grid:
         s = _abi.tb_grid()
@@ -315,11 +355,45 @@ class Grid:
             arr = getattr(s, name)
             for d, p in enumerate(_row_ptrs(getattr(self, name), D)):
                 arr[d] = p
+        if self.sparse:
+            s.block_numbering = _ptr(self.block_numbering)
+            s.active_blocks = _ptr(self.active_blocks)
+            s.nactive = _ptr(self.nactive)
+            s.capacity = self.capacity
         return s
 
     def numpy(self) -> dict:
+        keys = ("m", "mv", "f", "v", "vn") + (("block_numbering", "active_blocks", "nactive") if self.sparse else ())
         return {k: (getattr(self, k) if isinstance(getattr(self, k), np.ndarray)
-                    else getattr(self, k).detach().cpu().numpy()) for k in ("m", "mv", "f", "v", "vn")}
+                    else getattr(self, k).detach().cpu().numpy()) for k in keys}
+
+    def dense(self) -> dict:
+        """The fields on every node (numpy), zeros where a sparse grid stores nothing."""
+        g = self.numpy()
+        if not self.sparse:
+            return {k: g[k] for k in ("m", "mv", "f", "v", "vn")}
+        mesh, D = self.mesh, self.mesh.dim
+        n, nb, L = mesh.n_nodes, mesh.nblocks(), mesh.block_size_log2
+        W = 1 << L
+        k = int(g["nactive"][0])
+        stored = np.arange(k * self.blocklength)
+        blk = g["active_blocks"][stored >> (L * D)] - 1
+        q = stored & (self.blocklength - 1)
+        idx = []
+        for d in range(D):
+            b = (blk // int(np.prod(nb[:d]))) % nb[d]
+            idx.append(b * W + (q // W ** d) % W)
+        inside = np.all([idx[d] < n[d] for d in range(D)], axis=0)
+        lin = np.zeros_like(stored)
+        for d in reversed(range(D)):
+            lin = lin * n[d] + idx[d]
+        out = {}
+        for key in ("m", "mv", "f", "v", "vn"):
+            a = g[key]
+            full = np.zeros(a.shape[:-1] + (mesh.nnodes,), dtype=a.dtype)
+            full[..., lin[inside]] = a[..., stored[inside]]
+            out[key] = full
+        return out
 
 
 class Partition:
@@ -424,8 +498,11 @@ def generate_particles(mesh: CartesianMesh, alg: GridSampling = GridSampling(), 
     return P.to(backend, device=device, dtype=dtype, x64=x64)
 
 
-def generate_grid(mesh: CartesianMesh, dtype=np.float64, backend="numpy", device=None) -> Grid:
-    return Grid(mesh, dtype, backend, device)
+def generate_grid(mesh: CartesianMesh, dtype=np.float64, backend="numpy", device=None, sparse=False,
+                  capacity: int = 0) -> Grid:
+    """generate_grid(GridProp, mesh) (src/Grids/grid.jl); `sparse=True` is
+    generate_grid(SpArray, GridProp, mesh) (src/Grids/sparray.jl)."""
+    return Grid(mesh, dtype, backend, device, sparse, capacity)
 
 
 def generate_basis_weights(dim, n, dtype=np.float64, backend="numpy", device=None) -> BasisWeights:
