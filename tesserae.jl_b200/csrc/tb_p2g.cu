@@ -1164,7 +1164,11 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* rec = reinterpret_cast<float*>(smem_raw);
+    // staged partials as (m, m v_x), (m v_y, m v_z), (f_x, f_y) pairs, then f_z:
+    // [pair][jk][pencil][x] float2 and [jk][pencil][x] float (8-byte aligned)
     float* part = rec + NR * CRS + SKW * NPENCIL;
+    float2* part2 = reinterpret_cast<float2*>(part);
+    float* partz = part + 6 * CSTR;
     int* gcount = reinterpret_cast<int*>(part + NC * CSTR);
     int* gstart = gcount + NG;
     int* pslot = gstart + NG + 1;
@@ -1340,14 +1344,11 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
                     // x-node gx of rows (j, k) is final: stage it, shift the rows
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        float* dst = part + ((j + 3 * k) * NPENCIL + pc) * TS + gx;
-                        dst[0 * CSTR] = acc[0][j].a01.x;
-                        dst[1 * CSTR] = acc[0][j].a01.y;
-                        dst[2 * CSTR] = acc[0][j].a23.x;
-                        dst[3 * CSTR] = acc[0][j].a23.y;
-                        dst[4 * CSTR] = acc[0][j].f01.x;
-                        dst[5 * CSTR] = acc[0][j].f01.y;
-                        dst[6 * CSTR] = acc[0][j].f2;
+                        const int o = ((j + 3 * k) * NPENCIL + pc) * TS + gx;
+                        part2[o] = acc[0][j].a01;
+                        part2[CSTR + o] = acc[0][j].a23;
+                        part2[2 * CSTR + o] = acc[0][j].f01;
+                        partz[o] = acc[0][j].f2;
                         acc[0][j] = acc[1][j];
                         acc[1][j] = acc[2][j];
                         acc[2][j].a01 = acc[2][j].a23 = acc[2][j].f01 = make_float2(0.f, 0.f);
@@ -1360,9 +1361,8 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
             //      atomic per non-zero value (gravity from the summed mass)
             for (int t = tid; t < TN; t += NT) {
                 const int tx = t % TS, ty = (t / TS) % TS, tz = t / (TS * TS);
-                float val[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c) val[c] = 0.0f;
+                float2 a01 = make_float2(0.f, 0.f), a23 = a01, f01 = a01;
+                float f2 = 0.f;
 #pragma unroll
                 for (int kk = 0; kk < 3; ++kk)
 #pragma unroll
@@ -1370,9 +1370,16 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
                         const int gy = ty - jj, gz = tz - kk;
                         if (gy < 0 || gy >= G1 || gz < 0 || gz >= G1) continue;
                         const int idx = ((jj + 3 * kk) * NPENCIL + gy + G1 * gz) * TS + tx;
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) val[c] += part[idx + c * CSTR];
+                        const float2 p0 = part2[idx], p1 = part2[CSTR + idx], p2 = part2[2 * CSTR + idx];
+                        a01.x += p0.x;
+                        a01.y += p0.y;
+                        a23.x += p1.x;
+                        a23.y += p1.y;
+                        f01.x += p2.x;
+                        f01.y += p2.y;
+                        f2 += partz[idx];
                     }
+                float val[NC] = {a01.x, a01.y, a23.x, a23.y, f01.x, f01.y, f2};
 #pragma unroll
                 for (int d = 0; d < 3; ++d) val[4 + d] += s.g[d] * val[0];
                 grid_add<3>(G, M, err, org[0] + tx, org[1] + ty, org[2] + tz, val);
