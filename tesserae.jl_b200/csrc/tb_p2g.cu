@@ -1133,14 +1133,15 @@ __device__ __forceinline__ void accumulate_plane(const PairRec& o, const SlotPol
         const float wyz = wy[j] * wz, dyz = dy[j] * wz, wdz = wy[j] * dz;
         const float2 WYZ = make_float2(wyz, wyz);
         const float2 fa01 = __fmul2_rn(o.sa, WYZ);
+        // the row's (m, m v) times wyz once; each x-slot then needs one FMA per pair
+        const float2 m0j = __fmul2_rn(o.m0, WYZ), m1j = __fmul2_rn(o.m1, WYZ);
         const float2 fb01 = __ffma2_rn(o.sc, make_float2(wdz, wdz), __fmul2_rn(o.sb, make_float2(dyz, dyz)));
         const float fa2 = o.sc.x * wyz;
         const float fb2 = __fmaf_rn(o.s5z.x, wdz, o.sc.y * dyz);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const float2 w = __fmul2_rn(wxs[i], WYZ);
-            acc[i][j].a01 = __ffma2_rn(w, o.m0, acc[i][j].a01);
-            acc[i][j].a23 = __ffma2_rn(w, o.m1, acc[i][j].a23);
+            acc[i][j].a01 = __ffma2_rn(wxs[i], m0j, acc[i][j].a01);
+            acc[i][j].a23 = __ffma2_rn(wxs[i], m1j, acc[i][j].a23);
             acc[i][j].f01 = __ffma2_rn(dxs[i], fa01, __ffma2_rn(wxs[i], fb01, acc[i][j].f01));
             acc[i][j].f2 = __fmaf_rn(dxs[i].x, fa2, __fmaf_rn(wxs[i].x, fb2, acc[i][j].f2));
         }
