@@ -43,6 +43,25 @@ __device__ __forceinline__ int block_split(const int* totals, int per_cta) {
     return int(s < 1 ? 1 : (s > 8 ? 8 : s));
 }
 
+// The passes of one block's particle range [s0, s1) for kernels that hold `per`
+// particles (a multiple of 8) at a time: pass i of count() = ceil(n / per)
+// takes the 8-particle chunks i, i + count(), i + 2 count(), ..., so every pass
+// samples the whole block. A block denser than one pass whose particles lie in
+// lattice order (4^3 per cell: 16 lattice rows of x per block row) would
+// otherwise give each pass a few (y, z) rows of the block, all of its records
+// to a few pencils, and a sweep as long as the longest of them. A 32-particle
+// warp load touches 4 chunks of 8, the same sectors as a contiguous one for
+// 4-byte fields. With one pass this is the range itself, in order.
+struct BlockPasses {
+    int s0, s1, npass;
+    __device__ __forceinline__ BlockPasses(int a, int b, int per) : s0(a), s1(b), npass((b - a + per - 1) / per) {}
+    __device__ __forceinline__ int count() const { return npass; }
+    // position in the block list of item t (0 <= t < per) of pass i (>= s1: past the range)
+    __device__ __forceinline__ int pos(int i, int t) const { return s0 + ((i + npass * (t >> 3)) << 3) + (t & 7); }
+    // pos(i, t + nt) - pos(i, t) for nt a multiple of 8
+    __device__ __forceinline__ int step(int nt) const { return npass * nt; }
+};
+
 // Forward-mode dual number with the three derivatives with respect to a
 // particle's position: the weights evaluated in Dual3 give dN/dx_p and
 // d(grad N)/dx_p for the reverse step of every basis (WLS, KernelCorrection,

@@ -708,6 +708,7 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
     constexpr int ITEMS = (NR + NT - 1) / NT;
     constexpr int CSTR = NPENCIL * NJK * TS;  // stride between components in the staging array
     static_assert(NPENCIL <= 32, "pencil ranking runs in one warp");
+    static_assert(NR % 8 == 0 && NT % 8 == 0, "passes in 8-particle chunks");
 
     constexpr int RS = (MODE == 1) ? CRS : PRS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -752,8 +753,9 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
             }
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0 + piece * NR; b0 < s1; b0 += pieces * NR) {
-            const int nbat = min(NR, s1 - b0);
+        const BlockPasses bp(s0, s1, NR);
+        for (int bi = piece; bi < bp.count(); bi += pieces) {
+            const int q0 = bp.pos(bi, tid), qstep = bp.step(NT);
             // ---- 1a. every global load of the batch first (the ids, then all of
             //      the particles' fields at once: two dependent round trips per
             //      batch), then window start -> group, rank within the group. The
@@ -764,8 +766,8 @@ __global__ void __launch_bounds__(P2G_THREADS, MODE == 1 ? 3 : (sizeof(T) == 4 ?
             double pxd[ITEMS][3];
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
-                const int ti = tid + u * NT;
-                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+                const int ti = tid + u * NT, q = q0 + u * qstep;
+                pid[u] = (ti < NR && q < s1) ? perm[q] - 1 : -1;
             }
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
@@ -1160,7 +1162,7 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
     constexpr int NJK = SH::NJK, NPENCIL = SH::NPENCIL;
     constexpr int CSTR = NPENCIL * NJK * TS;  // stride between components in the staging array
     constexpr int SKW = 2;                    // record skew per pencil (words)
-    static_assert(NR % NT == 0, "whole items per thread");
+    static_assert(NR % NT == 0 && NT % 8 == 0, "whole items per thread, passes in 8-particle chunks");
     static_assert(3 * NPENCIL <= NT, "one plane lane per (pencil, z slot)");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1200,15 +1202,16 @@ __global__ void __launch_bounds__(PLANE_THREADS, 3)
             continue;
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0 + piece * NR; b0 < s1; b0 += split * NR) {
-            const int nbat = min(NR, s1 - b0);
+        const BlockPasses bp(s0, s1, NR);
+        for (int bi = piece; bi < bp.count(); bi += split) {
+            const int q0 = bp.pos(bi, tid), qstep = bp.step(NT);
             // ---- 1a. every global load of the batch first, then group and rank;
             //      the record's 14 values stay in registers until the slot is known
             int pid[ITEMS], grp[ITEMS], rank[ITEMS];
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
-                const int ti = tid + u * NT;
-                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+                const int ti = tid + u * NT, q = q0 + u * qstep;
+                pid[u] = (ti < NR && q < s1) ? perm[q] - 1 : -1;
             }
             float pv[ITEMS][3], pV[ITEMS], pm[ITEMS], psg[ITEMS][6], pt[ITEMS][3];
             double pxd[ITEMS][3];
@@ -1457,7 +1460,7 @@ __global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
     constexpr int NJK = SH::NJK, NPENCIL = SH::NPENCIL;
     constexpr int CSTR = NPENCIL * NJK * TS;
     constexpr int SKW = 2;
-    static_assert(NR % NT == 0, "whole items per thread");
+    static_assert(NR % NT == 0 && NT % 8 == 0, "whole items per thread, passes in 8-particle chunks");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* rec = reinterpret_cast<T*>(smem_raw);
@@ -1488,14 +1491,15 @@ __global__ void __launch_bounds__(GEN_THREADS, sizeof(T) == 4 ? 2 : 1)
             }
         }
         const int s0 = offsets[b], s1 = offsets[b + 1];
-        for (int b0 = s0 + piece * NR; b0 < s1; b0 += split * NR) {
-            const int nbat = min(NR, s1 - b0);
+        const BlockPasses bp(s0, s1, NR);
+        for (int bi = piece; bi < bp.count(); bi += split) {
+            const int q0 = bp.pos(bi, tid), qstep = bp.step(NT);
             // ---- 1a. window start -> group and rank
             int pid[ITEMS], grp[ITEMS], rank[ITEMS];
 #pragma unroll
             for (int u = 0; u < ITEMS; ++u) {
-                const int ti = tid + u * NT;
-                pid[u] = ti < nbat ? perm[b0 + ti] - 1 : -1;
+                const int ti = tid + u * NT, q = q0 + u * qstep;
+                pid[u] = (ti < NR && q < s1) ? perm[q] - 1 : -1;
                 grp[u] = -1;
                 rank[u] = 0;
             }
