@@ -432,6 +432,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
     constexpr int TS = SH::TS, TN = SH::TN, NC = SH::NC, G1 = SH::G1, NG = SH::NG;
     constexpr int NJK = SH::NJK, NSUB = SH::NSUB, NPENCIL = SH::NPENCIL, CSTR = SH::CSTR;
     static_assert((NPENCIL + NSUB - 1) / NSUB <= NW, "one pencil per lane");
+    static_assert(NT % 8 == 0 && SC_NR % 8 == 0, "passes in 8-particle chunks");
     constexpr int ITEMS = (SC_NR + NT - 1) / NT;
     extern __shared__ __align__(16) double sc_smem[];
     double* rec = sc_smem;   // batch records, at the thread's slot
@@ -458,14 +459,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
 
     const long long lo_r = min((long long)blockIdx.x * per_cta, (long long)nassigned);
     const int r0 = int(lo_r), r1 = int(min(lo_r + per_cta, (long long)nassigned));
-    int c0 = r0;
+    // c0: start of the current block's segment of [r0, r1), taken in passes
+    // that each sample the whole segment (BlockPasses); pass: the current one
+    int c0 = r0, pass = 0;
     int b = c0 < r1 ? blockids[perm[c0] - 1] - 1 : -1;
     while (c0 < r1) {
         int org[3];
         block_origin<D, T, BW>(M, b, org);
-        const int c1 = min(min(offsets[b + 1], r1), c0 + SC_NR);
+        const int c1 = min(offsets[b + 1], r1);
+        const BlockPasses bp(c0, c1, SC_NR);
+        const bool last = pass + 1 >= bp.count();
+        const int q0 = bp.pos(pass, tid), qstep = bp.step(NT);
         // the next batch's block, loaded early (uniform over the CTA)
-        const int nb_next = c1 < r1 ? blockids[perm[c1] - 1] - 1 : -1;
+        const int nb_next = !last ? b : (c1 < r1 ? blockids[perm[c1] - 1] - 1 : -1);
         // ---- 1a. particles tid, tid + NT, ...: window start -> group and rank in
         //      the group; the record goes to the particle's own slot. Every
         //      global load of the batch is issued before the first use.
@@ -475,7 +481,8 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
         for (int u = 0; u < ITEMS; ++u) {
             grp[u] = -1;
             rank[u] = 0;
-            pid[u] = tid + u * NT < c1 - c0 ? perm[c0 + tid + u * NT] - 1 : -1;
+            const int q = q0 + u * qstep;
+            pid[u] = (tid + u * NT < SC_NR && q < c1) ? perm[q] - 1 : -1;
         }
         double px[ITEMS][3];
         T pl[ITEMS];
@@ -490,7 +497,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
 #pragma unroll
         for (int u = 0; u < ITEMS; ++u) {
             if (pid[u] < 0) continue;
-            const int j = c0 + tid + u * NT;
+            const int j = q0 + u * qstep;
             double* r = rec + (tid + u * NT) * SC_RS;
 #pragma unroll
             for (int rr = 0; rr < D; ++rr) {
@@ -600,7 +607,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1) adj_scatter_kernel(DMesh<D, T> 
             }
         }
         __syncthreads();
-        c0 = c1;
+        if (last) {
+            c0 = c1;
+            pass = 0;
+        } else {
+            ++pass;
+        }
         if (nb_next != b) {
             // ---- 3. flush the block: rows to the staging array, then per tile
             //      node the staged rows, one global atomic per non-zero value
