@@ -933,106 +933,11 @@ __device__ __forceinline__ bool dual_basis(const DMesh<D, Dual3>& MD, const Scal
     return prepare_basis<D, Dual3, true>(MD, s.basis, xd, Dual3(double(l)), B, err);
 }
 
-// A particle's basis as the reverse step differentiates it. Every axis factor
-// depends on its own coordinate only, so per axis the jets (val, der) carry one
-// derivative, d/dx_a; the WLS moment inverse depends on all coordinates and
-// keeps Dual3 (its upper triangle: it is symmetric). Compressed from the Dual3
-// basis (whose axis entries have zero derivatives along the other axes), so the
-// window's node evaluations read 36 doubles (plus 40 with WLS) instead of the
-// whole Dual3 basis, and stay in registers.
+// N, grad N (values and x_p derivatives) at window slot (i, j, k), r = X - x_p.
 template <int D>
-struct CDBasis {
-    int lo[3], cnt[3];
-    double val[3][3], dval[3][3], der[3][3], dder[3][3];
-    Dual3 Mi[(D + 1) * (D + 2) / 2];
-    bool wls;
-};
-
-template <int D>
-__device__ __forceinline__ int mi_slot(int r, int c) {  // upper triangle of the (D+1)^2 matrix
-    if (r > c) {
-        const int t = r;
-        r = c;
-        c = t;
-    }
-    return r * (D + 1) - r * (r - 1) / 2 + (c - r);
-}
-
-template <int D>
-__device__ __forceinline__ void compress_basis(const Basis<D, Dual3>& B, CDBasis<D>& C) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        C.lo[a] = a < D ? B.ax[a].lo : 0;
-        C.cnt[a] = a < D ? B.ax[a].cnt : 1;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            C.val[a][q] = a < D ? B.ax[a].val[q].v : 1.0;
-            C.dval[a][q] = a < D ? B.ax[a].val[q].d[a] : 0.0;
-            C.der[a][q] = a < D ? B.ax[a].der[q].v : 0.0;
-            C.dder[a][q] = a < D ? B.ax[a].der[q].d[a] : 0.0;
-        }
-    }
-    C.wls = B.wls;
-    if (B.wls) {
-#pragma unroll
-        for (int r = 0; r <= D; ++r)
-#pragma unroll
-            for (int c = r; c <= D; ++c) C.Mi[mi_slot<D>(r, c)] = B.Mi[r][c];
-    }
-}
-
-// N, grad N (values and x_p derivatives) at window slot (i, j, k), r = X - x_p:
-// the kernel value as the product of the axis factors (grad N = the product
-// with one factor's derivative, times h_inv), or with WLS N = w (Mi P)_0 and
-// grad N = w (Mi P)_{1..D}, P = (1, r) (wls.jl:51-84) -- eval_node in Dual3,
-// with the zero cross derivatives of the axis factors left out.
-template <int D>
-__device__ __forceinline__ void dual_node(const CDBasis<D>& C, double hinv, int i, int j, int k, const Dual3* rel,
-                                          Dual3& N, Dual3* G) {
-    const int q[3] = {i, j, k};
-    double v[3], dv[3], g[3], dg[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        v[a] = C.val[a][q[a]];
-        dv[a] = C.dval[a][q[a]];
-        g[a] = C.der[a][q[a]];
-        dg[a] = C.dder[a][q[a]];
-    }
-    Dual3 w(v[0] * v[1] * v[2]);
-#pragma unroll
-    for (int b = 0; b < 3; ++b) w.d[b] = b < D ? (b == 0 ? dv[0] * v[1] * v[2] : b == 1 ? v[0] * dv[1] * v[2] : v[0] * v[1] * dv[2]) : 0.0;
-    if (!C.wls) {
-        N = w;
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-            // factor c replaced by its derivative; d/dx_b of that product
-            double f[3] = {v[0], v[1], v[2]}, df[3] = {dv[0], dv[1], dv[2]};
-            f[c] = g[c];
-            df[c] = dg[c];
-            G[c] = Dual3(f[0] * f[1] * f[2] * hinv);
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                double t = df[b];
-#pragma unroll
-                for (int e = 0; e < 3; ++e)
-                    if (e != b) t *= f[e];
-                G[c].d[b] = b < D ? t * hinv : 0.0;
-            }
-        }
-        return;
-    }
-    Dual3 P[D + 1];
-    P[0] = Dual3(1.0);
-#pragma unroll
-    for (int d = 0; d < D; ++d) P[d + 1] = rel[d];
-#pragma unroll
-    for (int r = 0; r <= D; ++r) {
-        Dual3 acc(0.0);
-#pragma unroll
-        for (int c = 0; c <= D; ++c) acc += C.Mi[mi_slot<D>(r, c)] * P[c];
-        if (r == 0) N = w * acc;
-        else G[r - 1] = w * acc;
-    }
+__device__ __forceinline__ void dual_node(const DMesh<D, Dual3>& MD, const Basis<D, Dual3>& B, int i, int j, int k,
+                                          const Dual3* rel, Dual3& N, Dual3* G) {
+    eval_node<D, Dual3>(MD, B, i, j, k, rel, N, G);
 }
 
 template <int D, class T>
@@ -1047,14 +952,8 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
         double x[3];
         load_xd<D, T>(P, p, x);
         const T l = P.l ? P.l[p] : s.gimp_l;
-        CDBasis<D> B;
-        bool in = false;
-        if (blockids[p] != 0) {
-            Basis<D, Dual3> Bd;
-            in = dual_basis<D, T>(MD, s, x, l, Bd, err);
-            if (in) compress_basis<D>(Bd, B);
-        }
-        const double hinv = MD.h_inv.v;
+        Basis<D, Dual3> B;
+        const bool in = blockids[p] != 0 && dual_basis<D, T>(MD, s, x, l, B, err);
         double F[3][3] = {}, Fb[3][3] = {}, L[3][3] = {};
         load_F<D, T>(P, p, F);
 #pragma unroll
@@ -1067,23 +966,20 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
             valid = true;
 #pragma unroll
             for (int d = D - 1; d >= 0; --d) {
-                valid = valid && idx[d] < B.cnt[d];
-                I = I * M.n[d] + min(B.lo[d] + idx[d], M.n[d] - 1);
+                valid = valid && idx[d] < B.ax[d].cnt;
+                I = I * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
 #pragma unroll
             for (int d = 0; d < D; ++d) {
-                rel[d] = node_coord(MD, d, B.lo[d] + idx[d]) - Dual3(x[d]);
+                rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(x[d]);
                 rel[d].d[d] = -1.0;
             }
         };
         if (in) {
-#pragma unroll
             for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
-#pragma unroll
                 for (int j = 0; j < 3; ++j)
-#pragma unroll
                     for (int i = 0; i < 3; ++i) {
                         long long I;
                         Dual3 rel[3];
@@ -1091,7 +987,7 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
                         node_of(i, j, k, I, rel, valid);
                         if (!valid) continue;
                         Dual3 N, Gn[3];
-                        dual_node<D>(B, hinv, i, j, k, rel, N, Gn);
+                        dual_node<D>(MD, B, i, j, k, rel, N, Gn);
 #pragma unroll
                         for (int r = 0; r < D; ++r)
 #pragma unroll
@@ -1131,11 +1027,8 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
                 for (int c = 0; c < D; ++c) Bb[r][c] = A.B[r + c * D][p];
         }
         if (in) {
-#pragma unroll
             for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
-#pragma unroll
                 for (int j = 0; j < 3; ++j)
-#pragma unroll
                     for (int i = 0; i < 3; ++i) {
                         long long I;
                         Dual3 rel[3];
@@ -1143,7 +1036,7 @@ __global__ void __launch_bounds__(128) adj_g2p_gen_kernel(DMesh<D, T> M, GView<T
                         node_of(i, j, k, I, rel, valid);
                         if (!valid) continue;
                         Dual3 N, Gn[3];
-                        dual_node<D>(B, hinv, i, j, k, rel, N, Gn);
+                        dual_node<D>(MD, B, i, j, k, rel, N, Gn);
                         double vi[3] = {}, vni[3] = {};
 #pragma unroll
                         for (int d = 0; d < D; ++d) {
@@ -1210,13 +1103,8 @@ __global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T
         double x[3];
         load_xd<D, T>(P, p, x);
         const T l = P.l ? P.l[p] : s.gimp_l;
-        CDBasis<D> B;
-        {
-            Basis<D, Dual3> Bd;
-            if (!dual_basis<D, T>(MD, s, x, l, Bd, err)) continue;
-            compress_basis<D>(Bd, B);
-        }
-        const double hinv = MD.h_inv.v;
+        Basis<D, Dual3> B;
+        if (!dual_basis<D, T>(MD, s, x, l, B, err)) continue;
         const double mp = P.m ? double(P.m[p]) : double(s.mass);
         const double Vp = double(P.V[p]);
         double vp[3] = {}, Bp[3][3] = {}, sg[3][3] = {};
@@ -1230,19 +1118,16 @@ __global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T
                 if (apic) Bp[r][c] = double(P.B[r + c * D][p]);
             }
         double xb[3] = {}, vbs[3] = {}, sb[3][3] = {}, Vb = 0.0, Bbs[3][3] = {};
-#pragma unroll
         for (int k = 0; k < (D == 3 ? 3 : 1); ++k)
-#pragma unroll
             for (int j = 0; j < 3; ++j)
-#pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     const int idx[3] = {i, j, k};
                     long long I = 0;
                     bool valid = true;
 #pragma unroll
                     for (int d = D - 1; d >= 0; --d) {
-                        valid = valid && idx[d] < B.cnt[d];
-                        I = I * M.n[d] + min(B.lo[d] + idx[d], M.n[d] - 1);
+                        valid = valid && idx[d] < B.ax[d].cnt;
+                        I = I * M.n[d] + min(B.ax[d].lo + idx[d], M.n[d] - 1);
                     }
                     if (!valid) continue;
                     Dual3 rel[3];
@@ -1250,11 +1135,11 @@ __global__ void __launch_bounds__(128) adj_p2g_gen_kernel(DMesh<D, T> M, PView<T
                     for (int d = 0; d < 3; ++d) rel[d] = Dual3(0.0);
 #pragma unroll
                     for (int d = 0; d < D; ++d) {
-                        rel[d] = node_coord(MD, d, B.lo[d] + idx[d]) - Dual3(x[d]);
+                        rel[d] = node_coord(MD, d, B.ax[d].lo + idx[d]) - Dual3(x[d]);
                         rel[d].d[d] = -1.0;
                     }
                     Dual3 N, Gn[3];
-                    dual_node<D>(B, hinv, i, j, k, rel, N, Gn);
+                    dual_node<D>(MD, B, i, j, k, rel, N, Gn);
                     double u[3] = {};
 #pragma unroll
                     for (int d = 0; d < D; ++d) {
