@@ -37,21 +37,22 @@ def make_consistent(P, prm):
 
 
 def box_scene(tb, dim=3, cells=8, lo=0.25, hi=0.75, seed=0, material=0, basis=0, alpha=1.0, walls=0,
-              E=1e3, nu=0.3, dt=1e-3, dtype=np.float64, vscale=0.5, gravity=None):
-    """A box of particles (2 per cell per axis, jittered) with random velocities
-    and per-particle Lame parameters, on a unit-square/cube mesh."""
+              E=1e3, nu=0.3, dt=1e-3, dtype=np.float64, vscale=0.5, gravity=None, ppc=2):
+    """A box of particles (`ppc` per cell per axis, jittered, in lattice order)
+    with random velocities and per-particle Lame parameters, on a unit-square/cube
+    mesh."""
     rng = np.random.default_rng(seed)
     h = 1.0 / cells
     mesh = tb.CartesianMesh(h, *([(0.0, 1.0)] * dim))
-    ax = np.arange(lo + h / 4, hi, h / 2)
+    ax = np.arange(lo + h / (2 * ppc), hi, h / ppc)
     grids = np.meshgrid(*([ax] * dim), indexing="ij")
     pts = np.stack([g.ravel(order="F") for g in grids])
-    pts = pts + rng.uniform(-h / 16, h / 16, size=pts.shape)
+    pts = pts + rng.uniform(-h / (8 * ppc), h / (8 * ppc), size=pts.shape)
     n = pts.shape[1]
     P = tb.Particles(n, dim, np.float64, optional=("mu", "lam"))
     P.x[...] = pts
     P.v[...] = rng.uniform(-vscale, vscale, size=(dim, n))
-    V0 = (h / 2) ** dim
+    V0 = (h / ppc) ** dim
     mu, lam = tb.lame(E * np.exp(rng.normal(0.0, 0.1, size=n)), nu)
     P.mu[...] = mu
     P.lam[...] = lam

@@ -28,6 +28,9 @@ CASES = {
     "fluid": dict(dim=3, material=1),
     "walls": dict(dim=3, lo=0.02, hi=0.4, walls=0b111111),
     "bspline2d": dict(dim=2, cells=16),
+    # 4^3 particles per cell in lattice order: 4096 per block, so the scatter
+    # takes each block in several passes
+    "dense": dict(dim=3, ppc=4),
 }
 
 
