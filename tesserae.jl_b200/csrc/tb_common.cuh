@@ -964,7 +964,7 @@ __device__ __forceinline__ void load_F(const PView<T>& P, long long p, double (&
         for (int c = 0; c < D; ++c) F[r][c] = P.F[r + c * D][p];
 }
 
-// F is passed in (loaded early by the caller so the load overlaps the gather).
+// F is passed in (the caller chooses when to load it).
 template <int D, class T, bool VM = false>
 __device__ __forceinline__ void particle_update(const PView<T>& P, const Scalars<T>& s, long long p,
                                                 const T (&gv)[3][3], const double (&F)[3][3]) {

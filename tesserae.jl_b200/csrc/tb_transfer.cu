@@ -331,8 +331,14 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
             }
 #pragma unroll
             for (int d = 0; d < D; ++d) vp[d] = P.v[d][p];
+            // F (72 bytes in FP64): the FP32 B-spline/uGIMP kernel (64 registers)
+            // loads it after the gather, where holding it across the gather cost
+            // spills (G2P 1.032 -> 1.019 ms on cube3d); the FP64 and WLS/APIC
+            // kernels load it here so that the load overlaps the gather (loading
+            // it late measured 7% and 1% slower there).
+            constexpr bool LATE_F = !GEN && sizeof(T) == 4;
             double F[3][3];
-            load_F<D, T>(P, p, F);
+            if constexpr (!LATE_F) load_F<D, T>(P, p, F);
             const T l = P.l ? P.l[p] : s.gimp_l;
             T vpic[3] = {T(0), T(0), T(0)}, dvf[3] = {T(0), T(0), T(0)}, dxs[3] = {T(0), T(0), T(0)};
             T gv[3][3] = {}, Bn[3][3] = {};
@@ -494,6 +500,7 @@ __global__ void __launch_bounds__(128, (GEN || VM) ? (sizeof(T) == 4 ? 4 : 2) : 
                             }
                 }
             }
+            if constexpr (LATE_F) load_F<D, T>(P, p, F);
             g2p_finish<D, T, VM>(P, s, p, x, vp, vpic, dvf, gv, dxs, Bn, F);
             int nb = 0;
             if constexpr (X64) {
